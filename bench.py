@@ -1,0 +1,299 @@
+"""Throughput of the WCSPH step in particle-steps/s on B200 (one JSON line).
+
+Workload (default): the 3D dam break at dx = 1 mm, 2,000,000 fluid particles,
+with the fixed sphere obstacle (r = 0.02 m at (0.25, 0.1, 0.03)) as geometry
+boundary particles plus 3-layer walls, CFL 0.25 with dt computed on the
+device each step, alpha = 0.02. Inputs are synthetic (seeded jitter), built
+on the host. A "step" is one full SPH step of every particle.
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl reference] [--workload dam_break_1mm_sphere]
+
+Under torchrun each rank runs its own replica (instances are independent, no
+collective on the data path); rank 0 prints the whole-job throughput.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import re
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "particle-steps/s on 1 B200: plain vs batched+closure at fixed error"
+UNIT = "particle-steps/s"
+WORKLOADS = {
+    "dam_break_1mm_sphere": dict(dx=0.001, sphere=True),   # 2,000,000 particles
+    "dam_break_4mm": dict(dx=0.004, sphere=False),          # 31,250 particles
+}
+
+
+def roofline_bytes():
+    src = open(os.path.join(ROOT, "include", "sph_roofline.h")).read()
+    return {k: int(v) for k, v in re.findall(r"#define (SPH_BYTES_\w+) (\d+)", src)}
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [s.strip() for s in line.split(",")]
+            if len(parts) >= 9:
+                self.rows.append(parts)
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in self.rows for k in range(4) if r[5 + k].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def build_scenario(name: str, seed: int):
+    from ultraballpit_b200 import domain
+    w = WORKLOADS[name]
+    return domain.dam_break(w["dx"], seed=seed, sphere=w["sphere"], with_sdf=w["sphere"])
+
+
+def cpu_reference_run(sc, steps: int, warmup: int, budget_s: float, threads: int):
+    """Time the CPU oracle (the reference algorithm, grid-accelerated boundary
+    loops with identical results) on the same workload."""
+    from oracle import oracle as orc
+    k = orc.OracleKernel(*sc.kernel_args(), alpha=sc.alpha, tier=1, threads=threads, pow_mode=0)
+    for _ in range(warmup):
+        k.step(k.compute_timestep(sc.cfl_number))
+    done, t0 = 0, time.perf_counter()
+    while done < steps:
+        k.step(k.compute_timestep(sc.cfl_number))
+        done += 1
+        if time.perf_counter() - t0 > budget_s:
+            break
+    el = time.perf_counter() - t0
+    return len(sc.particles) * done / el, done, el
+
+
+def run_reference_arm(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    sc = build_scenario(args.workload, seed=args.seed)
+    threads = os.cpu_count() or 1
+    value, done, el = cpu_reference_run(sc, args.steps, min(args.warmup, 1), args.ref_budget, threads)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": done, "warmup": min(args.warmup, 1), "ms_per_step": el / done * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded dam break)",
+        "config": {"workload": args.workload, "particles": len(sc.particles), "boundary": len(sc.boundary)},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": f"{done} full steps of {args.workload} ({len(sc.particles)} particles), "
+                                   f"oracle tier G (reference arithmetic, grid-visited boundary terms)"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_cuda_arm(args):
+    import torch
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    from ultraballpit_b200.kernel import CudaKernel
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x: float) -> float:
+        if dist is None:
+            return x
+        t = torch.tensor([x], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    sc = build_scenario(args.workload, seed=args.seed + rank)
+    n = len(sc.particles)
+    kw = dict(alpha=sc.alpha, beta=sc.beta, device=local)
+
+    # ---- device-resident throughput (value) ------------------------------
+    k = CudaKernel(*sc.kernel_args(), **kw)
+    stream = torch.cuda.ExternalStream(k.stream())
+    k.step_auto(args.warmup, want_dt=True)
+    state_bytes = n * 4 * (16 * 6 + 8 * 2 + 4 * 6)
+    barrier()
+    l0 = k.launch_count()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        e0.record(stream)
+        k.step_auto(args.steps, want_dt=False)
+        e1.record(stream)
+        e1.synchronize()
+    launches = k.launch_count() - l0
+    barrier()
+    ms = max_over_ranks(e0.elapsed_time(e1))
+    value = n * args.steps * world / (ms / 1e3)
+
+    # ---- per-kernel durations (profiled steps, events between stages) -----
+    prof_steps = max(3, min(args.steps // 4, 50))
+    acc = {}
+    for _ in range(prof_steps):
+        dt = k.compute_timestep()
+        p = k.step_profiled(dt)
+        for kk, v in p.items():
+            acc[kk] = acc.get(kk, 0.0) + v
+    avg = {kk: v / prof_steps for kk, v in acc.items()}
+    stage_keys = ["xsph_drift_us", "sort_us", "density_us", "boundary_pressure_us", "forces_us"]
+    dom = max(stage_keys, key=lambda s: avg[s])
+    rb = roofline_bytes()
+    bytes_of = {"xsph_drift_us": rb["SPH_BYTES_XSPH_DRIFT"] * n,
+                "sort_us": rb["SPH_BYTES_SORT"] * n + rb["SPH_BYTES_PER_CELL"] * k.grid_info()["total_cells"],
+                "density_us": rb["SPH_BYTES_DENSITY"] * n,
+                "boundary_pressure_us": rb["SPH_BYTES_PER_BOUNDARY"] * len(sc.boundary),
+                "forces_us": rb["SPH_BYTES_FORCES"] * n}
+    peak, peak_kind = measured_peaks()
+    achieved = bytes_of[dom] / (avg[dom] * 1e-6) / 1e9
+    traffic = None
+    tfile = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    if os.path.exists(tfile):
+        t = json.load(open(tfile)).get(dom.replace("_us", ""))
+        if t and "bytes_per_particle" in t:
+            traffic = t["bytes_per_particle"] * n
+    roofline = {"bound": "hbm", "kernel": dom.replace("_us", ""), "achieved": achieved, "peak": peak,
+                "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
+                "peak_source": peak_kind, "stage_us": {s.replace("_us", ""): round(avg[s], 2) for s in stage_keys},
+                "algorithmic_bytes_per_launch": bytes_of[dom]}
+    k.close()
+    del k
+
+    # ---- end to end through the public API from host arrays ---------------
+    barrier()
+    t0 = time.perf_counter()
+    k2 = CudaKernel(*sc.kernel_args(), **kw)
+    for _ in range(args.steps):
+        dt = k2.compute_timestep()
+        k2.step(dt)
+        k2.error_metrics()
+    final = k2.particles()
+    torch.cuda.synchronize()
+    e2e_s = max_over_ranks(time.perf_counter() - t0)
+    assert len(final) == n
+    k2.close()
+    h2d_init = n * (13 * 4 + 1) + len(sc.boundary) * 7 * 4
+    d2h_final = n * (13 * 4 + 1)
+    e2e = {"value": n * args.steps * world / e2e_s, "unit": UNIT,
+           "h2d_bytes_per_step": h2d_init / args.steps + 4,
+           "d2h_bytes_per_step": d2h_final / args.steps + 4 + 12 + 4,
+           "includes": "handle creation from host arrays, per step compute_timestep + step + "
+                       "error_metrics, final particles() readback"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        v, done, el = cpu_reference_run(sc, 3, 0, args.cpu_budget, threads)
+        cpu = {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
+               "sample": f"{done} full steps of {args.workload} ({n} particles) on {threads} host threads, "
+                         f"oracle tier G ({el:.1f} s)"}
+
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded dam break, host-built)",
+            "config": {"workload": args.workload, "particles_per_gpu": n, "boundary_particles": len(sc.boundary),
+                       "parallelism": f"replicas{world}", "dt": "device CFL each step",
+                       "l2": f"inputs larger than L2 (state {state_bytes / 1e6:.0f} MB per GPU)",
+                       "alpha": sc.alpha, "cell_order": "morton"},
+            "clocks": clk.summary(), "gpu_launches": launches, "e2e": e2e,
+            "roofline": roofline, "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="cuda", choices=["cuda", "reference"])
+    ap.add_argument("--workload", default="dam_break_1mm_sphere", choices=sorted(WORKLOADS))
+    ap.add_argument("--seed", type=int, default=2024)
+    ap.add_argument("--cpu-budget", type=float, default=25.0)
+    ap.add_argument("--ref-budget", type=float, default=120.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "cuda":
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference_arm(args)
+    else:
+        run_cuda_arm(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,210 @@
+/*
+ * sph_cuda.h - C ABI of the B200 (sm_100a) WCSPH step.
+ *
+ * Drop-in for the reference crate `kernel`'s backend interface
+ * (tim-ai-twin/ultraballpit, backend/crates/kernel/src/lib.rs:58-78):
+ *
+ *   pub trait SimulationKernel {
+ *       fn step(&mut self, dt: f32);
+ *       fn particles(&self) -> &ParticleArrays;
+ *       fn error_metrics(&self) -> ErrorMetrics;
+ *       fn particle_count(&self) -> usize;
+ *       fn save_checkpoint(&mut self) -> bool;
+ *       fn restore_checkpoint(&mut self) -> bool;
+ *   }
+ *
+ * A Rust `CudaKernel` implements that trait over an opaque SphHandle (the
+ * binding is written out in INTEGRATION.md). Every entry point returns an
+ * SphStatus (0 = ok) and never aborts; the handle is Send but not Sync:
+ * calls on one handle must not overlap, and each call makes the handle's
+ * device current, so the handle may move between host threads.
+ *
+ * All arrays are plain host pointers; the library copies inputs to its own
+ * device memory at creation and owns every device allocation, stream and
+ * CUDA graph it uses.
+ */
+#ifndef SPH_CUDA_H
+#define SPH_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SPH_ABI_VERSION 1
+
+typedef struct SphHandle SphHandle;
+
+typedef enum SphStatus {
+  SPH_OK = 0,
+  SPH_ERR_INVALID_ARG = 1,   /* null pointer, size mismatch, bad parameter */
+  SPH_ERR_OOM = 2,           /* device allocation failed */
+  SPH_ERR_CUDA = 3,          /* any other CUDA runtime error */
+  SPH_ERR_NONFINITE = 4,     /* a NaN/Inf state was detected (sph_health) */
+  SPH_ERR_TIMEOUT = 5,       /* a bounded device-side wait gave up */
+  SPH_ERR_CAPACITY = 6,      /* a per-cell / per-boundary-particle bound was exceeded */
+  SPH_ERR_NO_DEVICE = 7,     /* no CUDA device, or not an sm_100 device */
+  SPH_ERR_NO_CHECKPOINT = 8  /* restore without a saved checkpoint */
+} SphStatus;
+
+typedef enum SphBoundaryMode {
+  SPH_BOUNDARY_PARTICLES = 0, /* reference walls: frozen particles, Adami pressure */
+  SPH_BOUNDARY_SDF = 1        /* wall force from a trilinear SDF (no reference counterpart) */
+} SphBoundaryMode;
+
+typedef enum SphCellOrder {
+  SPH_CELL_ORDER_MORTON = 0, /* particles stored by (30-bit Morton cell rank, id) */
+  SPH_CELL_ORDER_LINEAR = 1  /* particles stored by (linear cell hash, id): the reference sorted_indices */
+} SphCellOrder;
+
+/* Stage switches; SPH_FLAGS_REFERENCE keeps every reference stage on
+ * (kernel/src/lib.rs:216-234, 310-324; boundary.rs:143-181, 239-291). */
+typedef enum SphFlags {
+  SPH_FLAG_DELTA_SPH = 1u << 0,
+  SPH_FLAG_XSPH = 1u << 1,
+  SPH_FLAG_REPULSION = 1u << 2,
+  SPH_FLAG_DOMAIN_CLAMP = 1u << 3,
+  SPH_FLAGS_REFERENCE = 0xFu
+} SphFlags;
+
+/* Arguments of CpuKernel::new (kernel/src/lib.rs:138-148) plus the stage
+ * parameters the reference hardcodes (alpha = 1, beta = 2 at sph.rs:440-441). */
+typedef struct SphParams {
+  float h;                /* smoothing length; cell size is 2h */
+  float gravity[3];
+  float speed_of_sound;   /* used as given (no auto-tune, orchestrator lib.rs:157-159) */
+  float cfl_number;
+  float viscosity;        /* kept for the trait's constructor; unused, as in the reference */
+  float domain_min[3];
+  float domain_max[3];
+  float alpha;            /* Monaghan alpha */
+  float beta;             /* Monaghan beta */
+  int32_t boundary_mode;  /* SphBoundaryMode */
+  int32_t cell_order;     /* SphCellOrder */
+  uint32_t flags;         /* SphFlags */
+  int32_t device;         /* CUDA device ordinal */
+  float sdf_wall_coef;    /* SPH_BOUNDARY_SDF: wall repulsion scale (m/s^2) */
+} SphParams;
+
+/* Fluid particles (kernel/src/particle.rs:22-58), host SoA, n entries each. */
+typedef struct SphParticlesView {
+  size_t n;
+  const float *x, *y, *z, *vx, *vy, *vz, *ax, *ay, *az;
+  const float *density, *pressure, *mass, *temperature;
+  const uint8_t *fluid_type; /* 0 = Water, 1 = Air */
+} SphParticlesView;
+
+typedef struct SphParticlesMut {
+  size_t n;
+  float *x, *y, *z, *vx, *vy, *vz, *ax, *ay, *az;
+  float *density, *pressure, *mass, *temperature;
+  uint8_t *fluid_type;
+} SphParticlesMut;
+
+/* Boundary particles (kernel/src/boundary.rs:20-37); pressure starts at 0. */
+typedef struct SphBoundaryView {
+  size_t n;
+  const float *x, *y, *z, *mass, *nx, *ny, *nz;
+} SphBoundaryView;
+
+/* GridSDF (orchestrator/src/geometry.rs:11-20): node (i,j,k) at
+ * origin + (i,j,k) * cell_size, index i*ny*nz + j*nz + k. */
+typedef struct SphSdfView {
+  float origin[3];
+  float cell_size;
+  uint32_t dims[3];
+  const float *distances;
+} SphSdfView;
+
+/* kernel/src/lib.rs:40-47 */
+typedef struct SphErrorMetrics {
+  float max_density_variation;
+  float energy_conservation;
+  float mass_conservation;
+} SphErrorMetrics;
+
+/* Per-stage device time of one step in microseconds (the counterpart of
+ * GpuStepProfile, kernel/src/gpu/mod.rs:35-52). */
+typedef struct SphStepProfile {
+  float xsph_drift_us;        /* kick 1 + XSPH + drift + clamp + binning */
+  float sort_us;              /* scan + fill + reorder */
+  float density_us;           /* density + delta-SPH + EOS */
+  float boundary_pressure_us; /* Adami boundary pressure */
+  float forces_us;            /* pressure + viscosity + gravity + walls + kick 2 + dt reduce */
+  float total_us;
+} SphStepProfile;
+
+typedef struct SphGridInfo {
+  uint32_t dims[3];
+  uint32_t total_cells;
+  float cell_size;
+  float grid_min[3];
+  uint64_t boundary_candidates; /* entries of the static per-cell boundary lists */
+} SphGridInfo;
+
+/* Fill `p` with the reference defaults: alpha 1, beta 2, Morton order, all
+ * reference stages on, boundary particles, device 0. */
+void sph_params_default(SphParams *p);
+
+/* CpuKernel::new / GpuKernel::new (lib.rs:138-174, gpu/mod.rs:190-200).
+ * `boundary` may be NULL (no walls); `sdf` is required for SPH_BOUNDARY_SDF
+ * and ignored otherwise. */
+int sph_create(const SphParams *params, const SphParticlesView *particles,
+               const SphBoundaryView *boundary, const SphSdfView *sdf, SphHandle **out);
+void sph_destroy(SphHandle *h);
+
+/* SimulationKernel::step (lib.rs:287-335). Enqueued asynchronously. */
+int sph_step(SphHandle *h, float dt);
+/* `nsteps` steps whose dt is computed on the device from the state, exactly
+ * as sph::compute_timestep (sph.rs:591-628) would on particles(); the last
+ * dt is written to `dt_out` (may be NULL, no host sync then). */
+int sph_step_auto(SphHandle *h, int nsteps, float *dt_out);
+/* sph::compute_timestep(particles(), h, c, cfl_number) evaluated on the device. */
+int sph_compute_timestep(SphHandle *h, float *dt_out);
+/* One step run stage by stage with CUDA events; fills `prof` (host sync). */
+int sph_step_profiled(SphHandle *h, float dt, SphStepProfile *prof);
+
+/* SimulationKernel::particles: copy the state into caller-owned arrays in the
+ * original particle order (synchronizes). `out->n` must equal the count. */
+int sph_read_particles(SphHandle *h, SphParticlesMut *out);
+/* Boundary pressures of the last force computation (n = boundary count). */
+int sph_read_boundary_pressure(SphHandle *h, float *out, size_t n);
+/* SimulationKernel::error_metrics (lib.rs:341-377): FP64 sums on the device. */
+int sph_error_metrics(SphHandle *h, SphErrorMetrics *out);
+/* SimulationKernel::particle_count */
+size_t sph_particle_count(const SphHandle *h);
+/* SimulationKernel::save_checkpoint / restore_checkpoint (lib.rs:383-395):
+ * device-to-device copies; restore takes the checkpoint (a second restore
+ * returns SPH_ERR_NO_CHECKPOINT). */
+int sph_save_checkpoint(SphHandle *h);
+int sph_restore_checkpoint(SphHandle *h);
+
+/* Wait for queued work; reports a deferred device-side error, if any. */
+int sph_synchronize(SphHandle *h);
+/* Count of particles with a non-finite position, velocity or density. */
+int sph_health(SphHandle *h, uint64_t *nonfinite_out);
+const char *sph_last_error(const SphHandle *h);
+/* The cudaStream_t all work of the handle is enqueued on. */
+void *sph_stream(SphHandle *h);
+/* Total kernels this handle has launched (graph replays counted per node). */
+uint64_t sph_launch_count(const SphHandle *h);
+
+/* ---- grid diagnostics (the bit-exact grid/sort checks) ---------------- */
+int sph_grid_info(SphHandle *h, SphGridInfo *out);
+/* Grid of the last force computation. Per particle, in original order:
+ * linear cell hash (neighbor.rs:75-77) and 30-bit Morton key of (cx,cy,cz).
+ * Per linear cell: count and storage start. Per storage slot: original id.
+ * Any pointer may be NULL. */
+int sph_read_grid(SphHandle *h, uint32_t *cell_linear, uint32_t *morton_key,
+                  uint32_t *cell_count, uint32_t *cell_start, uint32_t *slot_id);
+/* Neighbour list of particle `id` (original index) in the reference visit
+ * order (neighbor.rs:129-182) on the current grid; `*count` gets the full
+ * length, at most `cap` ids are written. */
+int sph_neighbors(SphHandle *h, uint32_t id, uint32_t *out, size_t cap, size_t *count);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SPH_CUDA_H */

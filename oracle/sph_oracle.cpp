@@ -1,0 +1,887 @@
+// CPU oracle for the WCSPH step: a restatement of the reference Rust CPU path
+// (tim-ai-twin/ultraballpit, crate `kernel`).
+//
+// TEST INFRASTRUCTURE ONLY. The product (libsph_cuda.so) never links, loads or
+// calls this file. It is used by tests/, by __graft_entry__.smoke() and by the
+// cpu_baseline / reference legs of bench.py, and only as the checker or as the
+// timed CPU baseline.
+//
+// Parity pin: the Rust reference cannot be compiled in this image (no cargo or
+// rustc), so this restatement is pinned against the reference's own
+// known-answer tests (sph.rs:634-722, eos.rs:70-94, neighbor.rs:185-269,
+// tests/two_particle.rs, tests/kernel_normalization.rs, tests/hydrostatic.rs,
+// orchestrator geometry.rs:188-250). tests/test_oracle_kat.py runs them.
+//
+// Build: -O2 -ffp-contract=off -fno-fast-math (no FMA contraction, IEEE f32
+// arithmetic in source order, like rustc which never contracts a*b+c).
+//
+// Two tiers share every formula:
+//   Tier L (literal): the boundary loops are the reference's O(N*N_b) scans.
+//   Tier G (grid): the same sums, visiting boundary candidates in ascending
+//     boundary index through static per-cell candidate lists, and the Adami
+//     fluid candidates through the fluid grid sorted by fluid index. Each
+//     candidate set is a provable superset of the in-support set, so the
+//     sums are identical to Tier L term for term.
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+#include <atomic>
+#include <thread>
+
+namespace {
+
+// Dynamic-schedule parallel loop over [0, n) on `threads` std::threads. Each
+// index is processed by exactly one thread with the same arithmetic as a
+// serial loop, so results do not depend on the thread count.
+template <class F>
+void parallel_for(size_t n, int threads, size_t chunk, F&& body) {
+  if (threads <= 1 || n <= chunk) {
+    for (size_t i = 0; i < n; ++i) body(i);
+    return;
+  }
+  std::atomic<size_t> next(0);
+  auto worker = [&]() {
+    for (;;) {
+      size_t s = next.fetch_add(chunk);
+      if (s >= n) break;
+      size_t e = std::min(n, s + chunk);
+      for (size_t i = s; i < e; ++i) body(i);
+    }
+  };
+  std::vector<std::thread> pool;
+  for (int t = 1; t < threads; ++t) pool.emplace_back(worker);
+  worker();
+  for (auto& t : pool) t.join();
+}
+
+// std::f32::consts::PI
+constexpr float kPi = 3.14159265358979323846f;
+// sph.rs:20  WENDLAND_C2_NORM_3D = 21 / (16 pi), evaluated in f32.
+const float kNorm = 21.0f / (16.0f * kPi);
+// sph.rs:93  DELTA_SPH; sph.rs:224 XSPH_EPSILON
+constexpr float kDeltaSph = 0.1f;
+constexpr float kXsphEps = 0.5f;
+// eos.rs:7-22
+constexpr float kWaterRho0 = 1000.0f;
+constexpr float kAirRho0 = 1.204f;
+constexpr float kWaterGamma = 7.0f;
+constexpr float kAirGamma = 1.4f;
+// sph.rs:579-581
+constexpr float kMinDt = 1.0e-8f;
+constexpr float kMaxDt = 0.01f;
+
+// sph.rs:35-46
+inline float wendland_c2(float r, float h) {
+  float q = r / h;
+  if (q >= 2.0f) return 0.0f;
+  float h3 = h * h * h;
+  float omq = 1.0f - 0.5f * q;
+  float t = omq * omq;
+  float t4 = t * t;
+  return kNorm / h3 * t4 * (1.0f + 2.0f * q);
+}
+
+// sph.rs:68-85
+inline void wendland_c2_gradient(float dx, float dy, float dz, float r, float h,
+                                 float* gx, float* gy, float* gz) {
+  float q = r / h;
+  if (q >= 2.0f || r < 1.0e-12f) {
+    *gx = 0.0f; *gy = 0.0f; *gz = 0.0f;
+    return;
+  }
+  float h3 = h * h * h;
+  float omq = 1.0f - 0.5f * q;
+  float t3 = omq * omq * omq;
+  float dw_dr = kNorm / (h3 * h) * (-5.0f * q) * t3;
+  float inv_r = 1.0f / r;
+  *gx = dw_dr * dx * inv_r;
+  *gy = dw_dr * dy * inv_r;
+  *gz = dw_dr * dz * inv_r;
+}
+
+// Power used by the Tait EOS. pow_mode 0 calls the platform libm powf, which
+// is what f32::powf lowers to on Linux (glibc; not correctly rounded in about
+// 0.07% of inputs near 1). pow_mode 1 returns the correctly rounded x^gamma:
+// for gamma = 7 a double-precision product (exact to well inside half an f32
+// ulp, checked exhaustively against long double on [0.5, 2]), otherwise the
+// double pow rounded to f32. The CUDA step implements pow_mode 1.
+inline float eos_pow(float x, float gamma, int pow_mode) {
+  if (pow_mode == 0) return powf(x, gamma);
+  if (gamma == 7.0f) {
+    double r = x, r2 = r * r, r4 = r2 * r2, r6 = r4 * r2;
+    return (float)(r6 * r);
+  }
+  return (float)pow((double)x, (double)gamma);
+}
+
+// eos.rs:39-47
+inline float tait_eos(float density, float rest_density, float c, float gamma, int pow_mode = 0) {
+  float b = rest_density * c * c / gamma;
+  float ratio = density / rest_density;
+  float p = b * (eos_pow(ratio, gamma, pow_mode) - 1.0f);
+  return fmaxf(p, 0.0f);
+}
+
+struct Particles {  // particle.rs:22-58 (SoA)
+  std::vector<float> x, y, z, vx, vy, vz, ax, ay, az, density, pressure, mass,
+      temperature;
+  std::vector<uint8_t> fluid_type;  // 0 = Water, 1 = Air
+  size_t len() const { return x.size(); }
+  std::vector<float>* field(int k) {
+    std::vector<float>* f[13] = {&x, &y, &z, &vx, &vy, &vz, &ax, &ay, &az,
+                                 &density, &pressure, &mass, &temperature};
+    return f[k];
+  }
+};
+
+// neighbor.rs:11-183
+struct NeighborGrid {
+  float cell_size;
+  float grid_min[3];
+  uint32_t dims[3];
+  std::vector<uint32_t> cell_indices, sorted_indices, cell_offsets, cell_counts;
+
+  NeighborGrid() = default;
+  // neighbor.rs:29-46
+  NeighborGrid(float cs, const float mn[3], const float mx[3]) : cell_size(cs) {
+    for (int k = 0; k < 3; ++k) {
+      grid_min[k] = mn[k];
+      dims[k] = (uint32_t)fmaxf(ceilf((mx[k] - mn[k]) / cs), 1.0f);
+    }
+    cell_offsets.assign(total_cells(), 0);
+    cell_counts.assign(total_cells(), 0);
+  }
+  size_t total_cells() const { return (size_t)dims[0] * dims[1] * dims[2]; }
+  // neighbor.rs:57-71
+  inline uint32_t axis_cell(float p, int k) const {
+    float f = floorf((p - grid_min[k]) / cell_size);
+    f = fmaxf(f, 0.0f);
+    f = fminf(f, (float)(dims[k] - 1));
+    return (uint32_t)f;
+  }
+  inline void pos_to_cell(float px, float py, float pz, uint32_t* cx, uint32_t* cy,
+                          uint32_t* cz) const {
+    *cx = axis_cell(px, 0);
+    *cy = axis_cell(py, 1);
+    *cz = axis_cell(pz, 2);
+  }
+  // neighbor.rs:75-77
+  inline uint32_t cell_hash(uint32_t cx, uint32_t cy, uint32_t cz) const {
+    return cx + cy * dims[0] + cz * dims[0] * dims[1];
+  }
+  // neighbor.rs:82-122: keys, count, exclusive scan, stable scatter.
+  void update(const float* x, const float* y, const float* z, size_t n) {
+    size_t tc = total_cells();
+    cell_indices.assign(n, 0);
+    for (size_t i = 0; i < n; ++i) {
+      uint32_t cx, cy, cz;
+      pos_to_cell(x[i], y[i], z[i], &cx, &cy, &cz);
+      cell_indices[i] = cell_hash(cx, cy, cz);
+    }
+    cell_counts.assign(tc, 0);
+    for (size_t i = 0; i < n; ++i) cell_counts[cell_indices[i]] += 1;
+    cell_offsets.assign(tc, 0);
+    uint32_t running = 0;
+    for (size_t c = 0; c < tc; ++c) {
+      cell_offsets[c] = running;
+      running += cell_counts[c];
+    }
+    sorted_indices.assign(n, 0);
+    std::vector<uint32_t> heads(cell_offsets);
+    for (size_t i = 0; i < n; ++i) {
+      uint32_t ci = cell_indices[i];
+      sorted_indices[heads[ci]] = (uint32_t)i;
+      heads[ci] += 1;
+    }
+  }
+  // neighbor.rs:129-182: 27 cells, dz -> dy -> dx, skip self, dist_sq <= r^2.
+  template <class F>
+  inline void for_each_neighbor(size_t pi, const float* x, const float* y,
+                                const float* z, float radius, F&& f) const {
+    float px = x[pi], py = y[pi], pz = z[pi];
+    uint32_t cx, cy, cz;
+    pos_to_cell(px, py, pz, &cx, &cy, &cz);
+    float radius_sq = radius * radius;
+    for (int dz = -1; dz <= 1; ++dz) {
+      int nz = (int)cz + dz;
+      if (nz < 0 || nz >= (int)dims[2]) continue;
+      for (int dy = -1; dy <= 1; ++dy) {
+        int ny = (int)cy + dy;
+        if (ny < 0 || ny >= (int)dims[1]) continue;
+        for (int dx = -1; dx <= 1; ++dx) {
+          int nx = (int)cx + dx;
+          if (nx < 0 || nx >= (int)dims[0]) continue;
+          uint32_t cell = cell_hash((uint32_t)nx, (uint32_t)ny, (uint32_t)nz);
+          uint32_t start = cell_offsets[cell], count = cell_counts[cell];
+          for (uint32_t s = start; s < start + count; ++s) {
+            uint32_t j = sorted_indices[s];
+            if (j == pi) continue;
+            float ddx = px - x[j], ddy = py - y[j], ddz = pz - z[j];
+            float dist_sq = ddx * ddx + ddy * ddy + ddz * ddz;
+            if (dist_sq <= radius_sq) f((size_t)j);
+          }
+        }
+      }
+    }
+  }
+};
+
+struct Boundary {  // boundary.rs:20-37
+  std::vector<float> x, y, z, mass, nx, ny, nz, pressure;
+  size_t len() const { return x.size(); }
+};
+
+// Morton interleave of three 10-bit cell coordinates (x in bit 0).
+inline uint32_t spread10(uint32_t v) {
+  v &= 0x3ffu;
+  v = (v | (v << 16)) & 0x030000ffu;
+  v = (v | (v << 8)) & 0x0300f00fu;
+  v = (v | (v << 4)) & 0x030c30c3u;
+  v = (v | (v << 2)) & 0x09249249u;
+  return v;
+}
+inline uint32_t morton30(uint32_t cx, uint32_t cy, uint32_t cz) {
+  return spread10(cx) | (spread10(cy) << 1) | (spread10(cz) << 2);
+}
+
+struct OrcParams {
+  float h;
+  float gravity[3];
+  float speed_of_sound;
+  float cfl_number;
+  float viscosity;
+  float domain_min[3];
+  float domain_max[3];
+  float alpha;  // sph.rs:440 hardcodes 1.0
+  float beta;   // sph.rs:441 hardcodes 2.0
+  int tier;      // 0 = literal, 1 = grid
+  int threads;   // worker threads for Tier G loops (results do not depend on it)
+  int pow_mode;  // 0 = libm powf (reference on Linux), 1 = correctly rounded
+};
+
+class Kernel {
+ public:
+  Particles p;
+  Boundary b;
+  NeighborGrid grid;
+  OrcParams prm;
+  double initial_energy = 0.0, initial_mass = 0.0;
+  bool needs_init = true;
+  bool has_checkpoint = false;
+  Particles checkpoint;
+  // Tier G: static boundary candidate lists per fluid cell (ascending b).
+  std::vector<uint32_t> bc_start, bc_list;
+
+  // lib.rs:138-174
+  Kernel(const OrcParams& pr, Particles&& parts, Boundary&& bnd)
+      : p(std::move(parts)), b(std::move(bnd)), prm(pr) {
+    grid = NeighborGrid(2.0f * prm.h, prm.domain_min, prm.domain_max);
+    double m = 0.0;
+    for (size_t i = 0; i < p.len(); ++i) m += (double)p.mass[i];
+    initial_mass = m;
+    initial_energy = total_energy();
+    if (prm.tier == 1) build_boundary_lists();
+  }
+
+  // lib.rs:177-194
+  double total_energy() const {
+    double e = 0.0;
+    const float* g = prm.gravity;
+    for (size_t i = 0; i < p.len(); ++i) {
+      double m = (double)p.mass[i];
+      double vx = p.vx[i], vy = p.vy[i], vz = p.vz[i];
+      e += 0.5 * m * (vx * vx + vy * vy + vz * vz);
+      double x = p.x[i], y = p.y[i], z = p.z[i];
+      e -= m * ((double)g[0] * x + (double)g[1] * y + (double)g[2] * z);
+    }
+    return e;
+  }
+
+  // Tier G: a boundary particle b is a candidate of fluid cell c when its
+  // distance to the cell's box, widened by a relative margin that exceeds
+  // the rounding of pos_to_cell and unbounded outward on clamped edge cells,
+  // is below 2h (with margin). Lists are in ascending b.
+  void build_boundary_lists() {
+    size_t tc = grid.total_cells();
+    double cs = grid.cell_size, margin = 1e-4 * cs;
+    double reach = 2.0 * (double)prm.h * (1.0 + 1e-4) + margin;
+    std::vector<std::vector<uint32_t>> per(tc);
+    for (size_t bi = 0; bi < b.len(); ++bi) {
+      double pos[3] = {b.x[bi], b.y[bi], b.z[bi]};
+      int lo[3], hi[3];
+      for (int k = 0; k < 3; ++k) {
+        double u0 = (pos[k] - reach - grid.grid_min[k]) / cs;
+        double u1 = (pos[k] + reach - grid.grid_min[k]) / cs;
+        lo[k] = (int)std::max(0.0, std::min((double)grid.dims[k] - 1, std::floor(u0)));
+        hi[k] = (int)std::max(0.0, std::min((double)grid.dims[k] - 1, std::floor(u1)));
+      }
+      for (int cz = lo[2]; cz <= hi[2]; ++cz)
+        for (int cy = lo[1]; cy <= hi[1]; ++cy)
+          for (int cx = lo[0]; cx <= hi[0]; ++cx) {
+            int c3[3] = {cx, cy, cz};
+            double d2 = 0.0;
+            for (int k = 0; k < 3; ++k) {
+              double blo = (c3[k] == 0) ? -1e300 : grid.grid_min[k] + c3[k] * cs - margin;
+              double bhi = (c3[k] == (int)grid.dims[k] - 1) ? 1e300
+                                                            : grid.grid_min[k] + (c3[k] + 1) * cs + margin;
+              double d = 0.0;
+              if (pos[k] < blo) d = blo - pos[k];
+              else if (pos[k] > bhi) d = pos[k] - bhi;
+              d2 += d * d;
+            }
+            if (d2 < reach * reach)
+              per[grid.cell_hash(cx, cy, cz)].push_back((uint32_t)bi);
+          }
+    }
+    bc_start.assign(tc + 1, 0);
+    for (size_t c = 0; c < tc; ++c) bc_start[c + 1] = bc_start[c] + (uint32_t)per[c].size();
+    bc_list.resize(bc_start[tc]);
+    for (size_t c = 0; c < tc; ++c)
+      std::copy(per[c].begin(), per[c].end(), bc_list.begin() + bc_start[c]);
+  }
+
+  // Visit boundary particles that may lie in support of fluid particle i, in
+  // ascending boundary index (Tier L: all of them).
+  template <class F>
+  inline void for_each_boundary(size_t i, F&& f) const {
+    if (prm.tier == 0) {
+      for (size_t bi = 0; bi < b.len(); ++bi) f(bi);
+    } else {
+      uint32_t cx, cy, cz;
+      grid.pos_to_cell(p.x[i], p.y[i], p.z[i], &cx, &cy, &cz);
+      uint32_t c = grid.cell_hash(cx, cy, cz);
+      for (uint32_t s = bc_start[c]; s < bc_start[c + 1]; ++s) f((size_t)bc_list[s]);
+    }
+  }
+
+  int nthreads() const { return prm.tier == 1 ? std::max(1, prm.threads) : 1; }
+
+  // sph.rs:169-216
+  std::vector<float> density_diffusion() const {
+    size_t n = p.len();
+    float h = prm.h, c = prm.speed_of_sound;
+    float support = 2.0f * h;
+    float eta_sq = 0.01f * h * h;
+    std::vector<float> diffusion(n, 0.0f);
+    parallel_for(n, nthreads(), 256, [&](size_t i) {
+      float diff_sum = 0.0f;
+      grid.for_each_neighbor(i, p.x.data(), p.y.data(), p.z.data(), support, [&](size_t j) {
+        float dx = p.x[i] - p.x[j], dy = p.y[i] - p.y[j], dz = p.z[i] - p.z[j];
+        float dist_sq = dx * dx + dy * dy + dz * dz;
+        float r = sqrtf(dist_sq);
+        float gx, gy, gz;
+        wendland_c2_gradient(dx, dy, dz, r, h, &gx, &gy, &gz);
+        float v_j = p.mass[j] / p.density[j];
+        float r_dot_grad = dx * gx + dy * gy + dz * gz;
+        float density_diff = p.density[i] - p.density[j];
+        diff_sum += v_j * density_diff * 2.0f * r_dot_grad / (dist_sq + eta_sq);
+      });
+      diffusion[i] = kDeltaSph * h * c * diff_sum;
+    });
+    return diffusion;
+  }
+
+  // sph.rs:112-160
+  void compute_density() {
+    size_t n = p.len();
+    float h = prm.h;
+    float support = 2.0f * h;
+    std::vector<float> out(n);
+    parallel_for(n, nthreads(), 256, [&](size_t i) {
+      float rho = p.mass[i] * wendland_c2(0.0f, h);
+      grid.for_each_neighbor(i, p.x.data(), p.y.data(), p.z.data(), support, [&](size_t j) {
+        float dx = p.x[i] - p.x[j], dy = p.y[i] - p.y[j], dz = p.z[i] - p.z[j];
+        float r = sqrtf(dx * dx + dy * dy + dz * dz);
+        rho += p.mass[j] * wendland_c2(r, h);
+      });
+      float px = p.x[i], py = p.y[i], pz = p.z[i];
+      for_each_boundary(i, [&](size_t bi) {
+        float dx = px - b.x[bi], dy = py - b.y[bi], dz = pz - b.z[bi];
+        float r = sqrtf(dx * dx + dy * dy + dz * dz);
+        if (r < support) rho += b.mass[bi] * wendland_c2(r, h);
+      });
+      out[i] = rho;
+    });
+    p.density.swap(out);
+  }
+
+  // sph.rs:295-312
+  void compute_pressure() {
+    float c = prm.speed_of_sound;
+    for (size_t i = 0; i < p.len(); ++i)
+      p.pressure[i] = p.fluid_type[i] == 0
+                          ? tait_eos(p.density[i], kWaterRho0, c, kWaterGamma, prm.pow_mode)
+                          : tait_eos(p.density[i], kAirRho0, c, kAirGamma, prm.pow_mode);
+  }
+
+  // boundary.rs:87-131 (Tier L: fluid index order 0..n; Tier G: the fluid
+  // candidates of a widened cell range, sorted by fluid index, then summed).
+  void update_boundary_pressures() {
+    float h = prm.h, support = 2.0f * h;
+    const float* g = prm.gravity;
+    size_t nf = p.len();
+    parallel_for(b.len(), nthreads(), 64, [&](size_t bi) {
+      float bx = b.x[bi], by = b.y[bi], bz = b.z[bi];
+      float weighted_pressure = 0.0f, weight_sum = 0.0f;
+      auto term = [&](size_t f) {
+        float dx = bx - p.x[f], dy = by - p.y[f], dz = bz - p.z[f];
+        float r = sqrtf(dx * dx + dy * dy + dz * dz);
+        if (r < support) {
+          float w = wendland_c2(r, h);
+          float g_dot_dr = g[0] * dx + g[1] * dy + g[2] * dz;
+          float p_ext = p.pressure[f] + p.density[f] * g_dot_dr;
+          weighted_pressure += w * p_ext;
+          weight_sum += w;
+        }
+      };
+      if (prm.tier == 0) {
+        for (size_t f = 0; f < nf; ++f) term(f);
+      } else {
+        std::vector<uint32_t> cand;
+        double cs = grid.cell_size;
+        double reach = 2.0 * (double)h * (1.0 + 1e-4) + 1e-4 * cs;
+        double pos[3] = {bx, by, bz};
+        int lo[3], hi[3];
+        for (int k = 0; k < 3; ++k) {
+          lo[k] = (int)grid.axis_cell((float)(pos[k] - reach), k);
+          hi[k] = (int)grid.axis_cell((float)(pos[k] + reach), k);
+        }
+        for (int cz = lo[2]; cz <= hi[2]; ++cz)
+          for (int cy = lo[1]; cy <= hi[1]; ++cy)
+            for (int cx = lo[0]; cx <= hi[0]; ++cx) {
+              uint32_t c = grid.cell_hash(cx, cy, cz);
+              for (uint32_t s = grid.cell_offsets[c]; s < grid.cell_offsets[c] + grid.cell_counts[c]; ++s)
+                cand.push_back(grid.sorted_indices[s]);
+            }
+        std::sort(cand.begin(), cand.end());
+        for (uint32_t f : cand) term(f);
+      }
+      if (weight_sum > 1.0e-12f) b.pressure[bi] = fmaxf(weighted_pressure / weight_sum, 0.0f);
+      else b.pressure[bi] = 0.0f;
+    });
+  }
+
+  // sph.rs:322-417
+  void compute_pressure_forces() {
+    size_t n = p.len();
+    float h = prm.h, support = 2.0f * h;
+    std::vector<float> fx(n, 0.0f), fy(n, 0.0f), fz(n, 0.0f);
+    parallel_for(n, nthreads(), 256, [&](size_t i) {
+      float pi_over_rho2_i = p.pressure[i] / (p.density[i] * p.density[i]);
+      grid.for_each_neighbor(i, p.x.data(), p.y.data(), p.z.data(), support, [&](size_t j) {
+        float dx = p.x[i] - p.x[j], dy = p.y[i] - p.y[j], dz = p.z[i] - p.z[j];
+        float r = sqrtf(dx * dx + dy * dy + dz * dz);
+        float gx, gy, gz;
+        wendland_c2_gradient(dx, dy, dz, r, h, &gx, &gy, &gz);
+        float pj_over_rho2_j = p.pressure[j] / (p.density[j] * p.density[j]);
+        float factor = -p.mass[i] * p.mass[j] * (pi_over_rho2_i + pj_over_rho2_j);
+        fx[i] += factor * gx;
+        fy[i] += factor * gy;
+        fz[i] += factor * gz;
+      });
+      float px = p.x[i], py = p.y[i], pz = p.z[i];
+      float m_i = p.mass[i];
+      float pi_clamped = fmaxf(p.pressure[i], 0.0f);
+      float pi_clamped_over_rho2 = pi_clamped / (p.density[i] * p.density[i]);
+      float boundary_rho = p.fluid_type[i] == 0 ? kWaterRho0 : kAirRho0;
+      for_each_boundary(i, [&](size_t bi) {
+        float dx = px - b.x[bi], dy = py - b.y[bi], dz = pz - b.z[bi];
+        float r = sqrtf(dx * dx + dy * dy + dz * dz);
+        if (r < support) {
+          float gx, gy, gz;
+          wendland_c2_gradient(dx, dy, dz, r, h, &gx, &gy, &gz);
+          float pb_over_rho2_b = b.pressure[bi] / (boundary_rho * boundary_rho);
+          float factor = -m_i * b.mass[bi] * (pi_clamped_over_rho2 + pb_over_rho2_b);
+          fx[i] += factor * gx;
+          fy[i] += factor * gy;
+          fz[i] += factor * gz;
+        }
+      });
+    });
+    for (size_t i = 0; i < n; ++i) {
+      p.ax[i] += fx[i] / p.mass[i];
+      p.ay[i] += fy[i] / p.mass[i];
+      p.az[i] += fz[i] / p.mass[i];
+    }
+  }
+
+  // sph.rs:432-492 (alpha, beta are parameters; the reference hardcodes 1, 2)
+  void compute_viscous_forces() {
+    size_t n = p.len();
+    float h = prm.h, support = 2.0f * h, c = prm.speed_of_sound;
+    float alpha = prm.alpha, beta = prm.beta;
+    float eta_sq = 0.01f * h * h;
+    std::vector<float> fx(n, 0.0f), fy(n, 0.0f), fz(n, 0.0f);
+    parallel_for(n, nthreads(), 256, [&](size_t i) {
+      grid.for_each_neighbor(i, p.x.data(), p.y.data(), p.z.data(), support, [&](size_t j) {
+        float dx = p.x[i] - p.x[j], dy = p.y[i] - p.y[j], dz = p.z[i] - p.z[j];
+        float r = sqrtf(dx * dx + dy * dy + dz * dz);
+        float dvx = p.vx[i] - p.vx[j], dvy = p.vy[i] - p.vy[j], dvz = p.vz[i] - p.vz[j];
+        float vr_dot = dvx * dx + dvy * dy + dvz * dz;
+        if (vr_dot < 0.0f) {
+          float r_sq = r * r;
+          float mu_ij = h * vr_dot / (r_sq + eta_sq);
+          float rho_avg = 0.5f * (p.density[i] + p.density[j]);
+          float pi_ij = (-alpha * c * mu_ij + beta * mu_ij * mu_ij) / rho_avg;
+          float gx, gy, gz;
+          wendland_c2_gradient(dx, dy, dz, r, h, &gx, &gy, &gz);
+          float factor = -p.mass[j] * pi_ij;
+          fx[i] += factor * gx;
+          fy[i] += factor * gy;
+          fz[i] += factor * gz;
+        }
+      });
+    });
+    for (size_t i = 0; i < n; ++i) {
+      p.ax[i] += fx[i];
+      p.ay[i] += fy[i];
+      p.az[i] += fz[i];
+    }
+  }
+
+  // boundary.rs:143-181
+  void compute_repulsive_forces() {
+    float h = prm.h;
+    float r0 = 0.5f * h;
+    float d = 10.0f * 9.81f * 0.01f;
+    parallel_for(p.len(), nthreads(), 256, [&](size_t i) {
+      float px = p.x[i], py = p.y[i], pz = p.z[i];
+      for_each_boundary(i, [&](size_t bi) {
+        float dx = px - b.x[bi], dy = py - b.y[bi], dz = pz - b.z[bi];
+        float r = sqrtf(dx * dx + dy * dy + dz * dz);
+        if (r < r0 && r > 1.0e-12f) {
+          float s = 1.0f - r / r0;
+          float force_mag = d * s * s / r0;
+          float inv_r = 1.0f / r;
+          p.ax[i] += force_mag * dx * inv_r;
+          p.ay[i] += force_mag * dy * inv_r;
+          p.az[i] += force_mag * dz * inv_r;
+        }
+      });
+    });
+  }
+
+  // lib.rs:203-283
+  void compute_forces(float dt) {
+    size_t n = p.len();
+    grid.update(p.x.data(), p.y.data(), p.z.data(), n);
+    std::vector<float> diffusion = density_diffusion();
+    compute_density();
+    for (size_t i = 0; i < n; ++i) p.density[i] += diffusion[i] * dt;
+    compute_pressure();
+    update_boundary_pressures();
+    for (size_t i = 0; i < n; ++i) { p.ax[i] = 0.0f; p.ay[i] = 0.0f; p.az[i] = 0.0f; }
+    compute_pressure_forces();
+    compute_viscous_forces();
+    for (size_t i = 0; i < n; ++i) {  // sph.rs:502-508
+      p.ax[i] += prm.gravity[0];
+      p.ay[i] += prm.gravity[1];
+      p.az[i] += prm.gravity[2];
+    }
+    compute_repulsive_forces();
+  }
+
+  // sph.rs:236-280
+  void xsph(std::vector<float>& dvx, std::vector<float>& dvy, std::vector<float>& dvz) const {
+    size_t n = p.len();
+    float h = prm.h, support = 2.0f * h;
+    dvx.assign(n, 0.0f); dvy.assign(n, 0.0f); dvz.assign(n, 0.0f);
+    parallel_for(n, nthreads(), 256, [&](size_t i) {
+      float cx = 0.0f, cy = 0.0f, cz = 0.0f;
+      grid.for_each_neighbor(i, p.x.data(), p.y.data(), p.z.data(), support, [&](size_t j) {
+        float dx = p.x[i] - p.x[j], dy = p.y[i] - p.y[j], dz = p.z[i] - p.z[j];
+        float r = sqrtf(dx * dx + dy * dy + dz * dz);
+        float w = wendland_c2(r, h);
+        float rho_avg = 0.5f * (p.density[i] + p.density[j]);
+        float factor = p.mass[j] / fmaxf(rho_avg, 1.0f) * w;
+        cx += factor * (p.vx[j] - p.vx[i]);
+        cy += factor * (p.vy[j] - p.vy[i]);
+        cz += factor * (p.vz[j] - p.vz[i]);
+      });
+      dvx[i] = kXsphEps * cx;
+      dvy[i] = kXsphEps * cy;
+      dvz[i] = kXsphEps * cz;
+    });
+  }
+
+  // boundary.rs:239-291
+  void enforce_no_penetration_domain() {
+    const float restitution = 0.2f;
+    const float* mn = prm.domain_min;
+    const float* mx = prm.domain_max;
+    for (size_t i = 0; i < p.len(); ++i) {
+      if (p.x[i] < mn[0]) { p.x[i] = mn[0]; if (p.vx[i] < 0.0f) p.vx[i] = -restitution * p.vx[i]; }
+      if (p.x[i] > mx[0]) { p.x[i] = mx[0]; if (p.vx[i] > 0.0f) p.vx[i] = -restitution * p.vx[i]; }
+      if (p.y[i] < mn[1]) { p.y[i] = mn[1]; if (p.vy[i] < 0.0f) p.vy[i] = -restitution * p.vy[i]; }
+      if (p.y[i] > mx[1]) { p.y[i] = mx[1]; if (p.vy[i] > 0.0f) p.vy[i] = -restitution * p.vy[i]; }
+      if (p.z[i] < mn[2]) { p.z[i] = mn[2]; if (p.vz[i] < 0.0f) p.vz[i] = -restitution * p.vz[i]; }
+      if (p.z[i] > mx[2]) { p.z[i] = mx[2]; if (p.vz[i] > 0.0f) p.vz[i] = -restitution * p.vz[i]; }
+    }
+  }
+
+  // lib.rs:287-335
+  void step(float dt) {
+    size_t n = p.len();
+    float half_dt = 0.5f * dt;
+    if (needs_init) {
+      compute_forces(dt);
+      needs_init = false;
+    }
+    for (size_t i = 0; i < n; ++i) {
+      p.vx[i] += p.ax[i] * half_dt;
+      p.vy[i] += p.ay[i] * half_dt;
+      p.vz[i] += p.az[i] * half_dt;
+    }
+    std::vector<float> dvx, dvy, dvz;
+    xsph(dvx, dvy, dvz);
+    for (size_t i = 0; i < n; ++i) {
+      p.x[i] += (p.vx[i] + dvx[i]) * dt;
+      p.y[i] += (p.vy[i] + dvy[i]) * dt;
+      p.z[i] += (p.vz[i] + dvz[i]) * dt;
+    }
+    enforce_no_penetration_domain();
+    compute_forces(dt);
+    for (size_t i = 0; i < n; ++i) {
+      p.vx[i] += p.ax[i] * half_dt;
+      p.vy[i] += p.ay[i] * half_dt;
+      p.vz[i] += p.az[i] * half_dt;
+    }
+  }
+
+  // lib.rs:341-377
+  void error_metrics(float out[3]) const {
+    float max_var = 0.0f;
+    for (size_t i = 0; i < p.len(); ++i) {
+      float rest = p.fluid_type[i] == 0 ? kWaterRho0 : kAirRho0;
+      float var = fabsf(p.density[i] - rest) / rest;
+      if (var > max_var) max_var = var;
+    }
+    double e = total_energy();
+    float ed = fabs(initial_energy) > 1.0e-12 ? (float)fabs((e - initial_energy) / initial_energy)
+                                               : (float)fabs(e - initial_energy);
+    double m = 0.0;
+    for (size_t i = 0; i < p.len(); ++i) m += (double)p.mass[i];
+    float md = fabs(initial_mass) > 1.0e-12 ? (float)fabs((m - initial_mass) / initial_mass)
+                                             : (float)fabs(m - initial_mass);
+    out[0] = max_var; out[1] = ed; out[2] = md;
+  }
+};
+
+// sph.rs:591-628
+float compute_timestep(const Particles& p, float h, float c, float cfl) {
+  float max_signal = c, max_accel = 0.0f;
+  for (size_t i = 0; i < p.len(); ++i) {
+    float v = sqrtf(p.vx[i] * p.vx[i] + p.vy[i] * p.vy[i] + p.vz[i] * p.vz[i]);
+    float signal = v + c;
+    if (signal > max_signal) max_signal = signal;
+    float a = sqrtf(p.ax[i] * p.ax[i] + p.ay[i] * p.ay[i] + p.az[i] * p.az[i]);
+    if (a > max_accel) max_accel = a;
+  }
+  float dt_cfl = cfl * h / max_signal;
+  float dt_force = max_accel > 1.0e-12f ? 0.25f * sqrtf(h / max_accel) : kMaxDt;
+  float dt = fminf(dt_cfl, dt_force);
+  return fminf(fmaxf(dt, kMinDt), kMaxDt);
+}
+
+Particles make_particles(size_t n, float* const* fields, const uint8_t* ft) {
+  Particles p;
+  for (int k = 0; k < 13; ++k) p.field(k)->assign(fields[k], fields[k] + n);
+  p.fluid_type.assign(ft, ft + n);
+  return p;
+}
+
+// orchestrator geometry.rs:178-181
+inline float sdf_get(const float* d, const uint32_t dims[3], uint32_t i, uint32_t j, uint32_t k) {
+  uint64_t idx = (uint64_t)(i * dims[1] * dims[2] + j * dims[2] + k);
+  uint64_t total = (uint64_t)dims[0] * dims[1] * dims[2];
+  return idx < total ? d[idx] : 3.40282347e38f;
+}
+
+// orchestrator geometry.rs:99-150
+float sdf_sample(const float* d, const uint32_t dims[3], const float origin[3], float cell,
+                 const float pt[3]) {
+  float gx = (pt[0] - origin[0]) / cell;
+  float gy = (pt[1] - origin[1]) / cell;
+  float gz = (pt[2] - origin[2]) / cell;
+  int i0 = (int)floorf(gx), j0 = (int)floorf(gy), k0 = (int)floorf(gz);
+  const float FMAX = 3.40282347e38f;
+  if (i0 < 0 || j0 < 0 || k0 < 0) return FMAX;
+  int i1 = i0 + 1, j1 = j0 + 1, k1 = k0 + 1;
+  if (i1 >= (int)dims[0] || j1 >= (int)dims[1] || k1 >= (int)dims[2]) return FMAX;
+  float fx = gx - (float)i0, fy = gy - (float)j0, fz = gz - (float)k0;
+  float c000 = sdf_get(d, dims, i0, j0, k0), c001 = sdf_get(d, dims, i0, j0, k1);
+  float c010 = sdf_get(d, dims, i0, j1, k0), c011 = sdf_get(d, dims, i0, j1, k1);
+  float c100 = sdf_get(d, dims, i1, j0, k0), c101 = sdf_get(d, dims, i1, j0, k1);
+  float c110 = sdf_get(d, dims, i1, j1, k0), c111 = sdf_get(d, dims, i1, j1, k1);
+  float c00 = c000 * (1.0f - fz) + c001 * fz;
+  float c01 = c010 * (1.0f - fz) + c011 * fz;
+  float c10 = c100 * (1.0f - fz) + c101 * fz;
+  float c11 = c110 * (1.0f - fz) + c111 * fz;
+  float c0 = c00 * (1.0f - fy) + c01 * fy;
+  float c1 = c10 * (1.0f - fy) + c11 * fy;
+  return c0 * (1.0f - fx) + c1 * fx;
+}
+
+// orchestrator geometry.rs:153-175
+void sdf_gradient(const float* d, const uint32_t dims[3], const float origin[3], float cell,
+                  const float pt[3], float out[3]) {
+  float h = cell * 0.5f;
+  float a[3], bb[3];
+  float g[3];
+  for (int k = 0; k < 3; ++k) {
+    for (int m = 0; m < 3; ++m) { a[m] = pt[m]; bb[m] = pt[m]; }
+    a[k] = pt[k] + h;
+    bb[k] = pt[k] - h;
+    g[k] = (sdf_sample(d, dims, origin, cell, a) - sdf_sample(d, dims, origin, cell, bb)) / (2.0f * h);
+  }
+  float mag = sqrtf(g[0] * g[0] + g[1] * g[1] + g[2] * g[2]);
+  if (mag > 1e-8f) { out[0] = g[0] / mag; out[1] = g[1] / mag; out[2] = g[2] / mag; }
+  else { out[0] = 0.0f; out[1] = 0.0f; out[2] = 0.0f; }
+}
+
+}  // namespace
+
+extern "C" {
+
+// ---- scalar known-answer functions -------------------------------------
+float orc_wendland(float r, float h) { return wendland_c2(r, h); }
+void orc_wendland_gradient(float dx, float dy, float dz, float r, float h, float* out3) {
+  wendland_c2_gradient(dx, dy, dz, r, h, &out3[0], &out3[1], &out3[2]);
+}
+float orc_tait(float rho, float rho0, float c, float gamma, int pow_mode) {
+  return tait_eos(rho, rho0, c, gamma, pow_mode);
+}
+float orc_norm() { return kNorm; }
+
+// ---- neighbour grid -----------------------------------------------------
+void orc_grid_dims(float cell, const float* mn, const float* mx, uint32_t* dims_out) {
+  NeighborGrid g(cell, mn, mx);
+  for (int k = 0; k < 3; ++k) dims_out[k] = g.dims[k];
+}
+
+// NeighborGrid::update restated; plus per-particle (cx,cy,cz), the 30-bit
+// Morton key of the cell, and the Morton-ordered layout: cells ranked by
+// Morton code, particles stably sorted by (cell rank, index).
+// counts/offsets/morton_offsets have total_cells entries.
+void orc_grid_build(size_t n, const float* x, const float* y, const float* z, float cell,
+                    const float* mn, const float* mx, uint32_t* cell_idx, uint32_t* counts,
+                    uint32_t* offsets, uint32_t* sorted, uint32_t* morton_key,
+                    uint32_t* morton_offsets, uint32_t* morton_perm) {
+  NeighborGrid g(cell, mn, mx);
+  g.update(x, y, z, n);
+  size_t tc = g.total_cells();
+  std::memcpy(cell_idx, g.cell_indices.data(), n * 4);
+  std::memcpy(counts, g.cell_counts.data(), tc * 4);
+  std::memcpy(offsets, g.cell_offsets.data(), tc * 4);
+  std::memcpy(sorted, g.sorted_indices.data(), n * 4);
+  for (size_t i = 0; i < n; ++i) {
+    uint32_t cx, cy, cz;
+    g.pos_to_cell(x[i], y[i], z[i], &cx, &cy, &cz);
+    morton_key[i] = morton30(cx, cy, cz);
+  }
+  // Cells in Morton order (dims <= 1024 per axis so codes are unique).
+  std::vector<std::pair<uint32_t, uint32_t>> cells(tc);
+  for (uint32_t cz = 0; cz < g.dims[2]; ++cz)
+    for (uint32_t cy = 0; cy < g.dims[1]; ++cy)
+      for (uint32_t cx = 0; cx < g.dims[0]; ++cx) {
+        uint32_t lin = g.cell_hash(cx, cy, cz);
+        cells[lin] = {morton30(cx, cy, cz), lin};
+      }
+  std::sort(cells.begin(), cells.end());
+  uint32_t running = 0;
+  for (size_t r = 0; r < tc; ++r) {
+    uint32_t lin = cells[r].second;
+    morton_offsets[lin] = running;
+    running += g.cell_counts[lin];
+  }
+  std::vector<uint32_t> heads(morton_offsets, morton_offsets + tc);
+  for (size_t i = 0; i < n; ++i) {
+    uint32_t ci = g.cell_indices[i];
+    morton_perm[heads[ci]++] = (uint32_t)i;
+  }
+}
+
+// Neighbour list of particle i in the reference visit order.
+size_t orc_neighbors(size_t n, const float* x, const float* y, const float* z, float h,
+                     const float* mn, const float* mx, size_t i, uint32_t* out, size_t cap) {
+  NeighborGrid g(2.0f * h, mn, mx);
+  g.update(x, y, z, n);
+  size_t k = 0;
+  g.for_each_neighbor(i, x, y, z, 2.0f * h, [&](size_t j) {
+    if (k < cap) out[k] = (uint32_t)j;
+    ++k;
+  });
+  return k;
+}
+
+// ---- kernel -------------------------------------------------------------
+void* orc_create(const OrcParams* prm, size_t n, float* const* fields, const uint8_t* ft,
+                 size_t nb, float* const* bfields) {
+  Particles p = make_particles(n, fields, ft);
+  Boundary b;
+  std::vector<float>* bf[7] = {&b.x, &b.y, &b.z, &b.mass, &b.nx, &b.ny, &b.nz};
+  for (int k = 0; k < 7; ++k) bf[k]->assign(bfields[k], bfields[k] + nb);
+  b.pressure.assign(nb, 0.0f);
+  return new Kernel(*prm, std::move(p), std::move(b));
+}
+void orc_destroy(void* k) { delete static_cast<Kernel*>(k); }
+void orc_step(void* k, float dt) { static_cast<Kernel*>(k)->step(dt); }
+void orc_compute_forces(void* k, float dt) { static_cast<Kernel*>(k)->compute_forces(dt); }
+size_t orc_particle_count(void* k) { return static_cast<Kernel*>(k)->p.len(); }
+void orc_get(void* kp, float* const* fields, uint8_t* ft) {
+  Kernel* k = static_cast<Kernel*>(kp);
+  size_t n = k->p.len();
+  for (int f = 0; f < 13; ++f) std::memcpy(fields[f], k->p.field(f)->data(), n * 4);
+  if (ft) std::memcpy(ft, k->p.fluid_type.data(), n);
+}
+void orc_get_boundary_pressure(void* kp, float* out) {
+  Kernel* k = static_cast<Kernel*>(kp);
+  std::memcpy(out, k->b.pressure.data(), k->b.len() * 4);
+}
+void orc_error_metrics(void* k, float* out3) { static_cast<Kernel*>(k)->error_metrics(out3); }
+float orc_compute_timestep(void* kp, float cfl) {
+  Kernel* k = static_cast<Kernel*>(kp);
+  return compute_timestep(k->p, k->prm.h, k->prm.speed_of_sound, cfl);
+}
+// lib.rs:383-395: the checkpoint holds the particle arrays only.
+int orc_save_checkpoint(void* kp) {
+  Kernel* k = static_cast<Kernel*>(kp);
+  k->checkpoint = k->p;
+  k->has_checkpoint = true;
+  return 1;
+}
+int orc_restore_checkpoint(void* kp) {
+  Kernel* k = static_cast<Kernel*>(kp);
+  if (!k->has_checkpoint) return 0;
+  k->p = std::move(k->checkpoint);
+  k->checkpoint = Particles();
+  k->has_checkpoint = false;
+  return 1;
+}
+// Number of (cell, boundary) candidate pairs of Tier G (0 for Tier L).
+size_t orc_boundary_list_size(void* kp) { return static_cast<Kernel*>(kp)->bc_list.size(); }
+
+float orc_compute_timestep_arrays(size_t n, const float* vx, const float* vy, const float* vz,
+                                  const float* ax, const float* ay, const float* az, float h,
+                                  float c, float cfl) {
+  Particles p;
+  p.vx.assign(vx, vx + n); p.vy.assign(vy, vy + n); p.vz.assign(vz, vz + n);
+  p.ax.assign(ax, ax + n); p.ay.assign(ay, ay + n); p.az.assign(az, az + n);
+  p.x.resize(n);
+  return compute_timestep(p, h, c, cfl);
+}
+
+// ---- GridSDF ------------------------------------------------------------
+float orc_sdf_sample(const float* d, const uint32_t* dims, const float* origin, float cell,
+                     const float* pt) {
+  return sdf_sample(d, dims, origin, cell, pt);
+}
+void orc_sdf_gradient(const float* d, const uint32_t* dims, const float* origin, float cell,
+                      const float* pt, float* out3) {
+  sdf_gradient(d, dims, origin, cell, pt, out3);
+}
+
+}  // extern "C"

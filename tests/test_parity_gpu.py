@@ -1,0 +1,254 @@
+"""Parity of the CUDA step against the CPU oracle, through the C ABI.
+
+The CUDA step is compared bit for bit with the oracle in pow_mode 1 (the
+correctly rounded Tait power it implements) and within 1e-6 relative on
+positions with the oracle in pow_mode 0 (libm powf, the reference on Linux).
+Grid keys, cell counts/starts, the Morton permutation and neighbour lists
+must be identical.
+"""
+import numpy as np
+import pytest
+
+from oracle import oracle as orc
+from ultraballpit_b200 import domain
+from ultraballpit_b200.kernel import CELL_ORDER_LINEAR, CELL_ORDER_MORTON, CudaKernel, SphError
+from ultraballpit_b200.particles import BoundaryParticles, ParticleArrays
+
+pytestmark = pytest.mark.gpu
+FIELDS = ("x", "y", "z", "vx", "vy", "vz", "ax", "ay", "az", "density", "pressure", "mass")
+POS_RTOL = 1e-6  # positions vs the libm-powf oracle, relative to the domain extent
+
+
+def make_pair(sc, pow_mode=1, threads=8, **kw):
+    args = sc.kernel_args()
+    gpu = CudaKernel(*args, alpha=sc.alpha, beta=sc.beta, **kw)
+    cpu = orc.OracleKernel(*args, alpha=sc.alpha, beta=sc.beta, tier=1, threads=threads,
+                           pow_mode=pow_mode)
+    return gpu, cpu
+
+
+def assert_same(a: ParticleArrays, b: ParticleArrays, fields=FIELDS):
+    for f in fields:
+        x, y = getattr(a, f), getattr(b, f)
+        bad = np.nonzero(~((x == y) | (np.isnan(x) & np.isnan(y))))[0]
+        assert bad.size == 0, f"{f}: {bad.size} differ, first id {bad[0]}: {x[bad[0]]!r} vs {y[bad[0]]!r}"
+    np.testing.assert_array_equal(a.fluid_type, b.fluid_type)
+    np.testing.assert_array_equal(a.temperature, b.temperature)
+
+
+def small_dam_break(seed=3):
+    return domain.dam_break(0.004, seed=seed, block=(0.04, 0.04, 0.04),
+                            domain_max=(0.08, 0.04, 0.04), with_sdf=False)
+
+
+# ---- grid / sort -------------------------------------------------------------
+
+def _grid_vs_oracle(sc, order):
+    gpu = CudaKernel(*sc.kernel_args(), cell_order=order)
+    g = gpu.read_grid()
+    p = sc.particles
+    o = orc.grid_build(p.x, p.y, p.z, 2 * sc.h, sc.domain_min, sc.domain_max)
+    assert tuple(g["dims"]) == o["dims"]
+    np.testing.assert_array_equal(g["cell_linear"], o["cell_idx"])
+    np.testing.assert_array_equal(g["morton_key"], o["morton_key"])
+    np.testing.assert_array_equal(g["cell_count"], o["counts"])
+    if order == CELL_ORDER_LINEAR:
+        np.testing.assert_array_equal(g["cell_start"], o["offsets"])
+        np.testing.assert_array_equal(g["slot_id"], o["sorted"])
+    else:
+        np.testing.assert_array_equal(g["cell_start"], o["morton_offsets"])
+        np.testing.assert_array_equal(g["slot_id"], o["morton_perm"])
+    return gpu, o
+
+
+@pytest.mark.parametrize("order", [CELL_ORDER_MORTON, CELL_ORDER_LINEAR])
+def test_grid_bit_exact_dam_break(order):
+    _grid_vs_oracle(domain.dam_break(0.004, seed=11, with_sdf=False), order)
+
+
+def _custom(x, y, z, dmin=(0, 0, 0), dmax=(1, 1, 1), h=0.05):
+    p = ParticleArrays.from_positions(x, y, z, 1e-3)
+    return domain.Scenario("custom", p, BoundaryParticles(), h, (0, 0, -9.81), 20.0, 0.25, 0.0, dmin, dmax)
+
+
+@pytest.mark.parametrize("order", [CELL_ORDER_MORTON, CELL_ORDER_LINEAR])
+def test_grid_adversarial(order):
+    rng = np.random.default_rng(5)
+    cell = np.float32(0.1)
+    # on cell faces, outside the domain (clamped), and a crowded cell
+    faces = (rng.integers(0, 11, size=(600, 3)).astype(np.float32) * cell).astype(np.float32)
+    outside = rng.uniform(-0.5, 1.5, size=(400, 3)).astype(np.float32)
+    crowd = (np.float32(0.55) + rng.uniform(-0.01, 0.01, size=(700, 3))).astype(np.float32)
+    pts = np.concatenate([faces, outside, crowd])
+    sc = _custom(pts[:, 0], pts[:, 1], pts[:, 2])
+    gpu, o = _grid_vs_oracle(sc, order)
+    for i in (0, 5, 600, 1000, 1500, 1699):
+        np.testing.assert_array_equal(gpu.neighbors(i), orc.neighbors(
+            sc.particles.x, sc.particles.y, sc.particles.z, sc.h, sc.domain_min, sc.domain_max, i))
+
+
+def test_grid_all_in_one_cell_and_single_particle():
+    pts = np.full((1000, 3), 0.5, np.float32) + np.random.default_rng(1).uniform(
+        -0.02, 0.02, size=(1000, 3)).astype(np.float32)
+    _grid_vs_oracle(_custom(pts[:, 0], pts[:, 1], pts[:, 2]), CELL_ORDER_MORTON)
+    _grid_vs_oracle(_custom([0.5], [0.5], [0.5]), CELL_ORDER_MORTON)
+
+
+def test_neighbor_lists_reference_order():
+    sc = domain.dam_break(0.004, seed=12, with_sdf=False)
+    gpu = CudaKernel(*sc.kernel_args())
+    p = sc.particles
+    for i in np.random.default_rng(0).integers(0, len(p), 64):
+        np.testing.assert_array_equal(
+            gpu.neighbors(int(i)), orc.neighbors(p.x, p.y, p.z, sc.h, sc.domain_min, sc.domain_max, int(i)))
+
+
+# ---- one step and short runs, bit for bit ---------------------------------------
+
+@pytest.mark.parametrize("make", [domain.two_particles, domain.hydrostatic_column,
+                                  domain.water_box_2mm, small_dam_break])
+def test_steps_bit_exact(make):
+    sc = make()
+    gpu, cpu = make_pair(sc)
+    assert_same(gpu.particles(), cpu.particles())
+    for s in range(5):
+        dt = 1e-4 if sc.name in ("two_particles", "hydrostatic_column") else cpu.compute_timestep(sc.cfl_number)
+        gpu.step(dt)
+        cpu.step(dt)
+        assert_same(gpu.particles(), cpu.particles())
+    np.testing.assert_array_equal(gpu.boundary_pressure(), cpu.boundary_pressure())
+
+
+def test_two_particle_newton3_on_gpu():
+    sc = domain.two_particles()
+    gpu = CudaKernel(*sc.kernel_args())
+    gpu.step(0.0001)
+    p = gpu.particles()
+    for a in ("ax", "ay", "az"):
+        assert abs(getattr(p, a)[0] + getattr(p, a)[1]) < 1e-6
+
+
+def test_dam_break_100_steps_bit_exact_and_within_tolerance_of_powf():
+    """BASELINE config 1 inputs (31,250 particles, 52,500 wall particles)."""
+    sc = domain.dam_break(0.004, seed=1234, with_sdf=False)
+    gpu, cpu = make_pair(sc, pow_mode=1)
+    ref = orc.OracleKernel(*sc.kernel_args(), alpha=sc.alpha, tier=1, threads=8, pow_mode=0)
+    for s in range(100):
+        dt = cpu.compute_timestep(sc.cfl_number)
+        assert gpu.compute_timestep() == dt
+        gpu.step(dt)
+        cpu.step(dt)
+        ref.step(dt)
+    g, c, r = gpu.particles(), cpu.particles(), ref.particles()
+    assert_same(g, c)
+    np.testing.assert_array_equal(gpu.boundary_pressure(), cpu.boundary_pressure())
+    extent = max(b - a for a, b in zip(sc.domain_min, sc.domain_max))
+    for f in ("x", "y", "z"):
+        err = np.max(np.abs(getattr(g, f).astype(np.float64) - getattr(r, f)))
+        assert err <= POS_RTOL * extent, (f, err)
+    em_g, em_c = gpu.error_metrics(), cpu.error_metrics()
+    assert em_g.max_density_variation == em_c.max_density_variation
+    assert abs(em_g.energy_conservation - em_c.energy_conservation) <= 1e-6 * max(1e-3, em_c.energy_conservation)
+    assert abs(em_g.mass_conservation - em_c.mass_conservation) <= 1e-9
+
+
+def test_step_auto_matches_host_loop():
+    sc = small_dam_break(seed=9)
+    a = CudaKernel(*sc.kernel_args(), alpha=sc.alpha)
+    b = CudaKernel(*sc.kernel_args(), alpha=sc.alpha)
+    for _ in range(20):
+        b.step(b.compute_timestep())
+    dt_last = a.step_auto(20)
+    assert_same(a.particles(), b.particles())
+    assert dt_last > 0
+
+
+def test_checkpoint_restore_matches_oracle():
+    sc = small_dam_break(seed=4)
+    gpu, cpu = make_pair(sc)
+    for k in (gpu, cpu):
+        k.step(1e-4)
+        assert k.save_checkpoint()
+        k.step(2e-4)
+        k.step(2e-4)
+        assert k.restore_checkpoint()
+        assert not k.restore_checkpoint()
+        k.step(1e-4)  # steps on the stale grid, as the reference does
+    assert_same(gpu.particles(), cpu.particles())
+
+
+def test_linear_and_morton_layouts_give_identical_physics():
+    sc = small_dam_break(seed=6)
+    a = CudaKernel(*sc.kernel_args(), alpha=sc.alpha, cell_order=CELL_ORDER_MORTON)
+    b = CudaKernel(*sc.kernel_args(), alpha=sc.alpha, cell_order=CELL_ORDER_LINEAR)
+    for _ in range(10):
+        dt = a.compute_timestep()
+        a.step(dt)
+        b.step(dt)
+    assert_same(a.particles(), b.particles())
+
+
+def test_profiled_step_equals_graph_step():
+    sc = small_dam_break(seed=8)
+    a = CudaKernel(*sc.kernel_args(), alpha=sc.alpha)
+    b = CudaKernel(*sc.kernel_args(), alpha=sc.alpha)
+    for _ in range(3):
+        prof = a.step_profiled(1e-4)
+        b.step(1e-4)
+        assert prof["total_us"] > 0
+    assert_same(a.particles(), b.particles())
+
+
+def test_empty_and_no_boundary():
+    p = ParticleArrays.empty(0)
+    k = CudaKernel(p, None, 0.01, (0, 0, -9.81), 20.0, 0.25, 0.0, (0, 0, 0), (1, 1, 1))
+    k.step(1e-4)
+    assert k.particle_count() == 0
+    assert len(k.particles()) == 0
+
+
+def test_invalid_arguments_raise():
+    sc = domain.two_particles()
+    with pytest.raises(SphError):
+        CudaKernel(sc.particles, None, -1.0, (0, 0, 0), 20.0, 0.3, 1.0, (-1, -1, -1), (1, 1, 1))
+    k = CudaKernel(*sc.kernel_args())
+    with pytest.raises(SphError):
+        k.step(float("nan"))
+    assert not k.restore_checkpoint()
+
+
+def test_health_counts_nonfinite():
+    sc = domain.two_particles()
+    p = sc.particles.copy()
+    p.vx[0] = np.float32("inf")
+    k = CudaKernel(p, None, sc.h, sc.gravity, sc.speed_of_sound, sc.cfl_number, sc.viscosity,
+                   sc.domain_min, sc.domain_max)
+    assert k.health() == 1
+
+
+# ---- BASELINE config 2 scale -------------------------------------------------------
+
+def test_dam_break_sphere_2m_particles_one_step_bit_exact_and_invariants():
+    """BASELINE config 2 inputs: 2,000,000 particles at dx = 1 mm with the sphere."""
+    sc = domain.dam_break(0.001, seed=2024, sphere=True)
+    assert len(sc.particles) == 2_000_000
+    gpu, cpu = make_pair(sc, threads=16)
+    g = gpu.read_grid()
+    assert int(g["cell_count"].sum()) == len(sc.particles)
+    assert np.array_equal(np.sort(g["slot_id"]), np.arange(len(sc.particles), dtype=np.uint32))
+    dt = cpu.compute_timestep(sc.cfl_number)
+    assert gpu.compute_timestep() == dt
+    gpu.step(dt)
+    cpu.step(dt)
+    assert_same(gpu.particles(), cpu.particles())
+    np.testing.assert_array_equal(gpu.boundary_pressure(), cpu.boundary_pressure())
+    # size-independent invariants over further steps
+    m0 = gpu.particles().mass.copy()
+    dt_last = gpu.step_auto(20)
+    p = gpu.particles()
+    assert dt_last > 0 and gpu.health() == 0
+    np.testing.assert_array_equal(p.mass, m0)
+    for k, f in enumerate(("x", "y", "z")):
+        v = getattr(p, f)
+        assert v.min() >= sc.domain_min[k] and v.max() <= sc.domain_max[k]
+    assert gpu.error_metrics().mass_conservation == 0.0

@@ -1,0 +1,832 @@
+// sph_api.cu - host side of libsph_cuda.so: the C ABI of include/sph_cuda.h.
+//
+// One SphHandle = one simulation on one device: its own stream, device
+// buffers and CUDA graphs. The step body (9 kernels) is captured once into a
+// graph and replayed; dt lives in device memory so the graph never changes.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "sph_cuda.h"
+#include "sph_kernels.cuh"
+
+using sph::SimConst;
+
+namespace {
+
+constexpr float kPiF = 3.14159265358979323846f;
+
+template <class T>
+struct DevBuf {
+  T* p = nullptr;
+  size_t n = 0;
+};
+
+inline int grid_for(long long n, int block) { return (int)((n + block - 1) / block); }
+
+}  // namespace
+
+struct SphHandle {
+  int dev = 0;
+  cudaStream_t st = nullptr;
+  SphParams prm{};
+  SimConst k{};
+  int n = 0, nb = 0, C = 0;
+  std::vector<float> temperature;
+  double init_energy = 0.0, init_mass = 0.0;
+  bool needs_init = true;
+  bool red_valid = false;
+  bool has_ck = false;
+  uint64_t launches = 0;
+  int body_kernels = 0;
+  uint64_t boundary_candidates = 0;
+  std::string error;
+
+  // sorted state
+  float4 *pos = nullptr, *vel = nullptr, *velout = nullptr, *acc = nullptr;
+  float2 *rv = nullptr, *rf = nullptr;
+  float* pr = nullptr;
+  uint32_t* id = nullptr;
+  // unsorted (post-drift) state and sort scratch
+  float4 *posU = nullptr, *velU = nullptr;
+  uint32_t *idU = nullptr, *keyU = nullptr, *tmp = nullptr, *tmpid = nullptr;
+  uint32_t *hist = nullptr, *cstart = nullptr, *ccount = nullptr, *cursor = nullptr, *bsum = nullptr;
+  uint32_t *rank_of_lin = nullptr, *lin_of_rank = nullptr;
+  uint2* ctab = nullptr;
+  int nbsum = 0;
+  // boundary
+  float4* bpos = nullptr;
+  float* bpress = nullptr;
+  uint32_t *bc_start = nullptr, *bc_list = nullptr;
+  // scalars
+  float *dt = nullptr, *dt_query = nullptr, *red = nullptr;
+  uint32_t* err = nullptr;
+  // metrics
+  int nparts = 0;
+  double *part_m = nullptr, *part_e = nullptr, *me = nullptr;
+  float *part_var = nullptr, *var = nullptr;
+  unsigned long long* bad = nullptr;
+  // checkpoint
+  float4 *ck_pos = nullptr, *ck_velout = nullptr, *ck_acc = nullptr;
+  float* ck_pr = nullptr;
+  uint32_t* ck_slot = nullptr;
+  // readback staging
+  float* stage = nullptr;
+  uint8_t* stage_ft = nullptr;
+  // diagnostics scratch
+  uint32_t* diag = nullptr;
+  // graphs
+  cudaGraphExec_t g_step = nullptr;
+  cudaGraphExec_t g_auto = nullptr;
+  std::vector<void*> allocs;
+};
+
+namespace {
+
+int set_err(SphHandle* h, int code, const std::string& msg) {
+  if (h) h->error = msg;
+  return code;
+}
+
+int cuda_status(SphHandle* h, cudaError_t e, const char* what) {
+  if (e == cudaSuccess) return SPH_OK;
+  std::string m = std::string(what) + ": " + cudaGetErrorString(e);
+  if (e == cudaErrorMemoryAllocation) return set_err(h, SPH_ERR_OOM, m);
+  return set_err(h, SPH_ERR_CUDA, m);
+}
+
+#define SPH_TRY(h, call)                                   \
+  do {                                                     \
+    cudaError_t _e = (call);                               \
+    if (_e != cudaSuccess) return cuda_status(h, _e, #call); \
+  } while (0)
+
+template <class T>
+cudaError_t dalloc(SphHandle* h, T** p, size_t count) {
+  *p = nullptr;
+  if (count == 0) count = 1;
+  cudaError_t e = cudaMalloc((void**)p, count * sizeof(T));
+  if (e == cudaSuccess) h->allocs.push_back((void*)*p);
+  return e;
+}
+
+uint64_t spread21(uint64_t v) {
+  uint64_t r = 0;
+  for (int b = 0; b < 21; ++b) r |= ((v >> b) & 1ull) << (3 * b);
+  return r;
+}
+
+// Step constants rounded in f32 as the reference evaluates them.
+SimConst make_const(const SphParams& p, const uint32_t dims[3]) {
+  SimConst k{};
+  float h = p.h;
+  k.h = h;
+  k.support = 2.0f * h;
+  k.radius_sq = k.support * k.support;
+  k.cell = 2.0f * h;
+  for (int a = 0; a < 3; ++a) {
+    k.gmin[a] = p.domain_min[a];
+    k.dims[a] = (int)dims[a];
+    k.grav[a] = p.gravity[a];
+    k.dmin[a] = p.domain_min[a];
+    k.dmax[a] = p.domain_max[a];
+  }
+  volatile float norm = 21.0f / (16.0f * kPiF);
+  float h3 = h * h * h;
+  k.norm_h3 = norm / h3;
+  k.norm_h4 = norm / (h3 * h);
+  k.eta_sq = 0.01f * h * h;
+  k.delta_coef = 0.1f * h * p.speed_of_sound;
+  k.neg_alpha_c = -p.alpha * p.speed_of_sound;
+  k.beta = p.beta;
+  k.b_water = 1000.0f * p.speed_of_sound * p.speed_of_sound / 7.0f;
+  k.b_air = 1.204f * p.speed_of_sound * p.speed_of_sound / 1.4f;
+  k.r0 = 0.5f * h;
+  volatile float ten = 10.0f;
+  k.rep_d = ten * 9.81f * 0.01f;
+  k.c = p.speed_of_sound;
+  k.reach = (float)(2.0 * (double)h * (1.0 + 1e-4) + 1e-4 * (double)k.cell);
+  k.sdf_coef = p.sdf_wall_coef;
+  k.flags = p.flags;
+  return k;
+}
+
+// Static per-cell candidate lists of boundary particles, ascending index. A
+// boundary particle is listed for every cell whose box (widened by a margin
+// above the rounding of pos_to_cell, unbounded outward on edge cells) comes
+// within 2h (plus margin): a superset of the particles in support.
+void build_boundary_lists(const SimConst& k, const SphBoundaryView* b, int C,
+                          std::vector<uint32_t>& start, std::vector<uint32_t>& list) {
+  start.assign((size_t)C + 1, 0);
+  list.clear();
+  if (!b || b->n == 0) return;
+  double cs = k.cell, margin = 1e-4 * cs;
+  double reach = 2.0 * (double)k.h * (1.0 + 1e-4) + margin;
+  std::vector<uint64_t> pairs;  // (cell << 32) | b
+  pairs.reserve(b->n * 12);
+  for (size_t bi = 0; bi < b->n; ++bi) {
+    double pos[3] = {b->x[bi], b->y[bi], b->z[bi]};
+    int lo[3], hi[3];
+    bool empty = false;
+    for (int a = 0; a < 3; ++a) {
+      double u0 = std::floor((pos[a] - reach - k.gmin[a]) / cs);
+      double u1 = std::floor((pos[a] + reach - k.gmin[a]) / cs);
+      lo[a] = (int)std::max(0.0, std::min((double)k.dims[a] - 1, u0));
+      hi[a] = (int)std::max(0.0, std::min((double)k.dims[a] - 1, u1));
+      if (!(pos[a] == pos[a])) empty = true;
+    }
+    if (empty) continue;
+    for (int cz = lo[2]; cz <= hi[2]; ++cz)
+      for (int cy = lo[1]; cy <= hi[1]; ++cy)
+        for (int cx = lo[0]; cx <= hi[0]; ++cx) {
+          int c3[3] = {cx, cy, cz};
+          double d2 = 0.0;
+          for (int a = 0; a < 3; ++a) {
+            double blo = c3[a] == 0 ? -1e300 : k.gmin[a] + c3[a] * cs - margin;
+            double bhi = c3[a] == k.dims[a] - 1 ? 1e300 : k.gmin[a] + (c3[a] + 1) * cs + margin;
+            double d = pos[a] < blo ? blo - pos[a] : (pos[a] > bhi ? pos[a] - bhi : 0.0);
+            d2 += d * d;
+          }
+          if (d2 < reach * reach) {
+            uint64_t lin = (uint64_t)cx + (uint64_t)cy * k.dims[0] + (uint64_t)cz * k.dims[0] * k.dims[1];
+            pairs.push_back((lin << 32) | (uint64_t)bi);
+          }
+        }
+  }
+  for (uint64_t pr : pairs) start[(pr >> 32) + 1]++;
+  for (int c = 0; c < C; ++c) start[c + 1] += start[c];
+  list.resize(pairs.size());
+  std::vector<uint32_t> head(start.begin(), start.end() - 1);
+  for (uint64_t pr : pairs) list[head[pr >> 32]++] = (uint32_t)(pr & 0xffffffffu);
+}
+
+// Sorting scratch + binning of posU into the cell tables (k_bin or the
+// xsph kernel fill `hist` first).
+void enqueue_scan_fill(SphHandle* h) {
+  using namespace sph;
+  int nbk = h->nbsum;
+  k_scan_reduce<<<nbk, kScanThreads, 0, h->st>>>(h->hist, h->C, h->bsum);
+  k_scan_bsum<<<1, kScanThreads, 0, h->st>>>(h->bsum, nbk);
+  k_scan_apply<<<nbk, kScanThreads, 0, h->st>>>(h->hist, h->C, h->bsum, h->lin_of_rank, h->cstart,
+                                                h->ccount, h->cursor, h->ctab);
+  k_fill<<<grid_for(h->n, 256), 256, 0, h->st>>>(h->n, h->keyU, h->idU, h->cursor, h->tmp, h->tmpid);
+  h->launches += 4;
+}
+
+void enqueue_density_adami(SphHandle* h) {
+  using namespace sph;
+  k_density<<<grid_for(h->n, 256), 256, 0, h->st>>>(h->k, h->n, h->dt, h->pos, h->rv, h->id, h->ctab,
+                                                    h->bc_start, h->bc_list, h->bpos, h->rf, h->pr,
+                                                    h->err);
+  h->launches += 1;
+  if (h->nb > 0) {
+    k_adami<<<grid_for(h->nb, kAdamiWarps), kAdamiWarps * 32, 0, h->st>>>(
+        h->k, h->nb, h->bpos, h->bpress, h->pos, h->rf, h->pr, h->id, h->ctab, h->err);
+    h->launches += 1;
+  }
+}
+
+void enqueue_forces(SphHandle* h, float hdt_scale) {
+  using namespace sph;
+  cudaMemsetAsync(h->red, 0, 2 * sizeof(float), h->st);
+  k_forces<<<grid_for(h->n, 256), 256, 0, h->st>>>(h->k, h->n, h->dt, hdt_scale, h->pos, h->vel, h->rf,
+                                                   h->pr, h->id, h->ctab, h->bc_start, h->bc_list,
+                                                   h->bpos, h->bpress, h->acc, h->velout, h->red,
+                                                   h->err);
+  h->launches += 1;
+}
+
+void enqueue_xsph_sort(SphHandle* h) {
+  using namespace sph;
+  k_xsph_drift<<<grid_for(h->n, 256), 256, 0, h->st>>>(h->k, h->n, h->dt, h->pos, h->velout, h->acc,
+                                                       h->id, h->ctab, h->rank_of_lin, h->posU,
+                                                       h->velU, h->idU, h->keyU, h->hist, h->err);
+  h->launches += 1;
+  enqueue_scan_fill(h);
+  k_reorder<<<grid_for(h->n, 256), 256, 0, h->st>>>(h->n, h->tmp, h->tmpid, h->keyU, h->cstart,
+                                                    h->ccount, h->posU, h->velU, h->pos, h->vel, h->rv,
+                                                    h->id, h->err, nullptr, nullptr, nullptr, nullptr,
+                                                    nullptr);
+  h->launches += 1;
+}
+
+// lib.rs:287-335 after the bootstrap: kick1+XSPH+drift+clamp, grid + reorder,
+// density, boundary pressure, forces + kick2.
+void enqueue_body(SphHandle* h) {
+  enqueue_xsph_sort(h);
+  enqueue_density_adami(h);
+  enqueue_forces(h, 1.0f);
+}
+
+// lib.rs:295-298: compute_forces(dt) once before the first step.
+void enqueue_bootstrap(SphHandle* h) {
+  enqueue_density_adami(h);
+  enqueue_forces(h, 0.0f);
+}
+
+int capture(SphHandle* h, bool with_finalize, cudaGraphExec_t* out) {
+  cudaGraph_t g = nullptr;
+  uint64_t before = h->launches;
+  SPH_TRY(h, cudaStreamBeginCapture(h->st, cudaStreamCaptureModeThreadLocal));
+  if (with_finalize)
+    sph::k_dt_finalize<<<1, 1, 0, h->st>>>(h->k.h, h->k.c, h->prm.cfl_number, h->red, h->dt);
+  enqueue_body(h);
+  cudaError_t e = cudaStreamEndCapture(h->st, &g);
+  if (e != cudaSuccess) return cuda_status(h, e, "cudaStreamEndCapture");
+  h->body_kernels = (int)(h->launches - before);
+  h->launches = before;
+  e = cudaGraphInstantiate(out, g, 0);
+  cudaGraphDestroy(g);
+  return cuda_status(h, e, "cudaGraphInstantiate");
+}
+
+int check_device_flags(SphHandle* h) {
+  uint32_t e = 0;
+  SPH_TRY(h, cudaMemcpyAsync(&e, h->err, sizeof(uint32_t), cudaMemcpyDeviceToHost, h->st));
+  SPH_TRY(h, cudaStreamSynchronize(h->st));
+  if (e & sph::kErrCellCap)
+    return set_err(h, SPH_ERR_CAPACITY, "a grid cell exceeded 4096 particles");
+  if (e & sph::kErrAdamiCap)
+    return set_err(h, SPH_ERR_CAPACITY, "a boundary particle has more than 256 fluid particles in support");
+  return SPH_OK;
+}
+
+void ensure_red(SphHandle* h) {
+  if (h->red_valid) return;
+  cudaMemsetAsync(h->red, 0, 2 * sizeof(float), h->st);
+  if (h->n > 0) {
+    sph::k_timestep_reduce<<<grid_for(h->n, 256), 256, 0, h->st>>>(h->k, h->n, h->velout, h->acc, h->red);
+    h->launches += 1;
+  }
+  h->red_valid = true;
+}
+
+void free_all(SphHandle* h) {
+  if (h->g_step) cudaGraphExecDestroy(h->g_step);
+  if (h->g_auto) cudaGraphExecDestroy(h->g_auto);
+  for (void* p : h->allocs) cudaFree(p);
+  h->allocs.clear();
+  if (h->st) cudaStreamDestroy(h->st);
+}
+
+}  // namespace
+
+extern "C" {
+
+void sph_params_default(SphParams* p) {
+  if (!p) return;
+  std::memset(p, 0, sizeof(*p));
+  p->alpha = 1.0f;
+  p->beta = 2.0f;
+  p->boundary_mode = SPH_BOUNDARY_PARTICLES;
+  p->cell_order = SPH_CELL_ORDER_MORTON;
+  p->flags = SPH_FLAGS_REFERENCE;
+  p->device = 0;
+  p->cfl_number = 0.25f;
+  p->sdf_wall_coef = 0.981f;
+}
+
+int sph_create(const SphParams* params, const SphParticlesView* pv, const SphBoundaryView* bv,
+               const SphSdfView* sdf, SphHandle** out) {
+  if (!out) return SPH_ERR_INVALID_ARG;
+  *out = nullptr;
+  if (!params || !pv) return SPH_ERR_INVALID_ARG;
+  const SphParams& P = *params;
+  if (!(P.h > 0.0f) || !std::isfinite(P.h) || !(P.speed_of_sound > 0.0f)) return SPH_ERR_INVALID_ARG;
+  for (int a = 0; a < 3; ++a)
+    if (!(P.domain_max[a] > P.domain_min[a])) return SPH_ERR_INVALID_ARG;
+  if (pv->n > 0x7fffffffull) return SPH_ERR_INVALID_ARG;
+  if (pv->n > 0 && (!pv->x || !pv->y || !pv->z || !pv->vx || !pv->vy || !pv->vz || !pv->ax || !pv->ay ||
+                    !pv->az || !pv->density || !pv->pressure || !pv->mass || !pv->temperature ||
+                    !pv->fluid_type))
+    return SPH_ERR_INVALID_ARG;
+  if (bv && bv->n > 0 && (!bv->x || !bv->y || !bv->z || !bv->mass)) return SPH_ERR_INVALID_ARG;
+  if (bv && bv->n > 0x7fffffffull) return SPH_ERR_INVALID_ARG;
+  if (P.boundary_mode != SPH_BOUNDARY_PARTICLES) return SPH_ERR_INVALID_ARG;
+  (void)sdf;
+
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0 || P.device < 0 || P.device >= ndev) {
+    cudaGetLastError();
+    return SPH_ERR_NO_DEVICE;
+  }
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, P.device) != cudaSuccess || prop.major != 10) {
+    cudaGetLastError();
+    return SPH_ERR_NO_DEVICE;
+  }
+
+  SphHandle* h = new (std::nothrow) SphHandle();
+  if (!h) return SPH_ERR_OOM;
+  h->prm = P;
+  h->dev = P.device;
+  h->n = (int)pv->n;
+  h->nb = bv ? (int)bv->n : 0;
+  auto fail = [&](int code) {
+    free_all(h);
+    delete h;
+    return code;
+  };
+  if (cudaSetDevice(h->dev) != cudaSuccess) return fail(SPH_ERR_NO_DEVICE);
+
+  // grid (neighbor.rs:29-46)
+  uint32_t dims[3];
+  float cell = 2.0f * P.h;
+  uint64_t C = 1;
+  for (int a = 0; a < 3; ++a) {
+    dims[a] = (uint32_t)fmaxf(ceilf((P.domain_max[a] - P.domain_min[a]) / cell), 1.0f);
+    C *= dims[a];
+  }
+  if (C > (1ull << 30) || dims[0] > (1u << 21) || dims[1] > (1u << 21) || dims[2] > (1u << 21))
+    return fail(SPH_ERR_INVALID_ARG);
+  h->C = (int)C;
+  h->k = make_const(P, dims);
+
+  // cell ranks: Morton order (21 bits per axis; the 30-bit key when all
+  // dims <= 1024) or linear order.
+  std::vector<uint32_t> lin_of_rank(C), rank_of_lin(C);
+  {
+    std::vector<std::pair<uint64_t, uint32_t>> cells(C);
+    for (uint32_t cz = 0; cz < dims[2]; ++cz)
+      for (uint32_t cy = 0; cy < dims[1]; ++cy)
+        for (uint32_t cx = 0; cx < dims[0]; ++cx) {
+          uint32_t lin = cx + cy * dims[0] + cz * dims[0] * dims[1];
+          uint64_t key = P.cell_order == SPH_CELL_ORDER_LINEAR
+                             ? lin
+                             : (spread21(cx) | (spread21(cy) << 1) | (spread21(cz) << 2));
+          cells[lin] = {key, lin};
+        }
+    std::sort(cells.begin(), cells.end());
+    for (uint64_t r = 0; r < C; ++r) {
+      lin_of_rank[r] = cells[r].second;
+      rank_of_lin[cells[r].second] = (uint32_t)r;
+    }
+  }
+  std::vector<uint32_t> bstart, blist;
+  build_boundary_lists(h->k, bv, h->C, bstart, blist);
+  h->boundary_candidates = blist.size();
+
+  // host-side initial conservation totals, in the reference's order
+  h->temperature.assign(pv->temperature ? pv->temperature : nullptr,
+                        pv->temperature ? pv->temperature + pv->n : nullptr);
+  {
+    double m = 0.0, e = 0.0;
+    for (size_t i = 0; i < pv->n; ++i) m += (double)pv->mass[i];
+    for (size_t i = 0; i < pv->n; ++i) {
+      double mi = (double)pv->mass[i];
+      double vx = pv->vx[i], vy = pv->vy[i], vz = pv->vz[i];
+      e += 0.5 * mi * (vx * vx + vy * vy + vz * vz);
+      double x = pv->x[i], y = pv->y[i], z = pv->z[i];
+      e -= mi * ((double)P.gravity[0] * x + (double)P.gravity[1] * y + (double)P.gravity[2] * z);
+    }
+    h->init_mass = m;
+    h->init_energy = e;
+  }
+
+  if (cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking) != cudaSuccess) return fail(SPH_ERR_CUDA);
+  size_t n = (size_t)h->n, nb = (size_t)h->nb;
+  h->nbsum = grid_for(h->C, sph::kScanTile);
+  h->nparts = std::max(1, std::min(grid_for((long long)n, sph::kMetricThreads), 1184));
+  cudaError_t e = cudaSuccess;
+#define ALLOC(ptr, cnt) \
+  if (e == cudaSuccess) e = dalloc(h, &h->ptr, (cnt))
+  ALLOC(pos, n); ALLOC(vel, n); ALLOC(velout, n); ALLOC(acc, n);
+  ALLOC(rv, n); ALLOC(rf, n); ALLOC(pr, n); ALLOC(id, n);
+  ALLOC(posU, n); ALLOC(velU, n); ALLOC(idU, n); ALLOC(keyU, n); ALLOC(tmp, n); ALLOC(tmpid, n);
+  ALLOC(hist, C); ALLOC(cstart, C); ALLOC(ccount, C); ALLOC(cursor, C); ALLOC(bsum, h->nbsum);
+  ALLOC(rank_of_lin, C); ALLOC(lin_of_rank, C); ALLOC(ctab, C);
+  ALLOC(bpos, nb); ALLOC(bpress, nb); ALLOC(bc_start, C + 1); ALLOC(bc_list, blist.size());
+  ALLOC(dt, 1); ALLOC(dt_query, 1); ALLOC(red, 2); ALLOC(err, 1);
+  ALLOC(part_m, h->nparts); ALLOC(part_e, h->nparts); ALLOC(part_var, h->nparts); ALLOC(me, 2);
+  ALLOC(var, 1); ALLOC(bad, 1);
+  ALLOC(stage, 12 * n); ALLOC(stage_ft, n); ALLOC(diag, 2);
+#undef ALLOC
+  if (e != cudaSuccess) return fail(e == cudaErrorMemoryAllocation ? SPH_ERR_OOM : SPH_ERR_CUDA);
+
+  // upload
+  std::vector<float4> hpos(n), hvel(n), hacc(n);
+  std::vector<uint32_t> hid(n);
+  for (size_t i = 0; i < n; ++i) {
+    hpos[i] = make_float4(pv->x[i], pv->y[i], pv->z[i], pv->mass[i]);
+    hvel[i] = make_float4(pv->vx[i], pv->vy[i], pv->vz[i], pv->density[i]);
+    hacc[i] = make_float4(pv->ax[i], pv->ay[i], pv->az[i], 0.0f);
+    hid[i] = (uint32_t)i | (pv->fluid_type[i] ? sph::kAirBit : 0u);
+  }
+  std::vector<float4> hb(nb);
+  for (size_t i = 0; i < nb; ++i) hb[i] = make_float4(bv->x[i], bv->y[i], bv->z[i], bv->mass[i]);
+  float4* accU = nullptr;
+  float* prU = nullptr;
+  auto up = [&](void* d, const void* s, size_t bytes) {
+    if (e == cudaSuccess && bytes) e = cudaMemcpyAsync(d, s, bytes, cudaMemcpyHostToDevice, h->st);
+  };
+  if (e == cudaSuccess) e = cudaMalloc(&accU, std::max<size_t>(1, n) * sizeof(float4));
+  if (e == cudaSuccess) e = cudaMalloc(&prU, std::max<size_t>(1, n) * sizeof(float));
+  up(h->posU, hpos.data(), n * sizeof(float4));
+  up(h->velU, hvel.data(), n * sizeof(float4));
+  up(accU, hacc.data(), n * sizeof(float4));
+  up(prU, pv->pressure, n * sizeof(float));
+  up(h->idU, hid.data(), n * sizeof(uint32_t));
+  up(h->bpos, hb.data(), nb * sizeof(float4));
+  up(h->rank_of_lin, rank_of_lin.data(), C * sizeof(uint32_t));
+  up(h->lin_of_rank, lin_of_rank.data(), C * sizeof(uint32_t));
+  up(h->bc_start, bstart.data(), (C + 1) * sizeof(uint32_t));
+  up(h->bc_list, blist.data(), blist.size() * sizeof(uint32_t));
+  if (e == cudaSuccess) e = cudaMemsetAsync(h->hist, 0, C * sizeof(uint32_t), h->st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(h->bpress, 0, std::max<size_t>(1, nb) * sizeof(float), h->st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(h->err, 0, sizeof(uint32_t), h->st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(h->ctab, 0, C * sizeof(uint2), h->st);
+  if (e == cudaSuccess && n > 0) {
+    using namespace sph;
+    k_bin<<<grid_for(h->n, 256), 256, 0, h->st>>>(h->k, h->n, h->posU, h->rank_of_lin, h->keyU, h->hist);
+    h->launches += 1;
+    enqueue_scan_fill(h);
+    k_reorder<<<grid_for(h->n, 256), 256, 0, h->st>>>(h->n, h->tmp, h->tmpid, h->keyU, h->cstart,
+                                                      h->ccount, h->posU, h->velU, h->pos, h->vel, h->rv,
+                                                      h->id, h->err, accU, h->acc, prU, h->pr, h->velout);
+    h->launches += 1;
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->st);
+  if (accU) cudaFree(accU);
+  if (prU) cudaFree(prU);
+  if (e != cudaSuccess) {
+    fprintf(stderr, "sph_create: %s\n", cudaGetErrorString(e));
+    return fail(e == cudaErrorMemoryAllocation ? SPH_ERR_OOM : SPH_ERR_CUDA);
+  }
+  ensure_red(h);
+  int s = check_device_flags(h);
+  if (s != SPH_OK) return fail(s);
+  *out = h;
+  return SPH_OK;
+}
+
+void sph_destroy(SphHandle* h) {
+  if (!h) return;
+  cudaSetDevice(h->dev);
+  if (h->st) cudaStreamSynchronize(h->st);
+  free_all(h);
+  delete h;
+}
+
+int sph_step(SphHandle* h, float dt) {
+  if (!h) return SPH_ERR_INVALID_ARG;
+  if (!std::isfinite(dt)) return set_err(h, SPH_ERR_INVALID_ARG, "dt must be finite");
+  SPH_TRY(h, cudaSetDevice(h->dev));
+  if (h->n == 0) return SPH_OK;
+  sph::k_set_dt<<<1, 1, 0, h->st>>>(h->dt, dt);
+  h->launches += 1;
+  if (h->needs_init) {
+    enqueue_bootstrap(h);
+    h->needs_init = false;
+  }
+  if (!h->g_step) {
+    int s = capture(h, false, &h->g_step);
+    if (s != SPH_OK) return s;
+  }
+  SPH_TRY(h, cudaGraphLaunch(h->g_step, h->st));
+  h->launches += h->body_kernels;
+  h->red_valid = true;
+  return cuda_status(h, cudaGetLastError(), "sph_step");
+}
+
+int sph_step_auto(SphHandle* h, int nsteps, float* dt_out) {
+  if (!h || nsteps < 0) return SPH_ERR_INVALID_ARG;
+  SPH_TRY(h, cudaSetDevice(h->dev));
+  if (h->n == 0) return SPH_OK;
+  for (int s = 0; s < nsteps; ++s) {
+    ensure_red(h);
+    if (h->needs_init) {
+      sph::k_dt_finalize<<<1, 1, 0, h->st>>>(h->k.h, h->k.c, h->prm.cfl_number, h->red, h->dt);
+      h->launches += 1;
+      enqueue_bootstrap(h);
+      h->needs_init = false;
+      if (!h->g_step) {
+        int st = capture(h, false, &h->g_step);
+        if (st != SPH_OK) return st;
+      }
+      SPH_TRY(h, cudaGraphLaunch(h->g_step, h->st));
+      h->launches += h->body_kernels;
+    } else {
+      if (!h->g_auto) {
+        int st = capture(h, true, &h->g_auto);
+        if (st != SPH_OK) return st;
+      }
+      SPH_TRY(h, cudaGraphLaunch(h->g_auto, h->st));
+      h->launches += h->body_kernels;
+    }
+    h->red_valid = true;
+  }
+  if (dt_out) {
+    SPH_TRY(h, cudaMemcpyAsync(dt_out, h->dt, sizeof(float), cudaMemcpyDeviceToHost, h->st));
+    SPH_TRY(h, cudaStreamSynchronize(h->st));
+    return check_device_flags(h);
+  }
+  return cuda_status(h, cudaGetLastError(), "sph_step_auto");
+}
+
+int sph_compute_timestep(SphHandle* h, float* dt_out) {
+  if (!h || !dt_out) return SPH_ERR_INVALID_ARG;
+  SPH_TRY(h, cudaSetDevice(h->dev));
+  if (h->n == 0) {
+    float dt = h->prm.cfl_number * h->prm.h / h->prm.speed_of_sound;
+    *dt_out = fminf(fmaxf(fminf(dt, 0.01f), 1.0e-8f), 0.01f);
+    return SPH_OK;
+  }
+  ensure_red(h);
+  sph::k_dt_finalize<<<1, 1, 0, h->st>>>(h->k.h, h->k.c, h->prm.cfl_number, h->red, h->dt_query);
+  h->launches += 1;
+  SPH_TRY(h, cudaMemcpyAsync(dt_out, h->dt_query, sizeof(float), cudaMemcpyDeviceToHost, h->st));
+  SPH_TRY(h, cudaStreamSynchronize(h->st));
+  return check_device_flags(h);
+}
+
+int sph_step_profiled(SphHandle* h, float dt, SphStepProfile* prof) {
+  if (!h || !prof) return SPH_ERR_INVALID_ARG;
+  if (!std::isfinite(dt)) return set_err(h, SPH_ERR_INVALID_ARG, "dt must be finite");
+  SPH_TRY(h, cudaSetDevice(h->dev));
+  std::memset(prof, 0, sizeof(*prof));
+  if (h->n == 0) return SPH_OK;
+  sph::k_set_dt<<<1, 1, 0, h->st>>>(h->dt, dt);
+  h->launches += 1;
+  if (h->needs_init) {
+    enqueue_bootstrap(h);
+    h->needs_init = false;
+  }
+  cudaEvent_t ev[6];
+  for (int i = 0; i < 6; ++i) SPH_TRY(h, cudaEventCreate(&ev[i]));
+  using namespace sph;
+  cudaEventRecord(ev[0], h->st);
+  k_xsph_drift<<<grid_for(h->n, 256), 256, 0, h->st>>>(h->k, h->n, h->dt, h->pos, h->velout, h->acc,
+                                                       h->id, h->ctab, h->rank_of_lin, h->posU, h->velU,
+                                                       h->idU, h->keyU, h->hist, h->err);
+  h->launches += 1;
+  cudaEventRecord(ev[1], h->st);
+  enqueue_scan_fill(h);
+  k_reorder<<<grid_for(h->n, 256), 256, 0, h->st>>>(h->n, h->tmp, h->tmpid, h->keyU, h->cstart, h->ccount,
+                                                    h->posU, h->velU, h->pos, h->vel, h->rv, h->id, h->err,
+                                                    nullptr, nullptr, nullptr, nullptr, nullptr);
+  h->launches += 1;
+  cudaEventRecord(ev[2], h->st);
+  k_density<<<grid_for(h->n, 256), 256, 0, h->st>>>(h->k, h->n, h->dt, h->pos, h->rv, h->id, h->ctab,
+                                                    h->bc_start, h->bc_list, h->bpos, h->rf, h->pr, h->err);
+  h->launches += 1;
+  cudaEventRecord(ev[3], h->st);
+  if (h->nb > 0) {
+    k_adami<<<grid_for(h->nb, kAdamiWarps), kAdamiWarps * 32, 0, h->st>>>(
+        h->k, h->nb, h->bpos, h->bpress, h->pos, h->rf, h->pr, h->id, h->ctab, h->err);
+    h->launches += 1;
+  }
+  cudaEventRecord(ev[4], h->st);
+  enqueue_forces(h, 1.0f);
+  cudaEventRecord(ev[5], h->st);
+  cudaError_t e = cudaEventSynchronize(ev[5]);
+  float t[5];
+  for (int i = 0; i < 5 && e == cudaSuccess; ++i) e = cudaEventElapsedTime(&t[i], ev[i], ev[i + 1]);
+  for (int i = 0; i < 6; ++i) cudaEventDestroy(ev[i]);
+  if (e != cudaSuccess) return cuda_status(h, e, "sph_step_profiled");
+  prof->xsph_drift_us = t[0] * 1e3f;
+  prof->sort_us = t[1] * 1e3f;
+  prof->density_us = t[2] * 1e3f;
+  prof->boundary_pressure_us = t[3] * 1e3f;
+  prof->forces_us = t[4] * 1e3f;
+  prof->total_us = (t[0] + t[1] + t[2] + t[3] + t[4]) * 1e3f;
+  h->red_valid = true;
+  return check_device_flags(h);
+}
+
+int sph_read_particles(SphHandle* h, SphParticlesMut* o) {
+  if (!h || !o) return SPH_ERR_INVALID_ARG;
+  if (o->n != (size_t)h->n) return set_err(h, SPH_ERR_INVALID_ARG, "particle count mismatch");
+  SPH_TRY(h, cudaSetDevice(h->dev));
+  size_t n = (size_t)h->n;
+  if (n == 0) return SPH_OK;
+  float* dst[12] = {o->x, o->y, o->z, o->vx, o->vy, o->vz, o->ax, o->ay, o->az, o->density, o->pressure, o->mass};
+  for (int f = 0; f < 12; ++f)
+    if (!dst[f]) return set_err(h, SPH_ERR_INVALID_ARG, "null output array");
+  sph::k_unsort<<<grid_for(h->n, 256), 256, 0, h->st>>>(h->n, h->pos, h->velout, h->acc, h->pr, h->id,
+                                                       h->stage, h->stage_ft);
+  h->launches += 1;
+  for (int f = 0; f < 12; ++f)
+    SPH_TRY(h, cudaMemcpyAsync(dst[f], h->stage + f * n, n * sizeof(float), cudaMemcpyDeviceToHost, h->st));
+  if (o->fluid_type)
+    SPH_TRY(h, cudaMemcpyAsync(o->fluid_type, h->stage_ft, n, cudaMemcpyDeviceToHost, h->st));
+  SPH_TRY(h, cudaStreamSynchronize(h->st));
+  if (o->temperature) std::memcpy(o->temperature, h->temperature.data(), n * sizeof(float));
+  return check_device_flags(h);
+}
+
+int sph_read_boundary_pressure(SphHandle* h, float* out, size_t nb) {
+  if (!h || (nb && !out) || nb != (size_t)h->nb) return SPH_ERR_INVALID_ARG;
+  SPH_TRY(h, cudaSetDevice(h->dev));
+  if (nb) SPH_TRY(h, cudaMemcpyAsync(out, h->bpress, nb * sizeof(float), cudaMemcpyDeviceToHost, h->st));
+  SPH_TRY(h, cudaStreamSynchronize(h->st));
+  return check_device_flags(h);
+}
+
+int sph_error_metrics(SphHandle* h, SphErrorMetrics* out) {
+  if (!h || !out) return SPH_ERR_INVALID_ARG;
+  SPH_TRY(h, cudaSetDevice(h->dev));
+  double me[2] = {0.0, 0.0};
+  float var = 0.0f;
+  if (h->n > 0) {
+    sph::k_metrics_partial<<<h->nparts, sph::kMetricThreads, 0, h->st>>>(h->k, h->n, h->pos, h->velout, h->id,
+                                                                       h->part_m, h->part_e, h->part_var);
+    sph::k_metrics_final<<<1, 32, 0, h->st>>>(h->nparts, h->part_m, h->part_e, h->part_var, h->me, h->var);
+    h->launches += 2;
+    SPH_TRY(h, cudaMemcpyAsync(me, h->me, 2 * sizeof(double), cudaMemcpyDeviceToHost, h->st));
+    SPH_TRY(h, cudaMemcpyAsync(&var, h->var, sizeof(float), cudaMemcpyDeviceToHost, h->st));
+    SPH_TRY(h, cudaStreamSynchronize(h->st));
+  }
+  double E0 = h->init_energy, M0 = h->init_mass;
+  out->max_density_variation = var;
+  out->energy_conservation = std::fabs(E0) > 1.0e-12 ? (float)std::fabs((me[1] - E0) / E0) : (float)std::fabs(me[1] - E0);
+  out->mass_conservation = std::fabs(M0) > 1.0e-12 ? (float)std::fabs((me[0] - M0) / M0) : (float)std::fabs(me[0] - M0);
+  return check_device_flags(h);
+}
+
+size_t sph_particle_count(const SphHandle* h) { return h ? (size_t)h->n : 0; }
+
+int sph_save_checkpoint(SphHandle* h) {
+  if (!h) return SPH_ERR_INVALID_ARG;
+  SPH_TRY(h, cudaSetDevice(h->dev));
+  size_t n = (size_t)h->n;
+  if (!h->ck_pos) {
+    cudaError_t e = cudaSuccess;
+    if (e == cudaSuccess) e = dalloc(h, &h->ck_pos, n);
+    if (e == cudaSuccess) e = dalloc(h, &h->ck_velout, n);
+    if (e == cudaSuccess) e = dalloc(h, &h->ck_acc, n);
+    if (e == cudaSuccess) e = dalloc(h, &h->ck_pr, n);
+    if (e == cudaSuccess) e = dalloc(h, &h->ck_slot, n);
+    if (e != cudaSuccess) return cuda_status(h, e, "checkpoint allocation");
+  }
+  if (n) {
+    SPH_TRY(h, cudaMemcpyAsync(h->ck_pos, h->pos, n * sizeof(float4), cudaMemcpyDeviceToDevice, h->st));
+    SPH_TRY(h, cudaMemcpyAsync(h->ck_velout, h->velout, n * sizeof(float4), cudaMemcpyDeviceToDevice, h->st));
+    SPH_TRY(h, cudaMemcpyAsync(h->ck_acc, h->acc, n * sizeof(float4), cudaMemcpyDeviceToDevice, h->st));
+    SPH_TRY(h, cudaMemcpyAsync(h->ck_pr, h->pr, n * sizeof(float), cudaMemcpyDeviceToDevice, h->st));
+    sph::k_index_ids<<<grid_for(h->n, 256), 256, 0, h->st>>>(h->n, h->id, h->ck_slot);
+    h->launches += 1;
+  }
+  h->has_ck = true;
+  return cuda_status(h, cudaGetLastError(), "sph_save_checkpoint");
+}
+
+int sph_restore_checkpoint(SphHandle* h) {
+  if (!h) return SPH_ERR_INVALID_ARG;
+  if (!h->has_ck) return set_err(h, SPH_ERR_NO_CHECKPOINT, "no checkpoint saved");
+  SPH_TRY(h, cudaSetDevice(h->dev));
+  if (h->n) {
+    sph::k_restore<<<grid_for(h->n, 256), 256, 0, h->st>>>(h->n, h->id, h->ck_slot, h->ck_pos, h->ck_velout,
+                                                          h->ck_acc, h->ck_pr, h->pos, h->velout, h->acc, h->pr);
+    h->launches += 1;
+  }
+  h->has_ck = false;
+  h->red_valid = false;
+  ensure_red(h);
+  return cuda_status(h, cudaGetLastError(), "sph_restore_checkpoint");
+}
+
+int sph_synchronize(SphHandle* h) {
+  if (!h) return SPH_ERR_INVALID_ARG;
+  SPH_TRY(h, cudaSetDevice(h->dev));
+  SPH_TRY(h, cudaStreamSynchronize(h->st));
+  return check_device_flags(h);
+}
+
+int sph_health(SphHandle* h, uint64_t* nonfinite) {
+  if (!h || !nonfinite) return SPH_ERR_INVALID_ARG;
+  SPH_TRY(h, cudaSetDevice(h->dev));
+  unsigned long long bad = 0;
+  SPH_TRY(h, cudaMemsetAsync(h->bad, 0, sizeof(unsigned long long), h->st));
+  if (h->n) {
+    sph::k_health<<<grid_for(h->n, 256), 256, 0, h->st>>>(h->n, h->pos, h->velout, h->bad);
+    h->launches += 1;
+  }
+  SPH_TRY(h, cudaMemcpyAsync(&bad, h->bad, sizeof(bad), cudaMemcpyDeviceToHost, h->st));
+  SPH_TRY(h, cudaStreamSynchronize(h->st));
+  *nonfinite = bad;
+  int s = check_device_flags(h);
+  if (s != SPH_OK) return s;
+  return bad ? set_err(h, SPH_ERR_NONFINITE, "non-finite particle state") : SPH_OK;
+}
+
+const char* sph_last_error(const SphHandle* h) { return h ? h->error.c_str() : "null handle"; }
+
+void* sph_stream(SphHandle* h) { return h ? (void*)h->st : nullptr; }
+
+uint64_t sph_launch_count(const SphHandle* h) { return h ? h->launches : 0; }
+
+int sph_grid_info(SphHandle* h, SphGridInfo* out) {
+  if (!h || !out) return SPH_ERR_INVALID_ARG;
+  for (int a = 0; a < 3; ++a) {
+    out->dims[a] = (uint32_t)h->k.dims[a];
+    out->grid_min[a] = h->k.gmin[a];
+  }
+  out->total_cells = (uint32_t)h->C;
+  out->cell_size = h->k.cell;
+  out->boundary_candidates = h->boundary_candidates;
+  return SPH_OK;
+}
+
+int sph_read_grid(SphHandle* h, uint32_t* cell_linear, uint32_t* morton_key, uint32_t* cell_count,
+                  uint32_t* cell_start, uint32_t* slot_id) {
+  if (!h) return SPH_ERR_INVALID_ARG;
+  SPH_TRY(h, cudaSetDevice(h->dev));
+  size_t n = (size_t)h->n, C = (size_t)h->C;
+  uint32_t* d_lin = nullptr;
+  uint32_t* d_mor = nullptr;
+  if ((cell_linear || morton_key) && n) {
+    SPH_TRY(h, cudaMalloc(&d_lin, n * sizeof(uint32_t)));
+    cudaError_t e = cudaMalloc(&d_mor, n * sizeof(uint32_t));
+    if (e != cudaSuccess) { cudaFree(d_lin); return cuda_status(h, e, "sph_read_grid"); }
+    sph::k_grid_keys<<<grid_for(h->n, 256), 256, 0, h->st>>>(h->k, h->n, h->pos, h->id, d_lin, d_mor);
+    h->launches += 1;
+    if (cell_linear) cudaMemcpyAsync(cell_linear, d_lin, n * 4, cudaMemcpyDeviceToHost, h->st);
+    if (morton_key) cudaMemcpyAsync(morton_key, d_mor, n * 4, cudaMemcpyDeviceToHost, h->st);
+  }
+  std::vector<uint2> tab;
+  if (cell_count || cell_start) {
+    tab.resize(C);
+    cudaMemcpyAsync(tab.data(), h->ctab, C * sizeof(uint2), cudaMemcpyDeviceToHost, h->st);
+  }
+  if (slot_id && n) cudaMemcpyAsync(slot_id, h->id, n * 4, cudaMemcpyDeviceToHost, h->st);
+  cudaError_t e = cudaStreamSynchronize(h->st);
+  if (d_lin) cudaFree(d_lin);
+  if (d_mor) cudaFree(d_mor);
+  if (e != cudaSuccess) return cuda_status(h, e, "sph_read_grid");
+  for (size_t c = 0; c < tab.size(); ++c) {
+    if (cell_start) cell_start[c] = tab[c].x;
+    if (cell_count) cell_count[c] = tab[c].y;
+  }
+  if (slot_id)
+    for (size_t s = 0; s < n; ++s) slot_id[s] &= sph::kIdMask;
+  return check_device_flags(h);
+}
+
+int sph_neighbors(SphHandle* h, uint32_t id, uint32_t* out, size_t cap, size_t* count) {
+  if (!h || !count || (cap && !out) || id >= (uint32_t)h->n) return SPH_ERR_INVALID_ARG;
+  SPH_TRY(h, cudaSetDevice(h->dev));
+  uint32_t* d_out = nullptr;
+  size_t c2 = std::max<size_t>(cap, 1);
+  SPH_TRY(h, cudaMalloc(&d_out, c2 * sizeof(uint32_t)));
+  sph::k_find_slot<<<grid_for(h->n, 256), 256, 0, h->st>>>(h->n, h->id, id, h->diag);
+  sph::k_list_neighbors<<<1, 1, 0, h->st>>>(h->k, h->pos, h->id, h->ctab, h->diag, d_out, (uint32_t)cap,
+                                            h->diag + 1);
+  h->launches += 2;
+  uint32_t cnt = 0;
+  cudaMemcpyAsync(&cnt, h->diag + 1, 4, cudaMemcpyDeviceToHost, h->st);
+  cudaError_t e = cudaStreamSynchronize(h->st);
+  if (e == cudaSuccess && cap) {
+    e = cudaMemcpy(out, d_out, std::min<size_t>(cap, cnt) * sizeof(uint32_t), cudaMemcpyDeviceToHost);
+  }
+  cudaFree(d_out);
+  if (e != cudaSuccess) return cuda_status(h, e, "sph_neighbors");
+  *count = cnt;
+  return SPH_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,361 @@
+"""Host-side scenario construction (initial particles, wall particles, analytic SDFs).
+
+Restates the reference orchestrator's setup in vectorised numpy with the same
+f32 arithmetic:
+
+* wall boundary particles: ``orchestrator/src/domain.rs:162-348`` (3 layers at
+  ``(layer + 0.5) * dx`` outside each wall face, tangential lattice
+  ``min + (j + 0.5) * dx`` with ``ceil(extent / dx)`` points per axis);
+* geometry boundary particles: ``domain.rs:351-402`` (fluid-lattice points with
+  ``0 < sdf < 0.5 dx`` get 3 layers along ``-grad(sdf)``);
+* ``GridSDF::sample`` / ``gradient``: ``orchestrator/src/geometry.rs:99-175``;
+* smoothing length ``1.3 * dx``: ``orchestrator/src/config.rs:269-271``;
+* the dam-break column: ``reference-tests/src/benchmarks.rs:89-109`` (lattice
+  block in the domain corner).
+
+The SDFs of the dam-break workloads are analytic (box, sphere), sampled at the
+node positions ``origin + i * cell`` that ``GridSDF::sample`` assumes.
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from .particles import BoundaryParticles, FluidType, GridSDF, ParticleArrays
+
+f32 = np.float32
+FMAX = np.float32(3.4028235e38)
+
+
+def smoothing_length(dx: float) -> np.float32:
+    """``config.rs:269-271``: ``1.3 * particle_spacing`` in f32."""
+    return f32(f32(1.3) * f32(dx))
+
+
+def particle_mass(dx: float, rest_density: float = 1000.0) -> np.float32:
+    """``domain.rs:43-44``: ``rho0 * dx^3`` in f32."""
+    dx = f32(dx)
+    return f32(f32(rest_density) * f32(f32(dx * dx) * dx))
+
+
+def _axis_count(lo, hi, dx) -> int:
+    return int(np.ceil(f32(f32(hi) - f32(lo)) / f32(dx)))
+
+
+def _lattice(lo, n, dx) -> np.ndarray:
+    """``lo + (i + 0.5) * dx`` for i < n, each op rounded to f32."""
+    i = np.arange(n, dtype=np.float32)
+    return (f32(lo) + (i + f32(0.5)) * f32(dx)).astype(np.float32)
+
+
+WALL_FACES = ("x_min", "x_max", "y_min", "y_max", "z_min", "z_max")
+
+
+def wall_boundary_particles(domain_min, domain_max, dx, mass,
+                            walls=WALL_FACES, n_layers: int = 3) -> BoundaryParticles:
+    """``domain.rs:162-348`` in the reference's face and loop order."""
+    mn = [f32(v) for v in domain_min]
+    mx = [f32(v) for v in domain_max]
+    dx = f32(dx)
+    out = {k: [] for k in ("x", "y", "z", "nx", "ny", "nz")}
+    for face in WALL_FACES:
+        if face not in walls:
+            continue
+        axis = "xyz".index(face[0])
+        t0, t1 = [a for a in range(3) if a != axis]
+        n0 = _axis_count(mn[t0], mx[t0], dx)
+        n1 = _axis_count(mn[t1], mx[t1], dx)
+        u = _lattice(mn[t0], n0, dx)
+        v = _lattice(mn[t1], n1, dx)
+        uu, vv = np.meshgrid(u, v, indexing="ij")
+        sign = 1.0 if face.endswith("min") else -1.0
+        for layer in range(n_layers):
+            off = f32(f32(layer) + f32(0.5)) * dx
+            c = f32(mn[axis] - off) if face.endswith("min") else f32(mx[axis] + off)
+            pos = [None, None, None]
+            pos[axis] = np.full(uu.size, c, dtype=np.float32)
+            pos[t0] = uu.ravel()
+            pos[t1] = vv.ravel()
+            nrm = [np.zeros(uu.size, np.float32) for _ in range(3)]
+            nrm[axis][:] = sign
+            for k, a in zip(("x", "y", "z"), pos):
+                out[k].append(a)
+            for k, a in zip(("nx", "ny", "nz"), nrm):
+                out[k].append(a)
+    cat = {k: (np.concatenate(v) if v else np.zeros(0, np.float32)) for k, v in out.items()}
+    n = cat["x"].shape[0]
+    return BoundaryParticles.from_arrays(cat["x"], cat["y"], cat["z"],
+                                         np.full(n, f32(mass), np.float32),
+                                         cat["nx"], cat["ny"], cat["nz"])
+
+
+def concat_boundary(*parts: BoundaryParticles) -> BoundaryParticles:
+    cols = {k: np.concatenate([getattr(p, k) for p in parts]).astype(np.float32)
+            for k in ("x", "y", "z", "mass", "nx", "ny", "nz")}
+    return BoundaryParticles.from_arrays(**cols)
+
+
+# ---------------------------------------------------------------------------
+# GridSDF (geometry.rs:99-175), vectorised
+# ---------------------------------------------------------------------------
+
+def sdf_sample(sdf: GridSDF, pts: np.ndarray) -> np.ndarray:
+    """Trilinear sample at points ``pts[..., 3]`` (f32); f32::MAX off-grid."""
+    pts = np.asarray(pts, dtype=np.float32)
+    o = [f32(v) for v in sdf.origin]
+    cs = f32(sdf.cell_size)
+    nx, ny, nz = (int(v) for v in sdf.dimensions)
+    g = [((pts[..., k] - o[k]) / cs).astype(np.float32) for k in range(3)]
+    i0 = [np.floor(gk).astype(np.int64) for gk in g]
+    ok = (i0[0] >= 0) & (i0[1] >= 0) & (i0[2] >= 0)
+    ok &= (i0[0] + 1 < nx) & (i0[1] + 1 < ny) & (i0[2] + 1 < nz)
+    ii = [np.where(ok, a, 0) for a in i0]
+    fr = [(g[k] - ii[k].astype(np.float32)).astype(np.float32) for k in range(3)]
+    d = sdf.distances
+
+    def at(di, dj, dk):
+        return d[(ii[0] + di) * ny * nz + (ii[1] + dj) * nz + (ii[2] + dk)]
+
+    one = f32(1.0)
+    fx, fy, fz = fr
+    c00 = at(0, 0, 0) * (one - fz) + at(0, 0, 1) * fz
+    c01 = at(0, 1, 0) * (one - fz) + at(0, 1, 1) * fz
+    c10 = at(1, 0, 0) * (one - fz) + at(1, 0, 1) * fz
+    c11 = at(1, 1, 0) * (one - fz) + at(1, 1, 1) * fz
+    c0 = c00 * (one - fy) + c01 * fy
+    c1 = c10 * (one - fy) + c11 * fy
+    val = (c0 * (one - fx) + c1 * fx).astype(np.float32)
+    return np.where(ok, val, FMAX).astype(np.float32)
+
+
+def sdf_gradient(sdf: GridSDF, pts: np.ndarray) -> np.ndarray:
+    """Central differences at +-0.5 cell, normalised (geometry.rs:153-175)."""
+    pts = np.asarray(pts, dtype=np.float32)
+    h = f32(f32(sdf.cell_size) * f32(0.5))
+    g = []
+    for k in range(3):
+        a = pts.copy()
+        b = pts.copy()
+        a[..., k] = (pts[..., k] + h).astype(np.float32)
+        b[..., k] = (pts[..., k] - h).astype(np.float32)
+        with np.errstate(over="ignore", invalid="ignore"):
+            g.append(((sdf_sample(sdf, a) - sdf_sample(sdf, b)) / f32(f32(2.0) * h)).astype(np.float32))
+    with np.errstate(over="ignore", invalid="ignore"):
+        mag = np.sqrt(g[0] * g[0] + g[1] * g[1] + g[2] * g[2]).astype(np.float32)
+        good = mag > f32(1e-8)
+        out = np.stack([np.where(good, gk / np.where(good, mag, 1), f32(0)) for gk in g], axis=-1)
+    return out.astype(np.float32)
+
+
+def sdf_node_grid(domain_min, domain_max, cell):
+    """Node counts ``ceil(extent / cell) + 1`` (geometry.rs:52-54) and positions."""
+    dims = tuple(_axis_count(domain_min[k], domain_max[k], cell) + 1 for k in range(3))
+    axes = [(f32(domain_min[k]) + np.arange(dims[k], dtype=np.float32) * f32(cell)).astype(np.float32)
+            for k in range(3)]
+    return dims, axes
+
+
+def box_sdf(domain_min, domain_max, cell) -> GridSDF:
+    """Distance to the nearest wall of the domain box: positive inside."""
+    dims, (ax, ay, az) = sdf_node_grid(domain_min, domain_max, cell)
+    X, Y, Z = np.meshgrid(ax.astype(np.float64), ay.astype(np.float64), az.astype(np.float64), indexing="ij")
+    d = np.minimum.reduce([X - domain_min[0], domain_max[0] - X, Y - domain_min[1],
+                           domain_max[1] - Y, Z - domain_min[2], domain_max[2] - Z])
+    return GridSDF(tuple(float(v) for v in domain_min), float(f32(cell)), dims,
+                   d.astype(np.float32).ravel())
+
+
+def sphere_sdf(domain_min, domain_max, cell, center, radius) -> GridSDF:
+    """Signed distance to a solid sphere: negative inside the solid."""
+    dims, (ax, ay, az) = sdf_node_grid(domain_min, domain_max, cell)
+    X, Y, Z = np.meshgrid(ax.astype(np.float64), ay.astype(np.float64), az.astype(np.float64), indexing="ij")
+    d = np.sqrt((X - center[0]) ** 2 + (Y - center[1]) ** 2 + (Z - center[2]) ** 2) - radius
+    return GridSDF(tuple(float(v) for v in domain_min), float(f32(cell)), dims,
+                   d.astype(np.float32).ravel())
+
+
+def merge_sdf(a: GridSDF, b: GridSDF) -> GridSDF:
+    """Union of solids: node-wise min of two SDFs on the same grid."""
+    assert a.dimensions == b.dimensions and a.cell_size == b.cell_size
+    return GridSDF(a.origin, a.cell_size, a.dimensions, np.minimum(a.distances, b.distances))
+
+
+def geometry_boundary_particles(sdf: GridSDF, domain_min, domain_max, dx, mass,
+                                n_layers: int = 3) -> BoundaryParticles:
+    """``domain.rs:351-402``: 3 layers along the inward normal at lattice points
+    within half a spacing outside the surface (i, j, k loop order kept)."""
+    dx = f32(dx)
+    n = [_axis_count(domain_min[k], domain_max[k], dx) for k in range(3)]
+    ax = [_lattice(domain_min[k], n[k], dx) for k in range(3)]
+    X, Y, Z = np.meshgrid(*ax, indexing="ij")
+    pts = np.stack([X.ravel(), Y.ravel(), Z.ravel()], axis=-1)
+    d = sdf_sample(sdf, pts)
+    sel = (d > f32(0)) & (d < f32(dx * f32(0.5)))
+    p = pts[sel]
+    nrm = sdf_gradient(sdf, p)
+    cols = {k: [] for k in ("x", "y", "z", "nx", "ny", "nz")}
+    # interleave layers per lattice point, as the reference pushes them
+    offs = [f32(f32(f32(layer) + f32(0.5)) * dx) for layer in range(n_layers)]
+    xs = np.stack([(p[:, 0] - nrm[:, 0] * o).astype(np.float32) for o in offs], axis=1).ravel()
+    ys = np.stack([(p[:, 1] - nrm[:, 1] * o).astype(np.float32) for o in offs], axis=1).ravel()
+    zs = np.stack([(p[:, 2] - nrm[:, 2] * o).astype(np.float32) for o in offs], axis=1).ravel()
+    rep = lambda a: np.repeat(a, n_layers).astype(np.float32)
+    cols = dict(x=xs, y=ys, z=zs, nx=rep(nrm[:, 0]), ny=rep(nrm[:, 1]), nz=rep(nrm[:, 2]))
+    m = np.full(xs.shape[0], f32(mass), np.float32)
+    return BoundaryParticles.from_arrays(cols["x"], cols["y"], cols["z"], m,
+                                         cols["nx"], cols["ny"], cols["nz"])
+
+
+# ---------------------------------------------------------------------------
+# Scenarios
+# ---------------------------------------------------------------------------
+
+@dataclass
+class Scenario:
+    """Everything ``CpuKernel::new`` (lib.rs:138-148) takes, plus extras."""
+
+    name: str
+    particles: ParticleArrays
+    boundary: BoundaryParticles
+    h: float
+    gravity: tuple
+    speed_of_sound: float
+    cfl_number: float
+    viscosity: float
+    domain_min: tuple
+    domain_max: tuple
+    alpha: float = 1.0
+    beta: float = 2.0
+    sdf: GridSDF | None = None
+    extras: dict = field(default_factory=dict)
+
+    def kernel_args(self):
+        return (self.particles, self.boundary, self.h, self.gravity, self.speed_of_sound,
+                self.cfl_number, self.viscosity, self.domain_min, self.domain_max)
+
+
+def dam_break_c0(height: float = 0.2, g: float = 9.81) -> float:
+    """``c0 = 10 sqrt(2 g H)`` (19.81 m/s at H = 0.2 m), no auto-tune."""
+    return float(f32(10.0 * math.sqrt(2.0 * g * height)))
+
+
+def block_particles(origin, counts, dx, seed: int | None, jitter: float = 0.01) -> ParticleArrays:
+    """Lattice block ``origin + (i + 0.5) dx`` in i (outer), j, k (inner) order,
+    jittered by U(-jitter dx, +jitter dx) per coordinate from ``seed``."""
+    dx = f32(dx)
+    axes = [_lattice(origin[k], counts[k], dx) for k in range(3)]
+    X, Y, Z = np.meshgrid(*axes, indexing="ij")
+    pos = np.stack([X.ravel(), Y.ravel(), Z.ravel()], axis=-1).astype(np.float32)
+    if seed is not None and jitter > 0:
+        rng = np.random.default_rng(seed)
+        pos = (pos.astype(np.float64) + rng.uniform(-jitter * float(dx), jitter * float(dx),
+                                                    size=pos.shape)).astype(np.float32)
+    return ParticleArrays.from_positions(pos[:, 0], pos[:, 1], pos[:, 2], particle_mass(dx))
+
+
+def dam_break(dx: float, seed: int = 1234, sphere: bool = False, alpha: float = 0.02,
+              block=(0.1, 0.2, 0.1), domain_max=(0.4, 0.2, 0.1), sdf_cell: float = 0.002,
+              with_sdf: bool = True) -> Scenario:
+    """The 3D dam break: domain [0, 0.4] x [0, 0.2] x [0, 0.1] m, water block
+    0.1 x 0.2 x 0.1 m in the corner, g = -9.81 z, c0 = 19.81 m/s, CFL 0.25,
+    walls on all six faces. ``sphere`` adds the fixed obstacle of radius
+    0.02 m at (0.25, 0.1, 0.03) as geometry boundary particles and merges it
+    into the SDF."""
+    dmin = (0.0, 0.0, 0.0)
+    dmax = tuple(float(v) for v in domain_max)
+    dx32 = f32(dx)
+    counts = tuple(_axis_count(0.0, block[k], dx32) for k in range(3))
+    parts = block_particles(dmin, counts, dx32, seed)
+    m = particle_mass(dx32)
+    walls = wall_boundary_particles(dmin, dmax, dx32, m)
+    sdf = None
+    extras = {"block": block, "counts": counts}
+    boundary = walls
+    if with_sdf or sphere:
+        sdf = box_sdf(dmin, dmax, sdf_cell)
+    if sphere:
+        center, radius = (0.25, 0.1, 0.03), 0.02
+        sph = sphere_sdf(dmin, dmax, sdf_cell, center, radius)
+        geo = geometry_boundary_particles(sph, dmin, dmax, dx32, m)
+        boundary = concat_boundary(walls, geo)
+        sdf = merge_sdf(sdf, sph)
+        extras.update(sphere_center=center, sphere_radius=radius, sphere_sdf=sph,
+                      n_geometry_boundary=len(geo))
+    return Scenario(
+        name=f"dam_break_dx{dx*1e3:g}mm" + ("_sphere" if sphere else ""),
+        particles=parts, boundary=boundary, h=float(smoothing_length(dx32)),
+        gravity=(0.0, 0.0, -9.81), speed_of_sound=dam_break_c0(), cfl_number=0.25,
+        viscosity=0.0, domain_min=dmin, domain_max=dmax, alpha=alpha, beta=2.0,
+        sdf=sdf, extras=extras)
+
+
+def two_particles(h: float = 0.05) -> Scenario:
+    """``kernel/tests/two_particle.rs:11-24``: two particles h apart on x."""
+    p = ParticleArrays.from_positions([0.0, h], [0.0, 0.0], [0.0, 0.0], 0.001)
+    return Scenario("two_particles", p, BoundaryParticles(), h, (0.0, 0.0, 0.0), 20.0, 0.3, 1.0,
+                    (-1.0, -1.0, -1.0), (1.0, 1.0, 1.0))
+
+
+def hydrostatic_column() -> Scenario:
+    """``kernel/tests/hydrostatic.rs:21-78``: 4x4x4 water column on 3 layers."""
+    h = f32(0.02)
+    spacing = f32(h / f32(1.3))
+    mass = f32(f32(1000.0) * spacing * spacing * spacing)
+    xs, ys, zs = [], [], []
+    for iy in range(4):
+        for iz in range(4):
+            for ix in range(4):
+                xs.append(f32(f32(ix + 0.5) * spacing))
+                ys.append(f32(f32(iy + 1.0) * spacing))
+                zs.append(f32(f32(iz + 0.5) * spacing))
+    p = ParticleArrays.from_positions(xs, ys, zs, mass)
+    b = BoundaryParticles()
+    bx, by, bz = [], [], []
+    for layer in range(3):
+        yb = f32(-f32(layer) * spacing)
+        for iz in range(-1, 4 + 2):
+            for ix in range(-1, 4 + 2):
+                bx.append(f32(f32(ix + 0.5) * spacing))
+                by.append(yb)
+                bz.append(f32(f32(iz + 0.5) * spacing))
+    nb = len(bx)
+    b = BoundaryParticles.from_arrays(bx, by, bz, np.full(nb, mass), np.zeros(nb), np.ones(nb), np.zeros(nb))
+    margin = f32(f32(6.0) * h)
+    dmin = (float(-margin),) * 3
+    dmax = (float(f32(f32(7) * spacing + margin)), float(f32(f32(14) * spacing + margin)),
+            float(f32(f32(7) * spacing + margin)))
+    return Scenario("hydrostatic_column", p, b, float(h), (0.0, -9.81, 0.0), 20.0, 0.2, 1.0, dmin, dmax)
+
+
+def water_box_2mm() -> Scenario:
+    """``kernel/tests/gpu_cpu_parity.rs:17-68``: 5x5x5 water box, bottom boundary."""
+    spacing = f32(0.002)
+    h = f32(f32(1.3) * spacing)
+    mass = f32(f32(1000.0) * f32(f32(spacing * spacing) * spacing))
+    xs, ys, zs = [], [], []
+    x = f32(f32(0.0) + f32(0.5) * spacing)
+    while x < f32(0.01):
+        y = f32(f32(0.5) * spacing)
+        while y < f32(0.01):
+            z = f32(f32(0.5) * spacing)
+            while z < f32(0.01):
+                xs.append(x); ys.append(y); zs.append(z)
+                z = f32(z + spacing)
+            y = f32(y + spacing)
+        x = f32(x + spacing)
+    p = ParticleArrays.from_positions(xs, ys, zs, mass)
+    bx, bz = [], []
+    xb = f32(0.0)
+    while xb <= f32(0.01):
+        zb = f32(0.0)
+        while zb <= f32(0.01):
+            bx.append(xb); bz.append(zb)
+            zb = f32(zb + spacing)
+        xb = f32(xb + spacing)
+    nb = len(bx)
+    b = BoundaryParticles.from_arrays(bx, np.zeros(nb), bz, np.full(nb, mass), np.zeros(nb),
+                                      np.ones(nb), np.zeros(nb))
+    return Scenario("water_box_2mm", p, b, float(h), (0.0, -9.81, 0.0), 10.0, 0.4, 0.001,
+                    (0.0, 0.0, 0.0), (0.01, 0.01, 0.01))

@@ -1,0 +1,356 @@
+"""Host-side mirror of the reference ``SimulationKernel`` trait over the C ABI.
+
+``CudaKernel`` is the ``cuda`` backend of ``kernel/src/lib.rs:58-78``: the same
+constructor arguments as ``CpuKernel::new`` (``lib.rs:138-148``) and the same
+methods (``step``, ``particles``, ``error_metrics``, ``particle_count``,
+``save_checkpoint``, ``restore_checkpoint``). Every call goes through
+``libsph_cuda.so`` (include/sph_cuda.h); there is no CPU fallback: a missing
+library or device raises ``SphError``.
+
+Like ``GpuKernel`` (``gpu/mod.rs:979-988``), ``particles()`` reads back lazily:
+the host copy is refreshed only after the state changed.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from abc import ABC, abstractmethod
+
+import numpy as np
+
+from .particles import (BOUNDARY_FIELDS, PARTICLE_FIELDS, BoundaryParticles, ErrorMetrics,
+                        GridSDF, ParticleArrays)
+
+LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "lib", "libsph_cuda.so")
+
+SPH_OK = 0
+STATUS_NAMES = {0: "SPH_OK", 1: "SPH_ERR_INVALID_ARG", 2: "SPH_ERR_OOM", 3: "SPH_ERR_CUDA",
+                4: "SPH_ERR_NONFINITE", 5: "SPH_ERR_TIMEOUT", 6: "SPH_ERR_CAPACITY",
+                7: "SPH_ERR_NO_DEVICE", 8: "SPH_ERR_NO_CHECKPOINT"}
+BOUNDARY_PARTICLES, BOUNDARY_SDF = 0, 1
+CELL_ORDER_MORTON, CELL_ORDER_LINEAR = 0, 1
+FLAG_DELTA_SPH, FLAG_XSPH, FLAG_REPULSION, FLAG_DOMAIN_CLAMP = 1, 2, 4, 8
+FLAGS_REFERENCE = 0xF
+
+# every entry point declared in include/sph_cuda.h
+EXPORTS = (
+    "sph_params_default", "sph_create", "sph_destroy", "sph_step", "sph_step_auto",
+    "sph_compute_timestep", "sph_step_profiled", "sph_read_particles",
+    "sph_read_boundary_pressure", "sph_error_metrics", "sph_particle_count",
+    "sph_save_checkpoint", "sph_restore_checkpoint", "sph_synchronize", "sph_health",
+    "sph_last_error", "sph_stream", "sph_launch_count", "sph_grid_info", "sph_read_grid",
+    "sph_neighbors",
+)
+
+
+class SphError(RuntimeError):
+    def __init__(self, status: int, msg: str = ""):
+        self.status = status
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {msg}")
+
+
+class SphParams(C.Structure):
+    _fields_ = [("h", C.c_float), ("gravity", C.c_float * 3), ("speed_of_sound", C.c_float),
+                ("cfl_number", C.c_float), ("viscosity", C.c_float),
+                ("domain_min", C.c_float * 3), ("domain_max", C.c_float * 3),
+                ("alpha", C.c_float), ("beta", C.c_float), ("boundary_mode", C.c_int32),
+                ("cell_order", C.c_int32), ("flags", C.c_uint32), ("device", C.c_int32),
+                ("sdf_wall_coef", C.c_float)]
+
+
+_FP = C.POINTER(C.c_float)
+_U8P = C.POINTER(C.c_uint8)
+_U32P = C.POINTER(C.c_uint32)
+
+
+class SphParticlesView(C.Structure):
+    _fields_ = [("n", C.c_size_t)] + [(f, _FP) for f in PARTICLE_FIELDS] + [("fluid_type", _U8P)]
+
+
+class SphParticlesMut(SphParticlesView):
+    pass
+
+
+class SphBoundaryView(C.Structure):
+    _fields_ = [("n", C.c_size_t)] + [(f, _FP) for f in BOUNDARY_FIELDS]
+
+
+class SphSdfView(C.Structure):
+    _fields_ = [("origin", C.c_float * 3), ("cell_size", C.c_float), ("dims", C.c_uint32 * 3),
+                ("distances", _FP)]
+
+
+class SphErrorMetrics(C.Structure):
+    _fields_ = [("max_density_variation", C.c_float), ("energy_conservation", C.c_float),
+                ("mass_conservation", C.c_float)]
+
+
+class SphStepProfile(C.Structure):
+    _fields_ = [(k, C.c_float) for k in ("xsph_drift_us", "sort_us", "density_us",
+                                         "boundary_pressure_us", "forces_us", "total_us")]
+
+    def as_dict(self) -> dict:
+        return {k: float(getattr(self, k)) for k, _ in self._fields_}
+
+
+class SphGridInfo(C.Structure):
+    _fields_ = [("dims", C.c_uint32 * 3), ("total_cells", C.c_uint32), ("cell_size", C.c_float),
+                ("grid_min", C.c_float * 3), ("boundary_candidates", C.c_uint64)]
+
+
+_lib = None
+
+
+def load_library(path: str | None = None):
+    """Load libsph_cuda.so; raises if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    p = path or LIB_PATH
+    if not os.path.exists(p):
+        raise SphError(7, f"{p} is missing: run python -m ultraballpit_b200.build")
+    L = C.CDLL(p)
+    vp, H = C.c_void_p, C.c_void_p
+    L.sph_params_default.argtypes = [C.POINTER(SphParams)]
+    L.sph_params_default.restype = None
+    L.sph_create.argtypes = [C.POINTER(SphParams), C.POINTER(SphParticlesView),
+                             C.POINTER(SphBoundaryView), C.POINTER(SphSdfView), C.POINTER(vp)]
+    L.sph_destroy.argtypes = [H]
+    L.sph_destroy.restype = None
+    L.sph_step.argtypes = [H, C.c_float]
+    L.sph_step_auto.argtypes = [H, C.c_int, _FP]
+    L.sph_compute_timestep.argtypes = [H, _FP]
+    L.sph_step_profiled.argtypes = [H, C.c_float, C.POINTER(SphStepProfile)]
+    L.sph_read_particles.argtypes = [H, C.POINTER(SphParticlesMut)]
+    L.sph_read_boundary_pressure.argtypes = [H, _FP, C.c_size_t]
+    L.sph_error_metrics.argtypes = [H, C.POINTER(SphErrorMetrics)]
+    L.sph_particle_count.argtypes = [H]
+    L.sph_particle_count.restype = C.c_size_t
+    L.sph_save_checkpoint.argtypes = [H]
+    L.sph_restore_checkpoint.argtypes = [H]
+    L.sph_synchronize.argtypes = [H]
+    L.sph_health.argtypes = [H, C.POINTER(C.c_uint64)]
+    L.sph_last_error.argtypes = [H]
+    L.sph_last_error.restype = C.c_char_p
+    L.sph_stream.argtypes = [H]
+    L.sph_stream.restype = vp
+    L.sph_launch_count.argtypes = [H]
+    L.sph_launch_count.restype = C.c_uint64
+    L.sph_grid_info.argtypes = [H, C.POINTER(SphGridInfo)]
+    L.sph_read_grid.argtypes = [H, _U32P, _U32P, _U32P, _U32P, _U32P]
+    L.sph_neighbors.argtypes = [H, C.c_uint32, _U32P, C.c_size_t, C.POINTER(C.c_size_t)]
+    for name in EXPORTS:
+        fn = getattr(L, name)
+        if getattr(fn, "restype", None) is C.c_int or name in (
+                "sph_create", "sph_step", "sph_step_auto", "sph_compute_timestep", "sph_step_profiled",
+                "sph_read_particles", "sph_read_boundary_pressure", "sph_error_metrics",
+                "sph_save_checkpoint", "sph_restore_checkpoint", "sph_synchronize", "sph_health",
+                "sph_grid_info", "sph_read_grid", "sph_neighbors"):
+            fn.restype = C.c_int
+    _lib = L
+    return L
+
+
+def _fp(a: np.ndarray):
+    return a.ctypes.data_as(_FP)
+
+
+def _u32p(a):
+    return None if a is None else a.ctypes.data_as(_U32P)
+
+
+def default_params() -> SphParams:
+    p = SphParams()
+    load_library().sph_params_default(C.byref(p))
+    return p
+
+
+class SimulationKernel(ABC):
+    """``kernel/src/lib.rs:58-78``."""
+
+    @abstractmethod
+    def step(self, dt: float) -> None: ...
+
+    @abstractmethod
+    def particles(self) -> ParticleArrays: ...
+
+    @abstractmethod
+    def error_metrics(self) -> ErrorMetrics: ...
+
+    @abstractmethod
+    def particle_count(self) -> int: ...
+
+    def save_checkpoint(self) -> bool:
+        return False
+
+    def restore_checkpoint(self) -> bool:
+        return False
+
+
+class CudaKernel(SimulationKernel):
+    """The ``cuda`` backend: one simulation on one B200 through libsph_cuda.so."""
+
+    def __init__(self, particles: ParticleArrays, boundary: BoundaryParticles | None, h: float,
+                 gravity, speed_of_sound: float, cfl_number: float, viscosity: float,
+                 domain_min, domain_max, *, alpha: float = 1.0, beta: float = 2.0,
+                 boundary_mode: int = BOUNDARY_PARTICLES, sdf: GridSDF | None = None,
+                 cell_order: int = CELL_ORDER_MORTON, flags: int = FLAGS_REFERENCE,
+                 device: int = 0, sdf_wall_coef: float = 0.981):
+        L = load_library()
+        particles.validate()
+        self._lib = L
+        self._n = len(particles)
+        self._nb = len(boundary) if boundary is not None else 0
+        self.h = float(h)
+        self.speed_of_sound = float(speed_of_sound)
+        self.cfl_number = float(cfl_number)
+        prm = default_params()
+        prm.h = h
+        prm.gravity = (C.c_float * 3)(*map(float, gravity))
+        prm.speed_of_sound = speed_of_sound
+        prm.cfl_number = cfl_number
+        prm.viscosity = viscosity
+        prm.domain_min = (C.c_float * 3)(*map(float, domain_min))
+        prm.domain_max = (C.c_float * 3)(*map(float, domain_max))
+        prm.alpha, prm.beta = alpha, beta
+        prm.boundary_mode, prm.cell_order, prm.flags, prm.device = boundary_mode, cell_order, flags, device
+        prm.sdf_wall_coef = sdf_wall_coef
+        keep = [np.ascontiguousarray(getattr(particles, f), np.float32) for f in PARTICLE_FIELDS]
+        ft = np.ascontiguousarray(particles.fluid_type, np.uint8)
+        pv = SphParticlesView(self._n, *[_fp(a) for a in keep], ft.ctypes.data_as(_U8P))
+        bv_p = None
+        if boundary is not None and self._nb:
+            bkeep = [np.ascontiguousarray(getattr(boundary, f), np.float32) for f in BOUNDARY_FIELDS]
+            bv = SphBoundaryView(self._nb, *[_fp(a) for a in bkeep])
+            bv_p = C.byref(bv)
+        sdf_p = None
+        if sdf is not None:
+            dist = np.ascontiguousarray(sdf.distances, np.float32)
+            sv = SphSdfView((C.c_float * 3)(*map(float, sdf.origin)), float(sdf.cell_size),
+                            (C.c_uint32 * 3)(*map(int, sdf.dimensions)), _fp(dist))
+            sdf_p = C.byref(sv)
+        handle = C.c_void_p()
+        st = L.sph_create(C.byref(prm), C.byref(pv), bv_p, sdf_p, C.byref(handle))
+        if st != SPH_OK:
+            raise SphError(st, "sph_create failed")
+        self._h = handle
+        self._cache: ParticleArrays | None = None
+
+    # -- lifecycle -------------------------------------------------------------
+    def close(self) -> None:
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            self._lib.sph_destroy(h)
+        self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, st: int, what: str) -> None:
+        if st != SPH_OK:
+            msg = self._lib.sph_last_error(self._h) if self._h is not None else b""
+            raise SphError(st, f"{what}: {msg.decode(errors='replace') if msg else ''}")
+
+    # -- SimulationKernel ------------------------------------------------------
+    def step(self, dt: float) -> None:
+        self._check(self._lib.sph_step(self._h, float(dt)), "sph_step")
+        self._cache = None
+
+    def particles(self) -> ParticleArrays:
+        if self._cache is None:
+            p = ParticleArrays.empty(self._n)
+            out = SphParticlesMut(self._n, *[_fp(getattr(p, f)) for f in PARTICLE_FIELDS],
+                                  p.fluid_type.ctypes.data_as(_U8P))
+            self._check(self._lib.sph_read_particles(self._h, C.byref(out)), "sph_read_particles")
+            self._cache = p
+        return self._cache
+
+    def error_metrics(self) -> ErrorMetrics:
+        m = SphErrorMetrics()
+        self._check(self._lib.sph_error_metrics(self._h, C.byref(m)), "sph_error_metrics")
+        return ErrorMetrics(float(m.max_density_variation), float(m.energy_conservation),
+                            float(m.mass_conservation))
+
+    def particle_count(self) -> int:
+        return int(self._lib.sph_particle_count(self._h))
+
+    def save_checkpoint(self) -> bool:
+        self._check(self._lib.sph_save_checkpoint(self._h), "sph_save_checkpoint")
+        return True
+
+    def restore_checkpoint(self) -> bool:
+        st = self._lib.sph_restore_checkpoint(self._h)
+        if st == 8:
+            return False
+        self._check(st, "sph_restore_checkpoint")
+        self._cache = None
+        return True
+
+    # -- device-side helpers beyond the trait ----------------------------------
+    def compute_timestep(self) -> float:
+        """``sph::compute_timestep(particles(), h, c, cfl)`` on the device."""
+        out = C.c_float()
+        self._check(self._lib.sph_compute_timestep(self._h, C.byref(out)), "sph_compute_timestep")
+        return float(out.value)
+
+    def step_auto(self, nsteps: int, want_dt: bool = True) -> float | None:
+        out = C.c_float()
+        st = self._lib.sph_step_auto(self._h, int(nsteps), C.byref(out) if want_dt else None)
+        self._check(st, "sph_step_auto")
+        self._cache = None
+        return float(out.value) if want_dt else None
+
+    def step_profiled(self, dt: float) -> dict:
+        prof = SphStepProfile()
+        self._check(self._lib.sph_step_profiled(self._h, float(dt), C.byref(prof)), "sph_step_profiled")
+        self._cache = None
+        return prof.as_dict()
+
+    def synchronize(self) -> None:
+        self._check(self._lib.sph_synchronize(self._h), "sph_synchronize")
+
+    def boundary_pressure(self) -> np.ndarray:
+        out = np.zeros(self._nb, np.float32)
+        self._check(self._lib.sph_read_boundary_pressure(self._h, _fp(out), self._nb),
+                    "sph_read_boundary_pressure")
+        return out
+
+    def health(self) -> int:
+        bad = C.c_uint64()
+        st = self._lib.sph_health(self._h, C.byref(bad))
+        if st not in (SPH_OK, 4):
+            self._check(st, "sph_health")
+        return int(bad.value)
+
+    def stream(self) -> int:
+        return int(self._lib.sph_stream(self._h) or 0)
+
+    def launch_count(self) -> int:
+        return int(self._lib.sph_launch_count(self._h))
+
+    def grid_info(self) -> dict:
+        g = SphGridInfo()
+        self._check(self._lib.sph_grid_info(self._h, C.byref(g)), "sph_grid_info")
+        return dict(dims=tuple(g.dims), total_cells=int(g.total_cells), cell_size=float(g.cell_size),
+                    grid_min=tuple(g.grid_min), boundary_candidates=int(g.boundary_candidates))
+
+    def read_grid(self) -> dict:
+        info = self.grid_info()
+        n, Cn = self._n, info["total_cells"]
+        out = dict(cell_linear=np.zeros(n, np.uint32), morton_key=np.zeros(n, np.uint32),
+                   cell_count=np.zeros(Cn, np.uint32), cell_start=np.zeros(Cn, np.uint32),
+                   slot_id=np.zeros(n, np.uint32))
+        self._check(self._lib.sph_read_grid(self._h, *[_u32p(out[k]) for k in (
+            "cell_linear", "morton_key", "cell_count", "cell_start", "slot_id")]), "sph_read_grid")
+        out.update(info)
+        return out
+
+    def neighbors(self, pid: int, cap: int = 4096) -> np.ndarray:
+        out = np.zeros(cap, np.uint32)
+        cnt = C.c_size_t()
+        self._check(self._lib.sph_neighbors(self._h, int(pid), _u32p(out), cap, C.byref(cnt)),
+                    "sph_neighbors")
+        return out[:min(cap, cnt.value)].copy()
