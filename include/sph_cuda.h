@@ -204,6 +204,36 @@ int sph_read_grid(SphHandle *h, uint32_t *cell_linear, uint32_t *morton_key,
  * length, at most `cap` ids are written. */
 int sph_neighbors(SphHandle *h, uint32_t id, uint32_t *out, size_t cap, size_t *count);
 
+/* ---- neighbour grid without device allocation ------------------------- */
+/* No counterpart in the reference. For callers that cannot call cudaMalloc:
+ * a host engine that owns all device memory through its own pool or budget
+ * and lets no library allocate, or a caller whose other streams must not be
+ * stalled by the device synchronization that cudaMalloc/cudaFree can cause.
+ *
+ * Builds NeighborGrid::update (kernel/src/neighbor.rs:82-122) on the device
+ * from caller-owned device arrays: d_cell_index[n] (linear cell hash per
+ * particle), d_cell_offsets[C] and d_cell_counts[C] (exclusive scan and
+ * count per linear cell, C = product of the grid dims of NeighborGrid::new
+ * for domain_min/max and cell_size, which must not exceed cells_capacity),
+ * d_sorted[n] (particle indices grouped by cell, ascending within a cell).
+ * domain_min/max are host arrays; `stream` is a cudaStream_t (NULL = legacy
+ * default stream). The call returns after the stream has finished it.
+ *
+ * It allocates nothing: its scratch is a static device array of
+ * SPH_NOALLOC_MAX_CELLS cursors plus tile sums (2 MiB + 1 KiB) that every
+ * GPU which loads this library holds until the process exits. Grids with
+ * more than SPH_NOALLOC_MAX_CELLS cells, or a cell holding more than 1024
+ * particles, return SPH_ERR_CAPACITY. The first call on a device looks up
+ * the array's device address (with that device current); make that first
+ * call before any stream capture. All calls share the one array, so calls
+ * that overlap on the GPU (different streams or host threads, same device)
+ * race and must be serialized by the caller. */
+#define SPH_NOALLOC_MAX_CELLS (1u << 19)
+int sph_grid_sort_noalloc(const float *d_x, const float *d_y, const float *d_z, uint32_t n,
+                          const float domain_min[3], const float domain_max[3], float cell_size,
+                          uint32_t *d_cell_index, uint32_t *d_cell_offsets, uint32_t *d_cell_counts,
+                          uint32_t *d_sorted, size_t cells_capacity, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

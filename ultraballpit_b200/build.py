@@ -19,8 +19,8 @@ CSRC = os.path.join(PKG, "csrc")
 LIB_DIR = os.path.join(PKG, "lib")
 LIB_PATH = os.path.join(LIB_DIR, "libsph_cuda.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-SOURCES = ["sph_api.cu"]
-DEPS = ["sph_api.cu", "sph_kernels.cuh"]
+SOURCES = ["sph_api.cu", "sph_noalloc.cu"]
+DEPS = ["sph_api.cu", "sph_kernels.cuh", "sph_noalloc.cu"]
 
 
 def nvcc() -> str:

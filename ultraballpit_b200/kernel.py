@@ -39,7 +39,7 @@ EXPORTS = (
     "sph_read_boundary_pressure", "sph_error_metrics", "sph_particle_count",
     "sph_save_checkpoint", "sph_restore_checkpoint", "sph_synchronize", "sph_health",
     "sph_last_error", "sph_stream", "sph_launch_count", "sph_grid_info", "sph_read_grid",
-    "sph_neighbors",
+    "sph_neighbors", "sph_grid_sort_noalloc",
 )
 
 
