@@ -136,6 +136,30 @@ typedef struct SphStepProfile {
   float total_us;
 } SphStepProfile;
 
+/* Force and moment on a geometry from orchestrator force.rs:39-129
+ * (compute_surface_forces): FP64 sums over the SDF surface nodes, and the
+ * reference's own f32 sums in node order. Moments about the origin. */
+typedef struct SphSurfaceForce {
+  double force[3];
+  double moment[3];
+  float force_f32[3];
+  float moment_f32[3];
+  uint32_t nodes;        /* SDF nodes with -2h <= d <= 0 and a defined normal */
+  uint32_t active_nodes; /* of those, nodes with fluid in support */
+} SphSurfaceForce;
+
+/* Reaction of the fluid on a range of boundary particles (a body), FP64:
+ * pressure = the boundary pressure force (kernel/src/sph.rs:391-408) the
+ * fluid receives from them, negated; repulsion = likewise for
+ * boundary.rs:161-179; viscous = Monaghan viscosity with the body at rest
+ * (a diagnostic: the reference applies no wall viscosity). Moments about the
+ * origin, taken at the boundary particles. */
+typedef struct SphBodyForce {
+  double pressure_force[3], pressure_moment[3];
+  double repulsion_force[3], repulsion_moment[3];
+  double viscous_force[3], viscous_moment[3];
+} SphBodyForce;
+
 typedef struct SphGridInfo {
   uint32_t dims[3];
   uint32_t total_cells;
@@ -190,6 +214,17 @@ const char *sph_last_error(const SphHandle *h);
 void *sph_stream(SphHandle *h);
 /* Total kernels this handle has launched (graph replays counted per node). */
 uint64_t sph_launch_count(const SphHandle *h);
+
+/* ---- force extraction ------------------------------------------------- */
+/* Register the geometry SDF whose surface force sph_surface_forces returns
+ * (the obstacle's SDF, as orchestrator/src/force.rs uses it): selects the
+ * nodes with -2h <= d <= 0 and a nonzero gradient once, on the host. */
+int sph_set_geometry_sdf(SphHandle *h, const SphSdfView *sdf);
+/* compute_surface_forces(particles(), sdf, h) on the current state. */
+int sph_surface_forces(SphHandle *h, SphSurfaceForce *out);
+/* Fluid reaction on boundary particles [first, first + count) from the last
+ * force computation (boundary-particle mode). */
+int sph_body_force(SphHandle *h, uint32_t first, uint32_t count, SphBodyForce *out);
 
 /* ---- grid diagnostics (the bit-exact grid/sort checks) ---------------- */
 int sph_grid_info(SphHandle *h, SphGridInfo *out);

@@ -39,7 +39,9 @@ class OrcParams(C.Structure):
                 ("cfl_number", C.c_float), ("viscosity", C.c_float),
                 ("domain_min", C.c_float * 3), ("domain_max", C.c_float * 3),
                 ("alpha", C.c_float), ("beta", C.c_float), ("tier", C.c_int),
-                ("threads", C.c_int), ("pow_mode", C.c_int)]
+                ("threads", C.c_int), ("pow_mode", C.c_int), ("boundary_mode", C.c_int),
+                ("sdf_wall_coef", C.c_float), ("sdf_origin", C.c_float * 3), ("sdf_cell", C.c_float),
+                ("sdf_dims", C.c_uint32 * 3), ("sdf", C.POINTER(C.c_float))]
 
 
 def lib():
@@ -82,6 +84,14 @@ def lib():
         L.orc_sdf_sample.restype = C.c_float
         L.orc_sdf_sample.argtypes = [fp, u32p, fp, C.c_float, fp]
         L.orc_sdf_gradient.argtypes = [fp, u32p, fp, C.c_float, fp, fp]
+        L.orc_surface_forces.argtypes = [vp, fp, u32p, fp, C.c_float, fp, C.POINTER(C.c_double),
+                                         C.POINTER(C.c_uint32)]
+        L.orc_body_force.argtypes = [vp, C.c_uint32, C.c_uint32, C.POINTER(C.c_double)]
+        L.orc_wall_table.restype = C.c_int
+        L.orc_wall_table.argtypes = [C.c_float, fp, fp, fp]
+        L.orc_sdf_sample_clamped.restype = C.c_float
+        L.orc_sdf_sample_clamped.argtypes = [fp, u32p, fp, C.c_float, fp]
+        L.orc_sdf_gradient_clamped.argtypes = [fp, u32p, fp, C.c_float, fp, fp]
         _lib = L
     return _lib
 
@@ -164,6 +174,24 @@ def sdf_gradient(sdf, pt) -> np.ndarray:
     return out
 
 
+WALL_N = 512
+
+
+def wall_table(h):
+    """(phi, grad, inv_step) of the SDF wall at smoothing length h."""
+    phi = np.zeros(WALL_N + 1, np.float32)
+    grad = np.zeros(WALL_N + 1, np.float32)
+    inv = np.zeros(1, np.float32)
+    lib().orc_wall_table(h, _fp(phi), _fp(grad), _fp(inv))
+    return phi, grad, float(inv[0])
+
+
+def sdf_sample_clamped(sdf, pt) -> float:
+    dims = np.asarray(sdf.dimensions, np.uint32)
+    return lib().orc_sdf_sample_clamped(_fp(sdf.distances), _u32p(dims), _f3(sdf.origin), sdf.cell_size,
+                                        _f3(pt))
+
+
 def compute_timestep_arrays(p: ParticleArrays, h, c, cfl) -> float:
     return lib().orc_compute_timestep_arrays(len(p), *[_fp(getattr(p, f)) for f in
                                                        ("vx", "vy", "vz", "ax", "ay", "az")], h, c, cfl)
@@ -177,14 +205,23 @@ class OracleKernel:
     def __init__(self, particles: ParticleArrays, boundary: BoundaryParticles, h, gravity,
                  speed_of_sound, cfl_number, viscosity, domain_min, domain_max, *,
                  alpha: float = 1.0, beta: float = 2.0, tier: int = 1, threads: int = 1,
-                 pow_mode: int = 0):
+                 pow_mode: int = 0, boundary_mode: int = 0, sdf=None, sdf_wall_coef: float = 0.981):
         particles.validate()
         self._n = len(particles)
         self._nb = len(boundary)
         prm = OrcParams(h=h, gravity=_f3(gravity), speed_of_sound=speed_of_sound,
                         cfl_number=cfl_number, viscosity=viscosity, domain_min=_f3(domain_min),
                         domain_max=_f3(domain_max), alpha=alpha, beta=beta, tier=tier,
-                        threads=threads, pow_mode=pow_mode)
+                        threads=threads, pow_mode=pow_mode, boundary_mode=boundary_mode,
+                        sdf_wall_coef=sdf_wall_coef)
+        if boundary_mode == 1:
+            if sdf is None:
+                raise ValueError("boundary_mode 1 needs an sdf")
+            self._sdf = np.ascontiguousarray(sdf.distances, np.float32)
+            prm.sdf_origin = _f3(sdf.origin)
+            prm.sdf_cell = float(sdf.cell_size)
+            prm.sdf_dims = (C.c_uint32 * 3)(*map(int, sdf.dimensions))
+            prm.sdf = _fp(self._sdf)
         self.h, self.speed_of_sound = float(h), float(speed_of_sound)
         keep = [np.ascontiguousarray(getattr(particles, f), np.float32) for f in PARTICLE_FIELDS]
         fields = (C.POINTER(C.c_float) * 13)(*[_fp(a) for a in keep])
@@ -235,6 +272,26 @@ class OracleKernel:
 
     def restore_checkpoint(self) -> bool:
         return bool(lib().orc_restore_checkpoint(self._h))
+
+    def surface_forces(self, sdf) -> dict:
+        """force.rs:39-129 literally (f32) plus the same nodes summed in FP64."""
+        dims = np.asarray(sdf.dimensions, np.uint32)
+        dist = np.ascontiguousarray(sdf.distances, np.float32)
+        f32 = np.zeros(6, np.float32)
+        f64 = np.zeros(6, np.float64)
+        nodes = C.c_uint32()
+        lib().orc_surface_forces(self._h, _fp(dist), _u32p(dims), _f3(sdf.origin), sdf.cell_size, _fp(f32),
+                                 f64.ctypes.data_as(C.POINTER(C.c_double)), C.byref(nodes))
+        return dict(force_f32=f32[:3], moment_f32=f32[3:], force=f64[:3], moment=f64[3:], nodes=nodes.value)
+
+    def body_force(self, first: int, count: int) -> dict:
+        """Fluid reaction on boundary particles [first, first + count) from
+        the last force computation."""
+        out = np.zeros(18, np.float64)
+        lib().orc_body_force(self._h, first, count, out.ctypes.data_as(C.POINTER(C.c_double)))
+        keys = ("pressure_force", "pressure_moment", "repulsion_force", "repulsion_moment", "viscous_force",
+                "viscous_moment")
+        return {k: out[3 * i:3 * i + 3] for i, k in enumerate(keys)}
 
     def boundary_list_size(self) -> int:
         return int(lib().orc_boundary_list_size(self._h))

@@ -260,7 +260,113 @@ struct OrcParams {
   int tier;      // 0 = literal, 1 = grid
   int threads;   // worker threads for Tier G loops (results do not depend on it)
   int pow_mode;  // 0 = libm powf (reference on Linux), 1 = correctly rounded
+  int boundary_mode;      // 0 = boundary particles (reference), 1 = SDF wall (tier S)
+  float sdf_wall_coef;    // SDF wall repulsion scale
+  float sdf_origin[3];
+  float sdf_cell;
+  uint32_t sdf_dims[3];
+  const float* sdf;       // node grid, i*ny*nz + j*nz + k (copied at creation)
 };
+
+// ---- Tier S: SDF wall (no reference counterpart; project definition) ----
+// The SDF wall stands in for the reference's 3 layers of wall particles
+// (orchestrator domain.rs:162-348: depths (layer + 0.5) dx behind the surface,
+// lattice spacing dx = h / 1.3, mass rho0 dx^3), homogenised along the wall:
+// for a particle at distance d in front of a plane wall, phi(d) is the
+// lattice sum of W * dx^3 over those layers and g(d) the sum of -dW/dn dx^3,
+// both averaged over 8 x 8 lateral offsets of the lattice. Tabulated at
+// kWallN + 1 points on [0, 2h] in double, rounded to f32, linearly
+// interpolated in f32.
+constexpr int kWallN = 512;
+struct WallTable {
+  float inv_step = 0.0f;
+  std::vector<float> phi, grad;
+};
+
+inline WallTable make_wall_table(float hf) {
+  WallTable t;
+  const double h = hf, dx = h / 1.3, sup = 2.0 * h;
+  const double C0 = 21.0 / (16.0 * 3.14159265358979323846);
+  const int M = (int)std::ceil(sup / dx) + 1;
+  t.phi.assign(kWallN + 1, 0.0f);
+  t.grad.assign(kWallN + 1, 0.0f);
+  for (int k = 0; k <= kWallN; ++k) {
+    double d = (double)k * (sup / kWallN);
+    double sw = 0.0, sg = 0.0;
+    for (int a = 0; a < 8; ++a)
+      for (int b = 0; b < 8; ++b) {
+        double ox = (a + 0.5) / 8.0 * dx, oy = (b + 0.5) / 8.0 * dx;
+        for (int layer = 0; layer < 3; ++layer) {
+          double z = d + (layer + 0.5) * dx;
+          for (int ix = -M; ix <= M; ++ix)
+            for (int iy = -M; iy <= M; ++iy) {
+              double X = ix * dx + ox, Y = iy * dx + oy;
+              double r = std::sqrt(X * X + Y * Y + z * z);
+              if (r >= sup) continue;
+              double q = r / h, om = 1.0 - 0.5 * q;
+              sw += C0 / (h * h * h) * om * om * om * om * (1.0 + 2.0 * q);
+              sg += C0 / (h * h * h * h) * 5.0 * q * om * om * om * (z / r);
+            }
+        }
+      }
+    double vol = dx * dx * dx / 64.0;
+    t.phi[k] = (float)(sw * vol);
+    t.grad[k] = (float)(sg * vol);
+  }
+  t.inv_step = (float)((double)kWallN / sup);
+  return t;
+}
+
+// Linear interpolation of a wall table at distance d (clamped to [0, 2h]).
+inline float wall_lookup(const std::vector<float>& v, float inv_step, float d) {
+  float u = fmaxf(d, 0.0f) * inv_step;
+  if (!(u < (float)kWallN)) return 0.0f;
+  int i = (int)u;
+  float f = u - (float)i;
+  return v[i] + f * (v[i + 1] - v[i]);
+}
+
+// GridSDF::sample (geometry.rs:99-150) with the grid coordinate clamped to
+// [0, dims-1-1e-3] so that points on or beyond the outer nodes still
+// interpolate in the last cell instead of returning f32::MAX.
+inline float sdf_sample_clamped(const float* d, const uint32_t dims[3], const float origin[3],
+                                float cell, float px, float py, float pz) {
+  float g[3] = {(px - origin[0]) / cell, (py - origin[1]) / cell, (pz - origin[2]) / cell};
+  int i0[3];
+  float fr[3];
+  for (int a = 0; a < 3; ++a) {
+    g[a] = fminf(fmaxf(g[a], 0.0f), (float)(dims[a] - 1) - 0.001f);
+    i0[a] = (int)floorf(g[a]);
+    fr[a] = g[a] - (float)i0[a];
+  }
+  uint32_t ny = dims[1], nz = dims[2];
+  auto at = [&](int di, int dj, int dk) {
+    return d[(uint64_t)(i0[0] + di) * ny * nz + (uint64_t)(i0[1] + dj) * nz + (uint64_t)(i0[2] + dk)];
+  };
+  float fx = fr[0], fy = fr[1], fz = fr[2];
+  float c00 = at(0, 0, 0) * (1.0f - fz) + at(0, 0, 1) * fz;
+  float c01 = at(0, 1, 0) * (1.0f - fz) + at(0, 1, 1) * fz;
+  float c10 = at(1, 0, 0) * (1.0f - fz) + at(1, 0, 1) * fz;
+  float c11 = at(1, 1, 0) * (1.0f - fz) + at(1, 1, 1) * fz;
+  float c0 = c00 * (1.0f - fy) + c01 * fy;
+  float c1 = c10 * (1.0f - fy) + c11 * fy;
+  return c0 * (1.0f - fx) + c1 * fx;
+}
+
+// GridSDF::gradient (geometry.rs:153-175) on the clamped sampler.
+inline void sdf_gradient_clamped(const float* d, const uint32_t dims[3], const float origin[3],
+                                 float cell, float px, float py, float pz, float out[3]) {
+  float h = cell * 0.5f;
+  float gx = (sdf_sample_clamped(d, dims, origin, cell, px + h, py, pz) -
+              sdf_sample_clamped(d, dims, origin, cell, px - h, py, pz)) / (2.0f * h);
+  float gy = (sdf_sample_clamped(d, dims, origin, cell, px, py + h, pz) -
+              sdf_sample_clamped(d, dims, origin, cell, px, py - h, pz)) / (2.0f * h);
+  float gz = (sdf_sample_clamped(d, dims, origin, cell, px, py, pz + h) -
+              sdf_sample_clamped(d, dims, origin, cell, px, py, pz - h)) / (2.0f * h);
+  float mag = sqrtf(gx * gx + gy * gy + gz * gz);
+  if (mag > 1e-8f) { out[0] = gx / mag; out[1] = gy / mag; out[2] = gz / mag; }
+  else { out[0] = 0.0f; out[1] = 0.0f; out[2] = 0.0f; }
+}
 
 class Kernel {
  public:
@@ -274,6 +380,9 @@ class Kernel {
   Particles checkpoint;
   // Tier G: static boundary candidate lists per fluid cell (ascending b).
   std::vector<uint32_t> bc_start, bc_list;
+  std::vector<float> vx_used, vy_used, vz_used;  // velocities seen by the last compute_forces
+  std::vector<float> sdf;  // tier S node grid
+  WallTable wall;          // tier S wall table
 
   // lib.rs:138-174
   Kernel(const OrcParams& pr, Particles&& parts, Boundary&& bnd)
@@ -283,7 +392,17 @@ class Kernel {
     for (size_t i = 0; i < p.len(); ++i) m += (double)p.mass[i];
     initial_mass = m;
     initial_energy = total_energy();
-    if (prm.tier == 1) build_boundary_lists();
+    if (prm.boundary_mode == 1 && prm.sdf) {
+      sdf.assign(prm.sdf, prm.sdf + (size_t)prm.sdf_dims[0] * prm.sdf_dims[1] * prm.sdf_dims[2]);
+      prm.sdf = sdf.data();
+      wall = make_wall_table(prm.h);
+    }
+    if (prm.tier == 1 && prm.boundary_mode == 0) build_boundary_lists();
+  }
+
+  bool sdf_mode() const { return prm.boundary_mode == 1; }
+  float wall_distance(size_t i) const {
+    return sdf_sample_clamped(prm.sdf, prm.sdf_dims, prm.sdf_origin, prm.sdf_cell, p.x[i], p.y[i], p.z[i]);
   }
 
   // lib.rs:177-194
@@ -347,6 +466,7 @@ class Kernel {
   // ascending boundary index (Tier L: all of them).
   template <class F>
   inline void for_each_boundary(size_t i, F&& f) const {
+    if (sdf_mode()) return;
     if (prm.tier == 0) {
       for (size_t bi = 0; bi < b.len(); ++bi) f(bi);
     } else {
@@ -403,6 +523,13 @@ class Kernel {
         float r = sqrtf(dx * dx + dy * dy + dz * dz);
         if (r < support) rho += b.mass[bi] * wendland_c2(r, h);
       });
+      if (sdf_mode()) {  // tier S: kernel mass of the wall half-space
+        float d = wall_distance(i);
+        if (d < support) {
+          float rest = p.fluid_type[i] == 0 ? kWaterRho0 : kAirRho0;
+          rho += rest * wall_lookup(wall.phi, wall.inv_step, d);
+        }
+      }
       out[i] = rho;
     });
     p.density.swap(out);
@@ -567,12 +694,13 @@ class Kernel {
   // lib.rs:203-283
   void compute_forces(float dt) {
     size_t n = p.len();
+    vx_used = p.vx; vy_used = p.vy; vz_used = p.vz;
     grid.update(p.x.data(), p.y.data(), p.z.data(), n);
     std::vector<float> diffusion = density_diffusion();
     compute_density();
     for (size_t i = 0; i < n; ++i) p.density[i] += diffusion[i] * dt;
     compute_pressure();
-    update_boundary_pressures();
+    if (!sdf_mode()) update_boundary_pressures();
     for (size_t i = 0; i < n; ++i) { p.ax[i] = 0.0f; p.ay[i] = 0.0f; p.az[i] = 0.0f; }
     compute_pressure_forces();
     compute_viscous_forces();
@@ -581,7 +709,42 @@ class Kernel {
       p.ay[i] += prm.gravity[1];
       p.az[i] += prm.gravity[2];
     }
-    compute_repulsive_forces();
+    if (sdf_mode()) compute_sdf_wall_forces();
+    else compute_repulsive_forces();
+  }
+
+  // Tier S wall force, after gravity: the boundary pressure force of the
+  // homogenised wall layers along the SDF normal with the mirrored pressure
+  // p_w = max(max(p_i, 0) + rho_i g.(r_w - r_i), 0), r_w taken at the middle
+  // layer (d + 1.5 dx behind the particle, boundary.rs:117-119), then the
+  // near-wall repulsion.
+  void compute_sdf_wall_forces() {
+    float h = prm.h, support = 2.0f * h, r0 = 0.5f * h;
+    float mid = 1.5f * (h / 1.3f);
+    const float* g = prm.gravity;
+    parallel_for(p.len(), nthreads(), 256, [&](size_t i) {
+      float d = wall_distance(i);
+      if (!(d < support)) return;
+      float n[3];
+      sdf_gradient_clamped(prm.sdf, prm.sdf_dims, prm.sdf_origin, prm.sdf_cell, p.x[i], p.y[i], p.z[i], n);
+      float rest = p.fluid_type[i] == 0 ? kWaterRho0 : kAirRho0;
+      float pic = fmaxf(p.pressure[i], 0.0f);
+      float depth = -(d + mid);
+      float g_dot_dr = g[0] * (depth * n[0]) + g[1] * (depth * n[1]) + g[2] * (depth * n[2]);
+      float pw = fmaxf(pic + p.density[i] * g_dot_dr, 0.0f);
+      float coef = (pic / (p.density[i] * p.density[i]) + pw / (rest * rest)) * rest *
+                   wall_lookup(wall.grad, wall.inv_step, d);
+      p.ax[i] += coef * n[0];
+      p.ay[i] += coef * n[1];
+      p.az[i] += coef * n[2];
+      if (d < r0) {
+        float s = 1.0f - fmaxf(d, 0.0f) / r0;
+        float fm = prm.sdf_wall_coef * s * s / r0;
+        p.ax[i] += fm * n[0];
+        p.ay[i] += fm * n[1];
+        p.az[i] += fm * n[2];
+      }
+    });
   }
 
   // sph.rs:236-280
@@ -872,6 +1035,131 @@ float orc_compute_timestep_arrays(size_t n, const float* vx, const float* vy, co
   p.ax.assign(ax, ax + n); p.ay.assign(ay, ay + n); p.az.assign(az, az + n);
   p.x.resize(n);
   return compute_timestep(p, h, c, cfl);
+}
+
+// ---- force extraction ---------------------------------------------------
+// orchestrator force.rs:39-129, literal: f32 sums over nodes in (i,j,k)
+// order with brute-force particle loops; out_f32[6] = force, moment. Also
+// the same per-node contributions summed in FP64 (out_f64[6]).
+void orc_surface_forces(void* kp, const float* d, const uint32_t* dims, const float* origin, float cell,
+                        float* out_f32, double* out_f64, uint32_t* nodes) {
+  Kernel* k = static_cast<Kernel*>(kp);
+  const Particles& p = k->p;
+  float h = k->prm.h;
+  float surface_threshold = 2.0f * h;
+  float d_area = cell * cell;
+  float nf[3] = {0, 0, 0}, nm[3] = {0, 0, 0};
+  double df[3] = {0, 0, 0}, dm[3] = {0, 0, 0};
+  uint32_t cnt = 0;
+  for (uint32_t i = 0; i < dims[0]; ++i)
+    for (uint32_t j = 0; j < dims[1]; ++j)
+      for (uint32_t kk = 0; kk < dims[2]; ++kk) {
+        float pt[3] = {origin[0] + (float)i * cell, origin[1] + (float)j * cell, origin[2] + (float)kk * cell};
+        float dist = sdf_sample(d, dims, origin, cell, pt);
+        if (fabsf(dist) > surface_threshold || dist > 0.0f) continue;
+        float n[3];
+        sdf_gradient(d, dims, origin, cell, pt, n);
+        float nmag = sqrtf(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
+        if (nmag < 1e-8f) continue;
+        ++cnt;
+        float lp = 0.0f, ws = 0.0f;
+        for (size_t q = 0; q < p.len(); ++q) {
+          float dx = p.x[q] - pt[0], dy = p.y[q] - pt[1], dz = p.z[q] - pt[2];
+          float r = sqrtf(dx * dx + dy * dy + dz * dz);
+          if (r < 2.0f * h) {
+            float w = wendland_c2(r, h);
+            lp += p.pressure[q] * w;
+            ws += w;
+          }
+        }
+        if (ws > 1e-12f) {
+          lp /= ws;
+          float fx = -lp * n[0] * d_area, fy = -lp * n[1] * d_area, fz = -lp * n[2] * d_area;
+          float mx = pt[1] * fz - pt[2] * fy, my = pt[2] * fx - pt[0] * fz, mz = pt[0] * fy - pt[1] * fx;
+          nf[0] += fx; nf[1] += fy; nf[2] += fz;
+          nm[0] += mx; nm[1] += my; nm[2] += mz;
+          df[0] += fx; df[1] += fy; df[2] += fz;
+          dm[0] += mx; dm[1] += my; dm[2] += mz;
+        }
+      }
+  for (int a = 0; a < 3; ++a) {
+    out_f32[a] = nf[a]; out_f32[3 + a] = nm[a];
+    out_f64[a] = df[a]; out_f64[3 + a] = dm[a];
+  }
+  *nodes = cnt;
+}
+
+// Fluid reaction on boundary particles [first, first+count) from the last
+// force computation (the negated terms of sph.rs:391-408 and
+// boundary.rs:161-179; viscous: Monaghan with the body at rest). 18 doubles:
+// pressure F, M; repulsion F, M; viscous F, M.
+void orc_body_force(void* kp, uint32_t first, uint32_t count, double* out) {
+  Kernel* k = static_cast<Kernel*>(kp);
+  const float* vx_used = k->vx_used.data();
+  const float* vy_used = k->vy_used.data();
+  const float* vz_used = k->vz_used.data();
+  const Particles& p = k->p;
+  const Boundary& b = k->b;
+  float h = k->prm.h, support = 2.0f * h, r0 = 0.5f * h, eta_sq = 0.01f * h * h;
+  float dconst = 10.0f * 9.81f * 0.01f;
+  float nac = -k->prm.alpha * k->prm.speed_of_sound;
+  for (int c = 0; c < 18; ++c) out[c] = 0.0;
+  for (size_t i = 0; i < p.len(); ++i) {
+    float rest = p.fluid_type[i] == 0 ? kWaterRho0 : kAirRho0;
+    float pic_over = fmaxf(p.pressure[i], 0.0f) / (p.density[i] * p.density[i]);
+    for (uint32_t bi = first; bi < first + count; ++bi) {
+      float dx = p.x[i] - b.x[bi], dy = p.y[i] - b.y[bi], dz = p.z[i] - b.z[bi];
+      float r = sqrtf(dx * dx + dy * dy + dz * dz);
+      if (!(r < support)) continue;
+      float g[3];
+      wendland_c2_gradient(dx, dy, dz, r, h, &g[0], &g[1], &g[2]);
+      float factor = -p.mass[i] * b.mass[bi] * (pic_over + b.pressure[bi] / (rest * rest));
+      double F[3] = {-(double)(factor * g[0]), -(double)(factor * g[1]), -(double)(factor * g[2])};
+      double R[3] = {0, 0, 0};
+      if (r < r0 && r > 1.0e-12f) {
+        float s = 1.0f - r / r0;
+        float fm = dconst * s * s / r0;
+        float inv_r = 1.0f / r;
+        R[0] = -(double)p.mass[i] * (double)(fm * dx * inv_r);
+        R[1] = -(double)p.mass[i] * (double)(fm * dy * inv_r);
+        R[2] = -(double)p.mass[i] * (double)(fm * dz * inv_r);
+      }
+      double V[3] = {0, 0, 0};
+      float vr = vx_used[i] * dx + vy_used[i] * dy + vz_used[i] * dz;
+      if (vr < 0.0f) {
+        float mu = h * vr / (r * r + eta_sq);
+        float pij = (nac * mu + k->prm.beta * mu * mu) / (0.5f * (p.density[i] + rest));
+        float fv = -p.mass[i] * b.mass[bi] * pij;
+        V[0] = -(double)(fv * g[0]); V[1] = -(double)(fv * g[1]); V[2] = -(double)(fv * g[2]);
+      }
+      double X[3] = {b.x[bi], b.y[bi], b.z[bi]};
+      const double* G[3] = {F, R, V};
+      for (int t = 0; t < 3; ++t) {
+        out[6 * t + 0] += G[t][0]; out[6 * t + 1] += G[t][1]; out[6 * t + 2] += G[t][2];
+        out[6 * t + 3] += X[1] * G[t][2] - X[2] * G[t][1];
+        out[6 * t + 4] += X[2] * G[t][0] - X[0] * G[t][2];
+        out[6 * t + 5] += X[0] * G[t][1] - X[1] * G[t][0];
+      }
+    }
+  }
+}
+
+// ---- Tier S helpers -----------------------------------------------------
+// Wall tables for smoothing length h: kWallN + 1 entries each.
+int orc_wall_table(float h, float* phi, float* grad, float* inv_step) {
+  WallTable t = make_wall_table(h);
+  std::memcpy(phi, t.phi.data(), t.phi.size() * 4);
+  std::memcpy(grad, t.grad.data(), t.grad.size() * 4);
+  *inv_step = t.inv_step;
+  return kWallN;
+}
+float orc_sdf_sample_clamped(const float* d, const uint32_t* dims, const float* origin, float cell,
+                             const float* pt) {
+  return sdf_sample_clamped(d, dims, origin, cell, pt[0], pt[1], pt[2]);
+}
+void orc_sdf_gradient_clamped(const float* d, const uint32_t* dims, const float* origin, float cell,
+                              const float* pt, float* out3) {
+  sdf_gradient_clamped(d, dims, origin, cell, pt[0], pt[1], pt[2], out3);
 }
 
 // ---- GridSDF ------------------------------------------------------------

@@ -296,3 +296,52 @@ def test_dam_break_builder_counts():
     # jitter stays within 0.01 dx of the lattice
     lat = (np.arange(25, dtype=np.float32) + f32(0.5)) * f32(0.004)
     assert np.max(np.abs(sc.particles.x.reshape(25, 50, 25)[:, 0, 0] - lat)) <= 0.01 * 0.004 + 1e-9
+
+
+# ---- SDF wall mode (no reference counterpart; project definition) ----------------
+
+def test_wall_table_matches_lattice_sums():
+    """The SDF wall table equals the reference's 3 wall layers, averaged over
+    lateral offsets (numpy restatement, float64)."""
+    h = 0.0052
+    dx = h / 1.3
+    C0 = 21.0 / (16.0 * np.pi)
+    phi, grad, inv = orc.wall_table(np.float32(h))
+    L = np.arange(-4, 5) * dx
+    offs = (np.arange(8) + 0.5) / 8.0 * dx
+    for k in (0, 60, 128, 300, 511):
+        d = k * (2 * h / 512)
+        sw = sg = 0.0
+        for ox in offs:
+            for oy in offs:
+                X, Y = np.meshgrid(L + ox, L + oy, indexing="ij")
+                for layer in range(3):
+                    z = d + (layer + 0.5) * dx
+                    r = np.sqrt(X * X + Y * Y + z * z)
+                    q = r / h
+                    m = r < 2 * h
+                    om = 1 - 0.5 * q[m]
+                    sw += np.sum(C0 / h ** 3 * om ** 4 * (1 + 2 * q[m]))
+                    sg += np.sum(C0 / h ** 4 * 5 * q[m] * om ** 3 * z / r[m])
+        assert abs(phi[k] - sw * dx ** 3 / 64) <= 1e-6 * max(1.0, abs(phi[k]))
+        assert abs(grad[k] - sg * dx ** 3 / 64) <= 1e-5 * max(1.0, abs(grad[k]))
+    assert phi[-1] == 0.0 and grad[-1] == 0.0
+    assert np.all(np.diff(phi) <= 0)
+
+
+def test_sdf_mode_tank_settles_with_hydrostatic_ordering():
+    """A water block resting on the SDF floor of a closed box (tier S)."""
+    sc = domain.dam_break(0.004, seed=21, block=(0.04, 0.04, 0.04), domain_max=(0.04, 0.04, 0.08))
+    k = orc.OracleKernel(*sc.kernel_args(), alpha=sc.alpha, tier=1, threads=4, pow_mode=1,
+                         boundary_mode=1, sdf=sc.sdf)
+    for _ in range(400):
+        k.step(k.compute_timestep(sc.cfl_number))
+    p = k.particles()
+    assert np.all(np.isfinite(p.z)) and p.z.min() >= 0.0
+    order = np.argsort(p.z, kind="stable")
+    q = len(p) // 4
+    assert p.pressure[order[:q]].mean() > p.pressure[order[-q:]].mean()
+    # the wall density term keeps the bottom layer near rest density, and the
+    # column stays near its initial height as with the reference's wall particles
+    assert abs(np.median(p.density[order[:q]]) - 1000.0) < 30.0
+    assert p.z.max() < 0.043

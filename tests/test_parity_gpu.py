@@ -252,3 +252,47 @@ def test_dam_break_sphere_2m_particles_one_step_bit_exact_and_invariants():
         v = getattr(p, f)
         assert v.min() >= sc.domain_min[k] and v.max() <= sc.domain_max[k]
     assert gpu.error_metrics().mass_conservation == 0.0
+
+
+# ---- SDF wall mode -------------------------------------------------------------------
+
+def test_sdf_mode_bit_exact_with_sphere():
+    from ultraballpit_b200.kernel import BOUNDARY_SDF
+    sc = domain.dam_break(0.004, seed=31, sphere=True)
+    args = sc.kernel_args()
+    gpu = CudaKernel(*args, alpha=sc.alpha, boundary_mode=BOUNDARY_SDF, sdf=sc.sdf)
+    cpu = orc.OracleKernel(*args, alpha=sc.alpha, tier=1, threads=8, pow_mode=1, boundary_mode=1,
+                           sdf=sc.sdf)
+    for _ in range(20):
+        dt = cpu.compute_timestep(sc.cfl_number)
+        assert gpu.compute_timestep() == dt
+        gpu.step(dt)
+        cpu.step(dt)
+    assert_same(gpu.particles(), cpu.particles())
+
+
+# ---- force extraction on the sphere (BASELINE config 2 reports these) ------------
+
+def test_surface_and_body_forces_on_sphere():
+    sc = domain.tank_with_sphere(0.004, seed=41, velocity=(0.3, 0.0, 0.0))
+    sph = sc.extras["sphere_sdf"]
+    nb_geo = sc.extras["n_geometry_boundary"]
+    first = len(sc.boundary) - nb_geo
+    gpu, cpu = make_pair(sc)
+    gpu.set_geometry_sdf(sph)
+    for _ in range(10):
+        dt = cpu.compute_timestep(sc.cfl_number)
+        gpu.step(dt)
+        cpu.step(dt)
+    assert_same(gpu.particles(), cpu.particles())
+    g = gpu.surface_forces()
+    assert g["active_nodes"] > 0
+    c = cpu.surface_forces(sph)
+    assert g["nodes"] == c["nodes"] > 0
+    np.testing.assert_array_equal(g["force_f32"], c["force_f32"])
+    np.testing.assert_array_equal(g["moment_f32"], c["moment_f32"])
+    np.testing.assert_allclose(g["force"], c["force"], rtol=1e-12, atol=1e-12)
+    np.testing.assert_allclose(g["moment"], c["moment"], rtol=1e-12, atol=1e-12)
+    gb, cb = gpu.body_force(first, nb_geo), cpu.body_force(first, nb_geo)
+    for key in gb:
+        np.testing.assert_allclose(gb[key], cb[key], rtol=1e-9, atol=1e-15, err_msg=key)

@@ -41,6 +41,7 @@ struct SphHandle {
   bool needs_init = true;
   bool red_valid = false;
   bool has_ck = false;
+  bool list_valid = false;  // nbr holds the in-support lists of the current grid/positions
   uint64_t launches = 0;
   int body_kernels = 0;
   uint64_t boundary_candidates = 0;
@@ -58,10 +59,15 @@ struct SphHandle {
   uint32_t *rank_of_lin = nullptr, *lin_of_rank = nullptr;
   uint2* ctab = nullptr;
   int nbsum = 0;
+  // neighbour lists recorded by k_density: nbr[c * n + i], count per particle
+  uint32_t *nbr = nullptr, *ncount = nullptr;
   // boundary
   float4* bpos = nullptr;
   float* bpress = nullptr;
   uint32_t *bc_start = nullptr, *bc_list = nullptr;
+  // SDF node grid and wall table (boundary_mode SPH_BOUNDARY_SDF)
+  float* sdf = nullptr;
+  float2* wall_tab = nullptr;
   // scalars
   float *dt = nullptr, *dt_query = nullptr, *red = nullptr;
   uint32_t* err = nullptr;
@@ -79,6 +85,15 @@ struct SphHandle {
   uint8_t* stage_ft = nullptr;
   // diagnostics scratch
   uint32_t* diag = nullptr;
+  // geometry for force extraction
+  float4 *geo_pos = nullptr, *geo_nrm = nullptr;
+  float* geo_out = nullptr;
+  double* geo_sum = nullptr;
+  int geo_nodes = 0;
+  float geo_area = 0.0f;
+  double* body_part = nullptr;
+  double* body_sum = nullptr;
+  int body_parts = 0;
   // graphs
   cudaGraphExec_t g_step = nullptr;
   cudaGraphExec_t g_auto = nullptr;
@@ -120,6 +135,23 @@ uint64_t spread21(uint64_t v) {
   return r;
 }
 
+// Largest float t with sqrtf(t) < s (sqrtf is correctly rounded on host and
+// device, and monotone), so that sqrtf(d2) < s  <=>  d2 <= t.
+float sqrt_below(float s) {
+  float t = s * s;
+  while (t > 0.0f && !(std::sqrt(t) < s)) t = std::nextafter(t, 0.0f);
+  while (std::sqrt(std::nextafter(t, INFINITY)) < s) t = std::nextafter(t, INFINITY);
+  return t;
+}
+
+// Largest float t with sqrtf(t) <= s, so that sqrtf(d2) > s  <=>  d2 > t.
+float sqrt_at_most(float s) {
+  float t = s * s;
+  while (t > 0.0f && !(std::sqrt(t) <= s)) t = std::nextafter(t, 0.0f);
+  while (std::sqrt(std::nextafter(t, INFINITY)) <= s) t = std::nextafter(t, INFINITY);
+  return t;
+}
+
 // Step constants rounded in f32 as the reference evaluates them.
 SimConst make_const(const SphParams& p, const uint32_t dims[3]) {
   SimConst k{};
@@ -152,7 +184,79 @@ SimConst make_const(const SphParams& p, const uint32_t dims[3]) {
   k.reach = (float)(2.0 * (double)h * (1.0 + 1e-4) + 1e-4 * (double)k.cell);
   k.sdf_coef = p.sdf_wall_coef;
   k.flags = p.flags;
+  k.sup_d2 = sqrt_below(k.support);
+  k.r0_d2 = sqrt_below(k.r0);
+  k.tiny_d2 = sqrt_at_most(1.0e-12f);
   return k;
+}
+
+// SDF wall table: for a particle at distance d in front of a plane wall, the
+// sums over the reference's 3 wall layers (depths (layer + 0.5) dx, lattice
+// spacing dx = h / 1.3, orchestrator domain.rs:162-348) of W dx^3 and of
+// -dW/dn dx^3, averaged over 8 x 8 lateral lattice offsets, at kWallN + 1
+// distances on [0, 2h]; evaluated in double and rounded to f32.
+std::vector<float2> make_wall_table(float hf, float* inv_step) {
+  const int N = sph::kWallN;
+  std::vector<float2> t(N + 1);
+  const double h = hf, dx = h / 1.3, sup = 2.0 * h;
+  const double C0 = 21.0 / (16.0 * 3.14159265358979323846);
+  const int M = (int)std::ceil(sup / dx) + 1;
+  for (int k = 0; k <= N; ++k) {
+    double d = (double)k * (sup / N);
+    double sw = 0.0, sg = 0.0;
+    for (int a = 0; a < 8; ++a)
+      for (int b = 0; b < 8; ++b) {
+        double ox = (a + 0.5) / 8.0 * dx, oy = (b + 0.5) / 8.0 * dx;
+        for (int layer = 0; layer < 3; ++layer) {
+          double z = d + (layer + 0.5) * dx;
+          for (int ix = -M; ix <= M; ++ix)
+            for (int iy = -M; iy <= M; ++iy) {
+              double X = ix * dx + ox, Y = iy * dx + oy;
+              double r = std::sqrt(X * X + Y * Y + z * z);
+              if (r >= sup) continue;
+              double q = r / h, om = 1.0 - 0.5 * q;
+              sw += C0 / (h * h * h) * om * om * om * om * (1.0 + 2.0 * q);
+              sg += C0 / (h * h * h * h) * 5.0 * q * om * om * om * (z / r);
+            }
+        }
+      }
+    double vol = dx * dx * dx / 64.0;
+    t[k] = make_float2((float)(sw * vol), (float)(sg * vol));
+  }
+  *inv_step = (float)((double)N / sup);
+  return t;
+}
+
+// GridSDF::sample and ::gradient (orchestrator geometry.rs:99-181), f32.
+float host_sdf_get(const SphSdfView& g, int i, int j, int k) {
+  uint64_t idx = (uint64_t)((uint32_t)i * g.dims[1] * g.dims[2] + (uint32_t)j * g.dims[2] + (uint32_t)k);
+  uint64_t total = (uint64_t)g.dims[0] * g.dims[1] * g.dims[2];
+  return idx < total ? g.distances[idx] : 3.40282347e38f;
+}
+float host_sdf_sample(const SphSdfView& g, float px, float py, float pz) {
+  float gx = (px - g.origin[0]) / g.cell_size, gy = (py - g.origin[1]) / g.cell_size;
+  float gz = (pz - g.origin[2]) / g.cell_size;
+  int i0 = (int)std::floor(gx), j0 = (int)std::floor(gy), k0 = (int)std::floor(gz);
+  if (i0 < 0 || j0 < 0 || k0 < 0) return 3.40282347e38f;
+  int i1 = i0 + 1, j1 = j0 + 1, k1 = k0 + 1;
+  if (i1 >= (int)g.dims[0] || j1 >= (int)g.dims[1] || k1 >= (int)g.dims[2]) return 3.40282347e38f;
+  float fx = gx - (float)i0, fy = gy - (float)j0, fz = gz - (float)k0;
+  float c00 = host_sdf_get(g, i0, j0, k0) * (1.0f - fz) + host_sdf_get(g, i0, j0, k1) * fz;
+  float c01 = host_sdf_get(g, i0, j1, k0) * (1.0f - fz) + host_sdf_get(g, i0, j1, k1) * fz;
+  float c10 = host_sdf_get(g, i1, j0, k0) * (1.0f - fz) + host_sdf_get(g, i1, j0, k1) * fz;
+  float c11 = host_sdf_get(g, i1, j1, k0) * (1.0f - fz) + host_sdf_get(g, i1, j1, k1) * fz;
+  float c0 = c00 * (1.0f - fy) + c01 * fy;
+  float c1 = c10 * (1.0f - fy) + c11 * fy;
+  return c0 * (1.0f - fx) + c1 * fx;
+}
+void host_sdf_gradient(const SphSdfView& g, float px, float py, float pz, float out[3]) {
+  float h = g.cell_size * 0.5f;
+  float dx = (host_sdf_sample(g, px + h, py, pz) - host_sdf_sample(g, px - h, py, pz)) / (2.0f * h);
+  float dy = (host_sdf_sample(g, px, py + h, pz) - host_sdf_sample(g, px, py - h, pz)) / (2.0f * h);
+  float dz = (host_sdf_sample(g, px, py, pz + h) - host_sdf_sample(g, px, py, pz - h)) / (2.0f * h);
+  float mag = std::sqrt(dx * dx + dy * dy + dz * dz);
+  if (mag > 1e-8f) { out[0] = dx / mag; out[1] = dy / mag; out[2] = dz / mag; }
+  else { out[0] = 0.0f; out[1] = 0.0f; out[2] = 0.0f; }
 }
 
 // Static per-cell candidate lists of boundary particles, ascending index. A
@@ -221,7 +325,7 @@ void enqueue_density_adami(SphHandle* h) {
   using namespace sph;
   k_density<<<grid_for(h->n, 256), 256, 0, h->st>>>(h->k, h->n, h->dt, h->pos, h->rv, h->id, h->ctab,
                                                     h->bc_start, h->bc_list, h->bpos, h->rf, h->pr,
-                                                    h->err);
+                                                    h->err, h->nbr, h->ncount, h->sdf, h->wall_tab);
   h->launches += 1;
   if (h->nb > 0) {
     k_adami<<<grid_for(h->nb, kAdamiWarps), kAdamiWarps * 32, 0, h->st>>>(
@@ -236,15 +340,16 @@ void enqueue_forces(SphHandle* h, float hdt_scale) {
   k_forces<<<grid_for(h->n, 256), 256, 0, h->st>>>(h->k, h->n, h->dt, hdt_scale, h->pos, h->vel, h->rf,
                                                    h->pr, h->id, h->ctab, h->bc_start, h->bc_list,
                                                    h->bpos, h->bpress, h->acc, h->velout, h->red,
-                                                   h->err);
+                                                   h->err, h->nbr, h->ncount, h->sdf, h->wall_tab);
   h->launches += 1;
 }
 
-void enqueue_xsph_sort(SphHandle* h) {
+void enqueue_xsph_sort(SphHandle* h, bool use_list) {
   using namespace sph;
   k_xsph_drift<<<grid_for(h->n, 256), 256, 0, h->st>>>(h->k, h->n, h->dt, h->pos, h->velout, h->acc,
                                                        h->id, h->ctab, h->rank_of_lin, h->posU,
-                                                       h->velU, h->idU, h->keyU, h->hist, h->err);
+                                                       h->velU, h->idU, h->keyU, h->hist, h->err,
+                                                       use_list ? h->nbr : nullptr, h->ncount);
   h->launches += 1;
   enqueue_scan_fill(h);
   k_reorder<<<grid_for(h->n, 256), 256, 0, h->st>>>(h->n, h->tmp, h->tmpid, h->keyU, h->cstart,
@@ -256,8 +361,8 @@ void enqueue_xsph_sort(SphHandle* h) {
 
 // lib.rs:287-335 after the bootstrap: kick1+XSPH+drift+clamp, grid + reorder,
 // density, boundary pressure, forces + kick2.
-void enqueue_body(SphHandle* h) {
-  enqueue_xsph_sort(h);
+void enqueue_body(SphHandle* h, bool use_list) {
+  enqueue_xsph_sort(h, use_list);
   enqueue_density_adami(h);
   enqueue_forces(h, 1.0f);
 }
@@ -274,7 +379,7 @@ int capture(SphHandle* h, bool with_finalize, cudaGraphExec_t* out) {
   SPH_TRY(h, cudaStreamBeginCapture(h->st, cudaStreamCaptureModeThreadLocal));
   if (with_finalize)
     sph::k_dt_finalize<<<1, 1, 0, h->st>>>(h->k.h, h->k.c, h->prm.cfl_number, h->red, h->dt);
-  enqueue_body(h);
+  enqueue_body(h, true);
   cudaError_t e = cudaStreamEndCapture(h->st, &g);
   if (e != cudaSuccess) return cuda_status(h, e, "cudaStreamEndCapture");
   h->body_kernels = (int)(h->launches - before);
@@ -346,8 +451,16 @@ int sph_create(const SphParams* params, const SphParticlesView* pv, const SphBou
     return SPH_ERR_INVALID_ARG;
   if (bv && bv->n > 0 && (!bv->x || !bv->y || !bv->z || !bv->mass)) return SPH_ERR_INVALID_ARG;
   if (bv && bv->n > 0x7fffffffull) return SPH_ERR_INVALID_ARG;
-  if (P.boundary_mode != SPH_BOUNDARY_PARTICLES) return SPH_ERR_INVALID_ARG;
-  (void)sdf;
+  if (P.boundary_mode != SPH_BOUNDARY_PARTICLES && P.boundary_mode != SPH_BOUNDARY_SDF)
+    return SPH_ERR_INVALID_ARG;
+  const bool sdf_mode = P.boundary_mode == SPH_BOUNDARY_SDF;
+  uint64_t sdf_nodes = 0;
+  if (sdf_mode) {
+    if (!sdf || !sdf->distances || !(sdf->cell_size > 0.0f)) return SPH_ERR_INVALID_ARG;
+    if (sdf->dims[0] < 2 || sdf->dims[1] < 2 || sdf->dims[2] < 2) return SPH_ERR_INVALID_ARG;
+    sdf_nodes = (uint64_t)sdf->dims[0] * sdf->dims[1] * sdf->dims[2];
+    bv = nullptr;  // walls come from the SDF
+  }
 
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0 || P.device < 0 || P.device >= ndev) {
@@ -385,6 +498,18 @@ int sph_create(const SphParams* params, const SphParticlesView* pv, const SphBou
     return fail(SPH_ERR_INVALID_ARG);
   h->C = (int)C;
   h->k = make_const(P, dims);
+  if (sdf_mode) {
+    h->nb = 0;
+    h->k.sdf_mode = 1;
+    for (int a = 0; a < 3; ++a) {
+      h->k.sdf_origin[a] = sdf->origin[a];
+      h->k.sdf_dims[a] = (int)sdf->dims[a];
+    }
+    h->k.sdf_cell = sdf->cell_size;
+    h->k.wall_mid = 1.5f * (P.h / 1.3f);
+  }
+  std::vector<float2> wall_host;
+  if (sdf_mode) wall_host = make_wall_table(P.h, &h->k.wall_inv_step);
 
   // cell ranks: Morton order (21 bits per axis; the 30-bit key when all
   // dims <= 1024) or linear order.
@@ -444,6 +569,9 @@ int sph_create(const SphParams* params, const SphParticlesView* pv, const SphBou
   ALLOC(part_m, h->nparts); ALLOC(part_e, h->nparts); ALLOC(part_var, h->nparts); ALLOC(me, 2);
   ALLOC(var, 1); ALLOC(bad, 1);
   ALLOC(stage, 12 * n); ALLOC(stage_ft, n); ALLOC(diag, 2);
+  ALLOC(nbr, (size_t)sph::kNbrCap * n); ALLOC(ncount, n);
+  if (sdf_mode) ALLOC(sdf, sdf_nodes);
+  if (sdf_mode) ALLOC(wall_tab, wall_host.size());
 #undef ALLOC
   if (e != cudaSuccess) return fail(e == cudaErrorMemoryAllocation ? SPH_ERR_OOM : SPH_ERR_CUDA);
 
@@ -475,6 +603,8 @@ int sph_create(const SphParams* params, const SphParticlesView* pv, const SphBou
   up(h->lin_of_rank, lin_of_rank.data(), C * sizeof(uint32_t));
   up(h->bc_start, bstart.data(), (C + 1) * sizeof(uint32_t));
   up(h->bc_list, blist.data(), blist.size() * sizeof(uint32_t));
+  if (sdf_mode) up(h->sdf, sdf->distances, sdf_nodes * sizeof(float));
+  if (sdf_mode) up(h->wall_tab, wall_host.data(), wall_host.size() * sizeof(float2));
   if (e == cudaSuccess) e = cudaMemsetAsync(h->hist, 0, C * sizeof(uint32_t), h->st);
   if (e == cudaSuccess) e = cudaMemsetAsync(h->bpress, 0, std::max<size_t>(1, nb) * sizeof(float), h->st);
   if (e == cudaSuccess) e = cudaMemsetAsync(h->err, 0, sizeof(uint32_t), h->st);
@@ -522,13 +652,20 @@ int sph_step(SphHandle* h, float dt) {
   if (h->needs_init) {
     enqueue_bootstrap(h);
     h->needs_init = false;
+    h->list_valid = true;
   }
-  if (!h->g_step) {
-    int s = capture(h, false, &h->g_step);
-    if (s != SPH_OK) return s;
+  if (!h->list_valid) {
+    // after a restore: XSPH rescans the stale grid with the restored positions
+    enqueue_body(h, false);
+  } else {
+    if (!h->g_step) {
+      int s = capture(h, false, &h->g_step);
+      if (s != SPH_OK) return s;
+    }
+    SPH_TRY(h, cudaGraphLaunch(h->g_step, h->st));
+    h->launches += h->body_kernels;
   }
-  SPH_TRY(h, cudaGraphLaunch(h->g_step, h->st));
-  h->launches += h->body_kernels;
+  h->list_valid = true;
   h->red_valid = true;
   return cuda_status(h, cudaGetLastError(), "sph_step");
 }
@@ -539,17 +676,15 @@ int sph_step_auto(SphHandle* h, int nsteps, float* dt_out) {
   if (h->n == 0) return SPH_OK;
   for (int s = 0; s < nsteps; ++s) {
     ensure_red(h);
-    if (h->needs_init) {
+    if (h->needs_init || !h->list_valid) {
       sph::k_dt_finalize<<<1, 1, 0, h->st>>>(h->k.h, h->k.c, h->prm.cfl_number, h->red, h->dt);
       h->launches += 1;
-      enqueue_bootstrap(h);
-      h->needs_init = false;
-      if (!h->g_step) {
-        int st = capture(h, false, &h->g_step);
-        if (st != SPH_OK) return st;
+      if (h->needs_init) {
+        enqueue_bootstrap(h);
+        h->needs_init = false;
+        h->list_valid = true;
       }
-      SPH_TRY(h, cudaGraphLaunch(h->g_step, h->st));
-      h->launches += h->body_kernels;
+      enqueue_body(h, h->list_valid);
     } else {
       if (!h->g_auto) {
         int st = capture(h, true, &h->g_auto);
@@ -558,6 +693,7 @@ int sph_step_auto(SphHandle* h, int nsteps, float* dt_out) {
       SPH_TRY(h, cudaGraphLaunch(h->g_auto, h->st));
       h->launches += h->body_kernels;
     }
+    h->list_valid = true;
     h->red_valid = true;
   }
   if (dt_out) {
@@ -595,6 +731,7 @@ int sph_step_profiled(SphHandle* h, float dt, SphStepProfile* prof) {
   if (h->needs_init) {
     enqueue_bootstrap(h);
     h->needs_init = false;
+    h->list_valid = true;
   }
   cudaEvent_t ev[6];
   for (int i = 0; i < 6; ++i) SPH_TRY(h, cudaEventCreate(&ev[i]));
@@ -602,7 +739,8 @@ int sph_step_profiled(SphHandle* h, float dt, SphStepProfile* prof) {
   cudaEventRecord(ev[0], h->st);
   k_xsph_drift<<<grid_for(h->n, 256), 256, 0, h->st>>>(h->k, h->n, h->dt, h->pos, h->velout, h->acc,
                                                        h->id, h->ctab, h->rank_of_lin, h->posU, h->velU,
-                                                       h->idU, h->keyU, h->hist, h->err);
+                                                       h->idU, h->keyU, h->hist, h->err,
+                                                       h->list_valid ? h->nbr : nullptr, h->ncount);
   h->launches += 1;
   cudaEventRecord(ev[1], h->st);
   enqueue_scan_fill(h);
@@ -612,7 +750,8 @@ int sph_step_profiled(SphHandle* h, float dt, SphStepProfile* prof) {
   h->launches += 1;
   cudaEventRecord(ev[2], h->st);
   k_density<<<grid_for(h->n, 256), 256, 0, h->st>>>(h->k, h->n, h->dt, h->pos, h->rv, h->id, h->ctab,
-                                                    h->bc_start, h->bc_list, h->bpos, h->rf, h->pr, h->err);
+                                                    h->bc_start, h->bc_list, h->bpos, h->rf, h->pr, h->err,
+                                                    h->nbr, h->ncount, h->sdf, h->wall_tab);
   h->launches += 1;
   cudaEventRecord(ev[3], h->st);
   if (h->nb > 0) {
@@ -635,6 +774,7 @@ int sph_step_profiled(SphHandle* h, float dt, SphStepProfile* prof) {
   prof->forces_us = t[4] * 1e3f;
   prof->total_us = (t[0] + t[1] + t[2] + t[3] + t[4]) * 1e3f;
   h->red_valid = true;
+  h->list_valid = true;
   return check_device_flags(h);
 }
 
@@ -726,6 +866,7 @@ int sph_restore_checkpoint(SphHandle* h) {
   }
   h->has_ck = false;
   h->red_valid = false;
+  h->list_valid = false;
   ensure_red(h);
   return cuda_status(h, cudaGetLastError(), "sph_restore_checkpoint");
 }
@@ -759,6 +900,110 @@ const char* sph_last_error(const SphHandle* h) { return h ? h->error.c_str() : "
 void* sph_stream(SphHandle* h) { return h ? (void*)h->st : nullptr; }
 
 uint64_t sph_launch_count(const SphHandle* h) { return h ? h->launches : 0; }
+
+int sph_set_geometry_sdf(SphHandle* h, const SphSdfView* g) {
+  if (!h || !g || !g->distances || !(g->cell_size > 0.0f)) return SPH_ERR_INVALID_ARG;
+  SPH_TRY(h, cudaSetDevice(h->dev));
+  // force.rs:47-81: nodes with |d| <= 2h and d <= 0 and a unit normal, in
+  // (i, j, k) order.
+  float thr = 2.0f * h->prm.h;
+  std::vector<float4> np_, nn_;
+  for (uint32_t i = 0; i < g->dims[0]; ++i)
+    for (uint32_t j = 0; j < g->dims[1]; ++j)
+      for (uint32_t k = 0; k < g->dims[2]; ++k) {
+        float px = g->origin[0] + (float)i * g->cell_size;
+        float py = g->origin[1] + (float)j * g->cell_size;
+        float pz = g->origin[2] + (float)k * g->cell_size;
+        float d = host_sdf_sample(*g, px, py, pz);
+        if (std::fabs(d) > thr || d > 0.0f) continue;
+        float n[3];
+        host_sdf_gradient(*g, px, py, pz, n);
+        float mag = std::sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
+        if (mag < 1e-8f) continue;
+        np_.push_back(make_float4(px, py, pz, d));
+        nn_.push_back(make_float4(n[0], n[1], n[2], 0.0f));
+      }
+  if (!h->geo_sum) {
+    cudaError_t e = dalloc(h, &h->geo_sum, 6);
+    if (e != cudaSuccess) return cuda_status(h, e, "geometry allocation");
+  }
+  h->geo_nodes = (int)np_.size();
+  h->geo_area = g->cell_size * g->cell_size;
+  cudaError_t e = cudaSuccess;
+  if (h->geo_nodes) {
+    e = dalloc(h, &h->geo_pos, np_.size());
+    if (e == cudaSuccess) e = dalloc(h, &h->geo_nrm, nn_.size());
+    if (e == cudaSuccess) e = dalloc(h, &h->geo_out, np_.size() * 6);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(h->geo_pos, np_.data(), np_.size() * sizeof(float4), cudaMemcpyHostToDevice, h->st);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(h->geo_nrm, nn_.data(), nn_.size() * sizeof(float4), cudaMemcpyHostToDevice, h->st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->st);
+  }
+  return cuda_status(h, e, "sph_set_geometry_sdf");
+}
+
+int sph_surface_forces(SphHandle* h, SphSurfaceForce* out) {
+  if (!h || !out) return SPH_ERR_INVALID_ARG;
+  if (!h->geo_sum) return set_err(h, SPH_ERR_INVALID_ARG, "no geometry SDF registered");
+  SPH_TRY(h, cudaSetDevice(h->dev));
+  std::memset(out, 0, sizeof(*out));
+  out->nodes = (uint32_t)h->geo_nodes;
+  if (h->geo_nodes == 0 || h->n == 0) return SPH_OK;
+  using namespace sph;
+  k_surface_nodes<<<grid_for(h->geo_nodes, kSurfWarps), kSurfWarps * 32, 0, h->st>>>(
+      h->k, h->geo_nodes, h->geo_pos, h->geo_nrm, h->geo_area, h->pos, h->pr, h->id, h->ctab, h->geo_out,
+      h->err);
+  k_sum_rows_f64<<<1, 256, 0, h->st>>>(h->geo_nodes, 6, h->geo_out, h->geo_sum);
+  h->launches += 2;
+  std::vector<float> rows((size_t)h->geo_nodes * 6);
+  double sums[6];
+  SPH_TRY(h, cudaMemcpyAsync(rows.data(), h->geo_out, rows.size() * 4, cudaMemcpyDeviceToHost, h->st));
+  SPH_TRY(h, cudaMemcpyAsync(sums, h->geo_sum, sizeof(sums), cudaMemcpyDeviceToHost, h->st));
+  SPH_TRY(h, cudaStreamSynchronize(h->st));
+  float f32[6] = {0, 0, 0, 0, 0, 0};
+  for (int nd = 0; nd < h->geo_nodes; ++nd) {
+    const float* r = &rows[(size_t)nd * 6];
+    if (r[0] != 0.0f || r[1] != 0.0f || r[2] != 0.0f || r[3] != 0.0f || r[4] != 0.0f || r[5] != 0.0f)
+      out->active_nodes++;
+    for (int a = 0; a < 6; ++a) f32[a] += r[a];
+  }
+  for (int a = 0; a < 3; ++a) {
+    out->force[a] = sums[a];
+    out->moment[a] = sums[3 + a];
+    out->force_f32[a] = f32[a];
+    out->moment_f32[a] = f32[3 + a];
+  }
+  return check_device_flags(h);
+}
+
+int sph_body_force(SphHandle* h, uint32_t first, uint32_t count, SphBodyForce* out) {
+  if (!h || !out) return SPH_ERR_INVALID_ARG;
+  if ((uint64_t)first + count > (uint64_t)h->nb) return set_err(h, SPH_ERR_INVALID_ARG, "body range");
+  SPH_TRY(h, cudaSetDevice(h->dev));
+  std::memset(out, 0, sizeof(*out));
+  if (h->n == 0 || count == 0) return SPH_OK;
+  using namespace sph;
+  int parts = grid_for(h->n, 256);
+  if (parts > h->body_parts) {
+    cudaError_t e = dalloc(h, &h->body_part, (size_t)parts * kBodyCols);
+    if (e == cudaSuccess && !h->body_sum) e = dalloc(h, &h->body_sum, kBodyCols);
+    if (e != cudaSuccess) return cuda_status(h, e, "body force allocation");
+    h->body_parts = parts;
+  }
+  k_body_force<<<parts, 256, 0, h->st>>>(h->k, h->n, first, count, h->pos, h->vel, h->rf, h->pr, h->id,
+                                         h->bc_start, h->bc_list, h->bpos, h->bpress, h->body_part);
+  k_sum_parts_f64<<<1, 32, 0, h->st>>>(parts, kBodyCols, h->body_part, h->body_sum);
+  h->launches += 2;
+  double v[kBodyCols];
+  SPH_TRY(h, cudaMemcpyAsync(v, h->body_sum, sizeof(v), cudaMemcpyDeviceToHost, h->st));
+  SPH_TRY(h, cudaStreamSynchronize(h->st));
+  double* dst[6] = {out->pressure_force, out->pressure_moment, out->repulsion_force,
+                    out->repulsion_moment, out->viscous_force, out->viscous_moment};
+  for (int t = 0; t < 6; ++t)
+    for (int a = 0; a < 3; ++a) dst[t][a] = v[3 * t + a];
+  return check_device_flags(h);
+}
 
 int sph_grid_info(SphHandle* h, SphGridInfo* out) {
   if (!h || !out) return SPH_ERR_INVALID_ARG;

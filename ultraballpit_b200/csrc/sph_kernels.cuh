@@ -28,6 +28,7 @@ constexpr float kWaterRho0 = 1000.0f;  // eos.rs:7
 constexpr float kAirRho0 = 1.204f;     // eos.rs:10
 constexpr int kAdamiCap = 256;         // fluid terms per boundary particle
 constexpr int kCellCap = 4096;         // particles per cell for the id ranking
+constexpr uint32_t kNbrCap = 128;      // listed neighbours per particle
 
 enum : uint32_t { kFlagDelta = 1, kFlagXsph = 2, kFlagRepulsion = 4, kFlagClamp = 8 };
 enum : uint32_t { kErrCellCap = 1, kErrAdamiCap = 2 };
@@ -51,6 +52,16 @@ struct SimConst {
   float reach;           // Adami candidate reach, > 2h with margin
   float sdf_coef;
   uint32_t flags;
+  // sqrtf is monotone: sqrtf(d2) < support  <=>  d2 <= sup_d2,
+  // sqrtf(d2) < r0 <=> d2 <= r0_d2, sqrtf(d2) > 1e-12 <=> d2 > tiny_d2.
+  float sup_d2, r0_d2, tiny_d2;
+  // SDF wall mode (boundary_mode 1): node grid geometry
+  int sdf_mode;
+  float wall_inv_step;   // kWallN / 2h
+  float wall_mid;        // 1.5 * (h / 1.3): depth of the middle wall layer
+  float sdf_origin[3];
+  float sdf_cell;
+  int sdf_dims[3];
 };
 
 // ---------------------------------------------------------------------------
@@ -113,6 +124,66 @@ __device__ __forceinline__ float tait(float rho, bool air, const SimConst& k) {
   return fmaxf(p, 0.0f);
 }
 
+// ---- SDF wall (boundary_mode 1; no reference counterpart) -----------------
+// The SDF wall stands in for the reference's 3 layers of wall particles,
+// homogenised along the wall: wall_tab holds, at kWallN + 1 distances on
+// [0, 2h], the lateral-average lattice sums (phi = sum W dx^3, grad =
+// sum -dW/dn dx^3) built on the host; linear interpolation in f32.
+constexpr int kWallN = 512;
+__device__ __forceinline__ float2 wall_lookup(const float2* __restrict__ tab, float inv_step, float d) {
+  float u = fmaxf(d, 0.0f) * inv_step;
+  if (!(u < (float)kWallN)) return make_float2(0.0f, 0.0f);
+  int i = (int)u;
+  float f = u - (float)i;
+  float2 a = __ldg(&tab[i]), b = __ldg(&tab[i + 1]);
+  return make_float2(a.x + f * (b.x - a.x), a.y + f * (b.y - a.y));
+}
+
+// GridSDF::sample (orchestrator geometry.rs:99-150) with the grid coordinate
+// clamped to [0, dims-1-1e-3]: points on or past the outer nodes interpolate
+// in the last cell instead of returning f32::MAX.
+__device__ __forceinline__ float sdf_sample_clamped(const float* __restrict__ d, const SimConst& k,
+                                                    float px, float py, float pz) {
+  float g[3] = {(px - k.sdf_origin[0]) / k.sdf_cell, (py - k.sdf_origin[1]) / k.sdf_cell,
+                (pz - k.sdf_origin[2]) / k.sdf_cell};
+  int i0[3];
+  float fr[3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    g[a] = fminf(fmaxf(g[a], 0.0f), (float)(k.sdf_dims[a] - 1) - 0.001f);
+    i0[a] = (int)floorf(g[a]);
+    fr[a] = g[a] - (float)i0[a];
+  }
+  size_t ny = (size_t)k.sdf_dims[1], nz = (size_t)k.sdf_dims[2];
+  size_t base = (size_t)i0[0] * ny * nz + (size_t)i0[1] * nz + (size_t)i0[2];
+  size_t si = ny * nz, sj = nz;
+  float c000 = __ldg(&d[base]), c001 = __ldg(&d[base + 1]);
+  float c010 = __ldg(&d[base + sj]), c011 = __ldg(&d[base + sj + 1]);
+  float c100 = __ldg(&d[base + si]), c101 = __ldg(&d[base + si + 1]);
+  float c110 = __ldg(&d[base + si + sj]), c111 = __ldg(&d[base + si + sj + 1]);
+  float fx = fr[0], fy = fr[1], fz = fr[2];
+  float c00 = c000 * (1.0f - fz) + c001 * fz;
+  float c01 = c010 * (1.0f - fz) + c011 * fz;
+  float c10 = c100 * (1.0f - fz) + c101 * fz;
+  float c11 = c110 * (1.0f - fz) + c111 * fz;
+  float c0 = c00 * (1.0f - fy) + c01 * fy;
+  float c1 = c10 * (1.0f - fy) + c11 * fy;
+  return c0 * (1.0f - fx) + c1 * fx;
+}
+
+// GridSDF::gradient (geometry.rs:153-175) on the clamped sampler.
+__device__ __forceinline__ void sdf_gradient_clamped(const float* __restrict__ d, const SimConst& k,
+                                                     float px, float py, float pz, float& nx,
+                                                     float& ny, float& nz) {
+  float h = k.sdf_cell * 0.5f;
+  float gx = (sdf_sample_clamped(d, k, px + h, py, pz) - sdf_sample_clamped(d, k, px - h, py, pz)) / (2.0f * h);
+  float gy = (sdf_sample_clamped(d, k, px, py + h, pz) - sdf_sample_clamped(d, k, px, py - h, pz)) / (2.0f * h);
+  float gz = (sdf_sample_clamped(d, k, px, py, pz + h) - sdf_sample_clamped(d, k, px, py, pz - h)) / (2.0f * h);
+  float mag = sqrtf(gx * gx + gy * gy + gz * gz);
+  if (mag > 1e-8f) { nx = gx / mag; ny = gy / mag; nz = gz / mag; }
+  else { nx = 0.0f; ny = 0.0f; nz = 0.0f; }
+}
+
 __device__ __forceinline__ uint32_t spread10(uint32_t v) {
   v &= 0x3ffu;
   v = (v | (v << 16)) & 0x030000ffu;
@@ -142,16 +213,38 @@ __device__ __forceinline__ void for_each_neighbor(float px, float py, float pz, 
   int cx = axis_cell(px, k.gmin[0], k.cell, k.dims[0]);
   int cy = axis_cell(py, k.gmin[1], k.cell, k.dims[1]);
   int cz = axis_cell(pz, k.gmin[2], k.cell, k.dims[2]);
+  // Squared distance to the lower / upper face of the home cell per axis,
+  // shrunk by a margin far above any rounding of the binning: a cell whose
+  // box lies farther than 2h holds no particle with dist_sq <= (2h)^2, so
+  // skipping it changes no sum.
+  const float margin = 1.0e-5f * k.cell + 1.0e-6f;
+  float lo2[3], hi2[3];
+  {
+    float p3[3] = {px, py, pz};
+    int c3[3] = {cx, cy, cz};
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      float face = k.gmin[a] + (float)c3[a] * k.cell;
+      float dl = fmaxf(p3[a] - face - margin, 0.0f);
+      float dh = fmaxf(face + k.cell - p3[a] - margin, 0.0f);
+      lo2[a] = dl * dl;
+      hi2[a] = dh * dh;
+    }
+  }
   for (int dz = -1; dz <= 1; ++dz) {
     int nz = cz + dz;
     if (nz < 0 || nz >= k.dims[2]) continue;
+    float ez = dz < 0 ? lo2[2] : (dz > 0 ? hi2[2] : 0.0f);
     for (int dy = -1; dy <= 1; ++dy) {
       int ny = cy + dy;
       if (ny < 0 || ny >= k.dims[1]) continue;
+      float ey = ez + (dy < 0 ? lo2[1] : (dy > 0 ? hi2[1] : 0.0f));
+      if (ey > k.radius_sq) continue;
       int row = (ny + nz * k.dims[1]) * k.dims[0];
       for (int dx = -1; dx <= 1; ++dx) {
         int nx = cx + dx;
         if (nx < 0 || nx >= k.dims[0]) continue;
+        if (ey + (dx < 0 ? lo2[0] : (dx > 0 ? hi2[0] : 0.0f)) > k.radius_sq) continue;
         uint2 se = __ldg(&ctab[row + nx]);
         int end = (int)(se.x + se.y);
         for (int s = (int)se.x; s < end; ++s) {
@@ -163,6 +256,30 @@ __device__ __forceinline__ void for_each_neighbor(float px, float py, float pz, 
         }
       }
     }
+  }
+}
+
+// Same visit as for_each_neighbor, replayed from the neighbour list that
+// k_density recorded on this grid (slots in visit order, nbr[c * n + i]).
+// Particles whose list overflowed kNbrCap, and calls without a list, scan.
+template <class F>
+__device__ __forceinline__ void visit_neighbors(int i, int n, float px, float py, float pz,
+                                                const float4* __restrict__ pos,
+                                                const uint2* __restrict__ ctab,
+                                                const uint32_t* __restrict__ nbr,
+                                                const uint32_t* __restrict__ ncount,
+                                                const SimConst& k, F&& f) {
+  uint32_t cnt = nbr ? __ldg(&ncount[i]) : 0xffffffffu;
+  if (cnt <= kNbrCap) {
+    for (uint32_t c = 0; c < cnt; ++c) {
+      int s = (int)__ldg(&nbr[(size_t)c * n + i]);
+      float4 pj = __ldg(&pos[s]);
+      float ddx = px - pj.x, ddy = py - pj.y, ddz = pz - pj.z;
+      float d2 = ddx * ddx + ddy * ddy + ddz * ddz;
+      f(s, pj, ddx, ddy, ddz, d2);
+    }
+  } else {
+    for_each_neighbor(px, py, pz, i, pos, ctab, k, f);
   }
 }
 
@@ -182,7 +299,8 @@ k_xsph_drift(SimConst k, int n, const float* __restrict__ dtp, const float4* __r
              const uint32_t* __restrict__ id, const uint2* __restrict__ ctab,
              const uint32_t* __restrict__ rank_of_lin, float4* __restrict__ posU,
              float4* __restrict__ velU, uint32_t* __restrict__ idU, uint32_t* __restrict__ keyU,
-             uint32_t* __restrict__ hist, const uint32_t* __restrict__ err) {
+             uint32_t* __restrict__ hist, const uint32_t* __restrict__ err,
+             const uint32_t* __restrict__ nbr, const uint32_t* __restrict__ ncount) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n || *err) return;
   float dt = *dtp;
@@ -196,7 +314,7 @@ k_xsph_drift(SimConst k, int n, const float* __restrict__ dtp, const float4* __r
   float sx = 0.0f, sy = 0.0f, sz = 0.0f;
   if (k.flags & kFlagXsph) {
     float rho_i = vi.w;
-    for_each_neighbor(pi.x, pi.y, pi.z, i, pos, ctab, k,
+    visit_neighbors(i, n, pi.x, pi.y, pi.z, pos, ctab, nbr, ncount, k,
                       [&](int s, const float4& pj, float dx, float dy, float dz, float d2) {
                         float r = sqrtf(d2);
                         float w = w_c2(r, k);
@@ -395,7 +513,9 @@ k_density(SimConst k, int n, const float* __restrict__ dtp, const float4* __rest
           const float2* __restrict__ rv, const uint32_t* __restrict__ id,
           const uint2* __restrict__ ctab, const uint32_t* __restrict__ bc_start,
           const uint32_t* __restrict__ bc_list, const float4* __restrict__ bpos,
-          float2* __restrict__ rf, float* __restrict__ pr, const uint32_t* __restrict__ err) {
+          float2* __restrict__ rf, float* __restrict__ pr, const uint32_t* __restrict__ err,
+          uint32_t* __restrict__ nbr, uint32_t* __restrict__ ncount, const float* __restrict__ sdf,
+          const float2* __restrict__ wall_tab) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n || *err) return;
   float dt = *dtp;
@@ -404,19 +524,37 @@ k_density(SimConst k, int n, const float* __restrict__ dtp, const float4* __rest
   float rho = pi.w * k.norm_h3;
   float diff_sum = 0.0f;
   bool delta = (k.flags & kFlagDelta) != 0;
+  // Phase 1: the 27-cell scan only records in-support slots, in visit order.
+  uint32_t listed = 0;
   for_each_neighbor(pi.x, pi.y, pi.z, i, pos, ctab, k,
-                    [&](int s, const float4& pj, float dx, float dy, float dz, float d2) {
-                      float r = sqrtf(d2);
-                      if (delta) {
-                        float gx, gy, gz;
-                        grad_c2(dx, dy, dz, r, k, gx, gy, gz);
-                        float2 rvj = __ldg(&rv[s]);
-                        float r_dot_grad = dx * gx + dy * gy + dz * gz;
-                        float density_diff = rho_old_i - rvj.x;
-                        diff_sum += rvj.y * density_diff * 2.0f * r_dot_grad / (d2 + k.eta_sq);
-                      }
-                      rho += pj.w * w_c2(r, k);
+                    [&](int s, const float4&, float, float, float, float) {
+                      if (listed < kNbrCap) nbr[(size_t)listed * n + i] = (uint32_t)s;
+                      ++listed;
                     });
+  ncount[i] = listed;
+  // Phase 2: density and delta-SPH terms over the list, same order.
+  auto term = [&](int s, const float4& pj, float dx, float dy, float dz, float d2) {
+    float r = sqrtf(d2);
+    if (delta) {
+      float gx, gy, gz;
+      grad_c2(dx, dy, dz, r, k, gx, gy, gz);
+      float2 rvj = __ldg(&rv[s]);
+      float r_dot_grad = dx * gx + dy * gy + dz * gz;
+      float density_diff = rho_old_i - rvj.x;
+      diff_sum += rvj.y * density_diff * 2.0f * r_dot_grad / (d2 + k.eta_sq);
+    }
+    rho += pj.w * w_c2(r, k);
+  };
+  if (listed <= kNbrCap) {
+    for (uint32_t c = 0; c < listed; ++c) {
+      int s = (int)nbr[(size_t)c * n + i];
+      float4 pj = __ldg(&pos[s]);
+      float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
+      term(s, pj, dx, dy, dz, dx * dx + dy * dy + dz * dz);
+    }
+  } else {
+    for_each_neighbor(pi.x, pi.y, pi.z, i, pos, ctab, k, term);
+  }
   int lin = cell_hash(axis_cell(pi.x, k.gmin[0], k.cell, k.dims[0]),
                       axis_cell(pi.y, k.gmin[1], k.cell, k.dims[1]),
                       axis_cell(pi.z, k.gmin[2], k.cell, k.dims[2]), k);
@@ -424,14 +562,18 @@ k_density(SimConst k, int n, const float* __restrict__ dtp, const float4* __rest
   for (uint32_t q = b0; q < b1; ++q) {
     float4 bp = __ldg(&bpos[__ldg(&bc_list[q])]);
     float dx = pi.x - bp.x, dy = pi.y - bp.y, dz = pi.z - bp.z;
-    float r = sqrtf(dx * dx + dy * dy + dz * dz);
-    if (r < k.support) rho += bp.w * w_c2(r, k);
+    float d2 = dx * dx + dy * dy + dz * dz;
+    if (d2 <= k.sup_d2) rho += bp.w * w_c2(sqrtf(d2), k);
+  }
+  bool air = (id[i] & kAirBit) != 0;
+  if (k.sdf_mode) {  // kernel mass of the wall half-space
+    float d = sdf_sample_clamped(sdf, k, pi.x, pi.y, pi.z);
+    if (d < k.support) rho += (air ? kAirRho0 : kWaterRho0) * wall_lookup(wall_tab, k.wall_inv_step, d).x;
   }
   if (delta) {
     float diffusion = k.delta_coef * diff_sum;
     rho += diffusion * dt;
   }
-  bool air = (id[i] & kAirBit) != 0;
   float p = tait(rho, air, k);
   rf[i] = make_float2(rho, p / (rho * rho));
   pr[i] = p;
@@ -462,42 +604,57 @@ k_adami(SimConst k, int nb, const float4* __restrict__ bpos, float* __restrict__
   }
   int count = 0;
   bool overflow = false;
-  for (int cz = lo[2]; cz <= hi[2]; ++cz)
-    for (int cy = lo[1]; cy <= hi[1]; ++cy)
-      for (int cx = lo[0]; cx <= hi[0]; ++cx) {
-        uint2 se = __ldg(&ctab[cell_hash(cx, cy, cz, k)]);
-        for (uint32_t base = se.x; base < se.x + se.y; base += 32) {
-          uint32_t s = base + lane;
-          bool inr = false;
-          float w = 0.0f, wp = 0.0f;
-          uint32_t fid = 0;
-          if (s < se.x + se.y) {
-            float4 pf = __ldg(&pos[s]);
-            float dx = bp.x - pf.x, dy = bp.y - pf.y, dz = bp.z - pf.z;
-            float r = sqrtf(dx * dx + dy * dy + dz * dz);
-            if (r < k.support) {
-              inr = true;
-              w = w_c2(r, k);
-              float g_dot_dr = k.grav[0] * dx + k.grav[1] * dy + k.grav[2] * dz;
-              float p_ext = __ldg(&pr[s]) + __ldg(&rf[s]).x * g_dot_dr;
-              wp = w * p_ext;
-              fid = __ldg(&id[s]) & kIdMask;
-            }
+  // Lanes look up the (at most 4x4x4) cells of the range in parallel; only
+  // occupied cells are then scanned. The terms are sorted by fluid index
+  // below, so the cell order does not matter.
+  int nx = hi[0] - lo[0] + 1, ny = hi[1] - lo[1] + 1, nz = hi[2] - lo[2] + 1;
+  int ncell = nx * ny * nz;
+  for (int cbase = 0; cbase < ncell; cbase += 32) {
+    int q = cbase + lane;
+    uint2 mine = make_uint2(0u, 0u);
+    if (q < ncell) {
+      int qx = q % nx, qy = (q / nx) % ny, qz = q / (nx * ny);
+      mine = __ldg(&ctab[cell_hash(lo[0] + qx, lo[1] + qy, lo[2] + qz, k)]);
+    }
+    unsigned occupied = __ballot_sync(0xffffffffu, mine.y > 0u);
+    while (occupied) {
+      int src = __ffs(occupied) - 1;
+      occupied &= occupied - 1u;
+      uint32_t st = __shfl_sync(0xffffffffu, mine.x, src);
+      uint32_t cn = __shfl_sync(0xffffffffu, mine.y, src);
+      for (uint32_t base = st; base < st + cn; base += 32) {
+        uint32_t s = base + lane;
+        bool inr = false;
+        float w = 0.0f, wp = 0.0f;
+        uint32_t fid = 0;
+        if (s < st + cn) {
+          float4 pf = __ldg(&pos[s]);
+          float dx = bp.x - pf.x, dy = bp.y - pf.y, dz = bp.z - pf.z;
+          float d2 = dx * dx + dy * dy + dz * dz;
+          if (d2 <= k.sup_d2) {
+            inr = true;
+            w = w_c2(sqrtf(d2), k);
+            float g_dot_dr = k.grav[0] * dx + k.grav[1] * dy + k.grav[2] * dz;
+            float p_ext = __ldg(&pr[s]) + __ldg(&rf[s]).x * g_dot_dr;
+            wp = w * p_ext;
+            fid = __ldg(&id[s]) & kIdMask;
           }
-          unsigned m = __ballot_sync(0xffffffffu, inr);
-          int off = count + __popc(m & ((1u << lane) - 1u));
-          if (inr) {
-            if (off < kAdamiCap) {
-              s_id[warp][off] = fid;
-              s_w[warp][off] = w;
-              s_wp[warp][off] = wp;
-            } else {
-              overflow = true;
-            }
-          }
-          count += __popc(m);
         }
+        unsigned m = __ballot_sync(0xffffffffu, inr);
+        int off = count + __popc(m & ((1u << lane) - 1u));
+        if (inr) {
+          if (off < kAdamiCap) {
+            s_id[warp][off] = fid;
+            s_w[warp][off] = w;
+            s_wp[warp][off] = wp;
+          } else {
+            overflow = true;
+          }
+        }
+        count += __popc(m);
       }
+    }
+  }
   if (__any_sync(0xffffffffu, overflow) || count > kAdamiCap) {
     if (lane == 0) atomicOr(err, kErrAdamiCap);
     return;
@@ -544,7 +701,9 @@ k_forces(SimConst k, int n, const float* __restrict__ dtp, float hdt_scale,
          const uint32_t* __restrict__ bc_start, const uint32_t* __restrict__ bc_list,
          const float4* __restrict__ bpos, const float* __restrict__ bpress,
          float4* __restrict__ acc, float4* __restrict__ velout, float* __restrict__ red,
-         const uint32_t* __restrict__ err) {
+         const uint32_t* __restrict__ err, const uint32_t* __restrict__ nbr,
+         const uint32_t* __restrict__ ncount, const float* __restrict__ sdf,
+         const float2* __restrict__ wall_tab) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   float sig = 0.0f, amag = 0.0f;
   if (i < n && !*err) {
@@ -556,7 +715,7 @@ k_forces(SimConst k, int n, const float* __restrict__ dtp, float hdt_scale,
     float fpx = 0.0f, fpy = 0.0f, fpz = 0.0f;
     float fvx = 0.0f, fvy = 0.0f, fvz = 0.0f;
     float neg_mi = -pi.w;
-    for_each_neighbor(pi.x, pi.y, pi.z, i, pos, ctab, k,
+    visit_neighbors(i, n, pi.x, pi.y, pi.z, pos, ctab, nbr, ncount, k,
                       [&](int s, const float4& pj, float dx, float dy, float dz, float d2) {
                         float r = sqrtf(d2);
                         float gx, gy, gz;
@@ -594,8 +753,9 @@ k_forces(SimConst k, int n, const float* __restrict__ dtp, float hdt_scale,
         uint32_t bi = __ldg(&bc_list[q]);
         float4 bp = __ldg(&bpos[bi]);
         float dx = pi.x - bp.x, dy = pi.y - bp.y, dz = pi.z - bp.z;
-        float r = sqrtf(dx * dx + dy * dy + dz * dz);
-        if (r < k.support) {
+        float d2 = dx * dx + dy * dy + dz * dz;
+        if (d2 <= k.sup_d2) {
+          float r = sqrtf(d2);
           float gx, gy, gz;
           grad_c2(dx, dy, dz, r, k, gx, gy, gz);
           float pb_over = __ldg(&bpress[bi]) / brho2;
@@ -609,12 +769,40 @@ k_forces(SimConst k, int n, const float* __restrict__ dtp, float hdt_scale,
     float ax = 0.0f + fpx / pi.w, ay = 0.0f + fpy / pi.w, az = 0.0f + fpz / pi.w;
     ax += fvx; ay += fvy; az += fvz;
     ax += k.grav[0]; ay += k.grav[1]; az += k.grav[2];
+    if (k.sdf_mode) {
+      // boundary pressure force of the homogenised wall layers along the
+      // SDF normal, with the mirrored pressure p_w = max(max(p_i,0) +
+      // rho_i g.(r_w - r_i), 0) at the middle layer, then the repulsion
+      float d = sdf_sample_clamped(sdf, k, pi.x, pi.y, pi.z);
+      if (d < k.support) {
+        float nx, ny, nz;
+        sdf_gradient_clamped(sdf, k, pi.x, pi.y, pi.z, nx, ny, nz);
+        float rest = air ? kAirRho0 : kWaterRho0;
+        float pic = fmaxf(pr[i], 0.0f);
+        float depth = -(d + k.wall_mid);
+        float g_dot_dr = k.grav[0] * (depth * nx) + k.grav[1] * (depth * ny) + k.grav[2] * (depth * nz);
+        float pw = fmaxf(pic + rho_i * g_dot_dr, 0.0f);
+        float coef = (pic / (rho_i * rho_i) + pw / (rest * rest)) * rest *
+                     wall_lookup(wall_tab, k.wall_inv_step, d).y;
+        ax += coef * nx;
+        ay += coef * ny;
+        az += coef * nz;
+        if ((k.flags & kFlagRepulsion) && d < k.r0) {
+          float s = 1.0f - fmaxf(d, 0.0f) / k.r0;
+          float fm = k.sdf_coef * s * s / k.r0;
+          ax += fm * nx;
+          ay += fm * ny;
+          az += fm * nz;
+        }
+      }
+    }
     if ((k.flags & kFlagRepulsion) && b1 > b0) {
       for (uint32_t q = b0; q < b1; ++q) {
         float4 bp = __ldg(&bpos[__ldg(&bc_list[q])]);
         float dx = pi.x - bp.x, dy = pi.y - bp.y, dz = pi.z - bp.z;
-        float r = sqrtf(dx * dx + dy * dy + dz * dz);
-        if (r < k.r0 && r > 1.0e-12f) {
+        float d2 = dx * dx + dy * dy + dz * dz;
+        if (d2 <= k.r0_d2 && d2 > k.tiny_d2) {
+          float r = sqrtf(d2);
           float s = 1.0f - r / k.r0;
           float force_mag = k.rep_d * s * s / k.r0;
           float inv_r = 1.0f / r;
@@ -826,6 +1014,249 @@ __global__ void k_list_neighbors(SimConst k, const float4* __restrict__ pos,
                       ++c;
                     });
   *count = c;
+}
+
+}  // namespace sph
+
+namespace sph {
+
+// ---- force extraction (orchestrator force.rs:39-129) and body reaction ----
+
+// GridSDF::sample (geometry.rs:99-150) exactly, f32::MAX off the grid.
+__device__ __forceinline__ float sdf_sample_exact(const float* __restrict__ d, const float origin[3],
+                                                  float cell, const int dims[3], float px, float py,
+                                                  float pz) {
+  float gx = (px - origin[0]) / cell, gy = (py - origin[1]) / cell, gz = (pz - origin[2]) / cell;
+  int i0 = (int)floorf(gx), j0 = (int)floorf(gy), k0 = (int)floorf(gz);
+  if (i0 < 0 || j0 < 0 || k0 < 0) return 3.40282347e38f;
+  if (i0 + 1 >= dims[0] || j0 + 1 >= dims[1] || k0 + 1 >= dims[2]) return 3.40282347e38f;
+  float fx = gx - (float)i0, fy = gy - (float)j0, fz = gz - (float)k0;
+  size_t ny = dims[1], nz = dims[2];
+  size_t b = (size_t)i0 * ny * nz + (size_t)j0 * nz + (size_t)k0, si = ny * nz, sj = nz;
+  float c00 = d[b] * (1.0f - fz) + d[b + 1] * fz;
+  float c01 = d[b + sj] * (1.0f - fz) + d[b + sj + 1] * fz;
+  float c10 = d[b + si] * (1.0f - fz) + d[b + si + 1] * fz;
+  float c11 = d[b + si + sj] * (1.0f - fz) + d[b + si + sj + 1] * fz;
+  float c0 = c00 * (1.0f - fy) + c01 * fy;
+  float c1 = c10 * (1.0f - fy) + c11 * fy;
+  return c0 * (1.0f - fx) + c1 * fx;
+}
+
+// One warp per surface node: Shepard-averaged fluid pressure (terms sorted by
+// particle index, force.rs:88-100), then -p n dA and r x F in f32 as the
+// reference computes them (force.rs:103-119). out[node] = (Fx, Fy, Fz, Mx, My,
+// Mz) or zeros when no fluid particle is in support.
+constexpr int kSurfWarps = 4;
+__global__ void __launch_bounds__(kSurfWarps * 32)
+k_surface_nodes(SimConst k, int nnodes, const float4* __restrict__ node_pos,
+                const float4* __restrict__ node_nrm, float d_area, const float4* __restrict__ pos,
+                const float* __restrict__ pr, const uint32_t* __restrict__ id,
+                const uint2* __restrict__ ctab, float* __restrict__ out, uint32_t* __restrict__ err) {
+  __shared__ uint32_t s_id[kSurfWarps][kAdamiCap];
+  __shared__ float s_w[kSurfWarps][kAdamiCap];
+  __shared__ float s_wp[kSurfWarps][kAdamiCap];
+  int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  int nd = blockIdx.x * kSurfWarps + warp;
+  if (nd >= nnodes) return;
+  float4 np4 = node_pos[nd];
+  float c[3] = {np4.x, np4.y, np4.z};
+  int lo[3], hi[3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    lo[a] = axis_cell(c[a] - k.reach, k.gmin[a], k.cell, k.dims[a]);
+    hi[a] = axis_cell(c[a] + k.reach, k.gmin[a], k.cell, k.dims[a]);
+  }
+  int count = 0;
+  bool overflow = false;
+  int nx = hi[0] - lo[0] + 1, ny = hi[1] - lo[1] + 1, nz = hi[2] - lo[2] + 1;
+  int ncell = nx * ny * nz;
+  for (int cbase = 0; cbase < ncell; cbase += 32) {
+    int q = cbase + lane;
+    uint2 mine = make_uint2(0u, 0u);
+    if (q < ncell) {
+      int qx = q % nx, qy = (q / nx) % ny, qz = q / (nx * ny);
+      mine = __ldg(&ctab[cell_hash(lo[0] + qx, lo[1] + qy, lo[2] + qz, k)]);
+    }
+    unsigned occupied = __ballot_sync(0xffffffffu, mine.y > 0u);
+    while (occupied) {
+      int src = __ffs(occupied) - 1;
+      occupied &= occupied - 1u;
+      uint32_t st = __shfl_sync(0xffffffffu, mine.x, src);
+      uint32_t cn = __shfl_sync(0xffffffffu, mine.y, src);
+      for (uint32_t base = st; base < st + cn; base += 32) {
+        uint32_t s = base + lane;
+        bool inr = false;
+        float w = 0.0f, wp = 0.0f;
+        uint32_t fid = 0;
+        if (s < st + cn) {
+          float4 pf = __ldg(&pos[s]);
+          float dx = pf.x - np4.x, dy = pf.y - np4.y, dz = pf.z - np4.z;
+          float d2 = dx * dx + dy * dy + dz * dz;
+          if (d2 <= k.sup_d2) {
+            inr = true;
+            w = w_c2(sqrtf(d2), k);
+            wp = __ldg(&pr[s]) * w;
+            fid = __ldg(&id[s]) & kIdMask;
+          }
+        }
+        unsigned m = __ballot_sync(0xffffffffu, inr);
+        int off = count + __popc(m & ((1u << lane) - 1u));
+        if (inr) {
+          if (off < kAdamiCap) { s_id[warp][off] = fid; s_w[warp][off] = w; s_wp[warp][off] = wp; }
+          else overflow = true;
+        }
+        count += __popc(m);
+      }
+    }
+  }
+  if (__any_sync(0xffffffffu, overflow) || count > kAdamiCap) {
+    if (lane == 0) atomicOr(err, kErrAdamiCap);
+    return;
+  }
+  int m2 = 1;
+  while (m2 < count) m2 <<= 1;
+  for (int q = count + lane; q < m2; q += 32) s_id[warp][q] = 0xffffffffu;
+  __syncwarp();
+  for (int kk = 2; kk <= m2; kk <<= 1)
+    for (int j = kk >> 1; j > 0; j >>= 1) {
+      for (int q = lane; q < m2; q += 32) {
+        int pq = q ^ j;
+        if (pq > q) {
+          bool up = (q & kk) == 0;
+          uint32_t a = s_id[warp][q], cc = s_id[warp][pq];
+          if ((a > cc) == up) {
+            s_id[warp][q] = cc; s_id[warp][pq] = a;
+            float t = s_w[warp][q]; s_w[warp][q] = s_w[warp][pq]; s_w[warp][pq] = t;
+            t = s_wp[warp][q]; s_wp[warp][q] = s_wp[warp][pq]; s_wp[warp][pq] = t;
+          }
+        }
+      }
+      __syncwarp();
+    }
+  if (lane == 0) {
+    float lp = 0.0f, ws = 0.0f;
+    for (int q = 0; q < count; ++q) { lp += s_wp[warp][q]; ws += s_w[warp][q]; }
+    float f[6] = {0, 0, 0, 0, 0, 0};
+    if (ws > 1e-12f) {
+      lp = lp / ws;
+      float4 n = node_nrm[nd];
+      float fx = -lp * n.x * d_area, fy = -lp * n.y * d_area, fz = -lp * n.z * d_area;
+      f[0] = fx; f[1] = fy; f[2] = fz;
+      f[3] = np4.y * fz - np4.z * fy;
+      f[4] = np4.z * fx - np4.x * fz;
+      f[5] = np4.x * fy - np4.y * fx;
+    }
+    for (int a = 0; a < 6; ++a) out[(size_t)nd * 6 + a] = f[a];
+  }
+}
+
+// Deterministic FP64 sum of `cols` interleaved columns of f32 rows (one
+// block; fixed thread->row assignment and tree order).
+__global__ void k_sum_rows_f64(int rows, int cols, const float* __restrict__ in, double* __restrict__ out) {
+  __shared__ double sh[256];
+  for (int c = 0; c < cols; ++c) {
+    double acc = 0.0;
+    for (int r = threadIdx.x; r < rows; r += blockDim.x) acc += (double)in[(size_t)r * cols + c];
+    sh[threadIdx.x] = acc;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+      if ((int)threadIdx.x < o) sh[threadIdx.x] += sh[threadIdx.x + o];
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) out[c] = sh[0];
+    __syncthreads();
+  }
+}
+
+// Reaction of the fluid on the boundary particles [b_first, b_first+b_count)
+// from the last force computation, per block in FP64: the boundary pressure
+// force (sph.rs:391-408) and repulsion (boundary.rs:161-179) the fluid
+// receives from them, negated; and the Monaghan viscous force with the body
+// at rest (diagnostic; the reference has no wall viscosity). 18 columns:
+// pressure F, M; repulsion F, M; viscous F, M (moments about the origin at
+// the boundary particle's position).
+constexpr int kBodyCols = 18;
+__global__ void __launch_bounds__(256)
+k_body_force(SimConst k, int n, uint32_t b_first, uint32_t b_count, const float4* __restrict__ pos,
+             const float4* __restrict__ vel, const float2* __restrict__ rf, const float* __restrict__ pr,
+             const uint32_t* __restrict__ id, const uint32_t* __restrict__ bc_start,
+             const uint32_t* __restrict__ bc_list, const float4* __restrict__ bpos,
+             const float* __restrict__ bpress, double* __restrict__ part) {
+  double acc[kBodyCols];
+#pragma unroll
+  for (int c = 0; c < kBodyCols; ++c) acc[c] = 0.0;
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) {
+    float4 pi = pos[i];
+    int lin = cell_hash(axis_cell(pi.x, k.gmin[0], k.cell, k.dims[0]),
+                        axis_cell(pi.y, k.gmin[1], k.cell, k.dims[1]),
+                        axis_cell(pi.z, k.gmin[2], k.cell, k.dims[2]), k);
+    uint32_t q0 = bc_start[lin], q1 = bc_start[lin + 1];
+    if (q1 > q0) {
+      float4 vi = vel[i];
+      float2 rfi = rf[i];
+      bool air = (id[i] & kAirBit) != 0;
+      float rest = air ? kAirRho0 : kWaterRho0;
+      float pic_over = fmaxf(pr[i], 0.0f) / (rfi.x * rfi.x);
+      for (uint32_t q = q0; q < q1; ++q) {
+        uint32_t b = bc_list[q];
+        if (b < b_first || b >= b_first + b_count) continue;
+        float4 bp = bpos[b];
+        float dx = pi.x - bp.x, dy = pi.y - bp.y, dz = pi.z - bp.z;
+        float d2 = dx * dx + dy * dy + dz * dz;
+        if (!(d2 <= k.sup_d2)) continue;
+        float r = sqrtf(d2);
+        float gx, gy, gz;
+        grad_c2(dx, dy, dz, r, k, gx, gy, gz);
+        float factor = -pi.w * bp.w * (pic_over + bpress[b] / (rest * rest));
+        double F[3] = {-(double)(factor * gx), -(double)(factor * gy), -(double)(factor * gz)};
+        double R[3] = {0.0, 0.0, 0.0};
+        if (d2 <= k.r0_d2 && d2 > k.tiny_d2) {
+          float s = 1.0f - r / k.r0;
+          float fm = k.rep_d * s * s / k.r0;
+          float inv_r = 1.0f / r;
+          R[0] = -(double)pi.w * (double)(fm * dx * inv_r);
+          R[1] = -(double)pi.w * (double)(fm * dy * inv_r);
+          R[2] = -(double)pi.w * (double)(fm * dz * inv_r);
+        }
+        double V[3] = {0.0, 0.0, 0.0};
+        float vr = vi.x * dx + vi.y * dy + vi.z * dz;
+        if (vr < 0.0f) {
+          float mu = k.h * vr / (r * r + k.eta_sq);
+          float pij = (k.neg_alpha_c * mu + k.beta * mu * mu) / (0.5f * (rfi.x + rest));
+          float fv = -pi.w * bp.w * pij;
+          V[0] = -(double)(fv * gx); V[1] = -(double)(fv * gy); V[2] = -(double)(fv * gz);
+        }
+        double X[3] = {bp.x, bp.y, bp.z};
+        const double* G[3] = {F, R, V};
+        for (int t = 0; t < 3; ++t) {
+          acc[6 * t + 0] += G[t][0]; acc[6 * t + 1] += G[t][1]; acc[6 * t + 2] += G[t][2];
+          acc[6 * t + 3] += X[1] * G[t][2] - X[2] * G[t][1];
+          acc[6 * t + 4] += X[2] * G[t][0] - X[0] * G[t][2];
+          acc[6 * t + 5] += X[0] * G[t][1] - X[1] * G[t][0];
+        }
+      }
+    }
+  }
+  __shared__ double sh[256];
+  for (int c = 0; c < kBodyCols; ++c) {
+    sh[threadIdx.x] = acc[c];
+    __syncthreads();
+    for (int o = 128; o > 0; o >>= 1) {
+      if ((int)threadIdx.x < o) sh[threadIdx.x] += sh[threadIdx.x + o];
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) part[(size_t)blockIdx.x * kBodyCols + c] = sh[0];
+    __syncthreads();
+  }
+}
+
+__global__ void k_sum_parts_f64(int parts, int cols, const double* __restrict__ in, double* __restrict__ out) {
+  int c = threadIdx.x;
+  if (c >= cols) return;
+  double s = 0.0;
+  for (int p = 0; p < parts; ++p) s += in[(size_t)p * cols + c];
+  out[c] = s;
 }
 
 }  // namespace sph

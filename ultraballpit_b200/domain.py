@@ -291,6 +291,35 @@ def dam_break(dx: float, seed: int = 1234, sphere: bool = False, alpha: float = 
         sdf=sdf, extras=extras)
 
 
+def tank_with_sphere(dx: float, domain_max=(0.12, 0.08, 0.08), center=(0.06, 0.04, 0.035),
+                     radius: float = 0.02, fill_height: float | None = None, seed: int = 5,
+                     alpha: float = 0.02, sdf_cell: float = 0.002, velocity=(0.0, 0.0, 0.0)) -> Scenario:
+    """A closed tank filled with water up to ``fill_height`` around a fixed
+    sphere. Lattice points inside the solid (sphere SDF < 0) are skipped as
+    ``place_fluid_particles`` does (domain.rs:127-130); the sphere becomes
+    geometry boundary particles (domain.rs:351-402) and is merged into the
+    SDF. ``velocity`` is an initial uniform fluid velocity."""
+    dmin = (0.0, 0.0, 0.0)
+    dmax = tuple(float(v) for v in domain_max)
+    dx32 = f32(dx)
+    fill = dmax[2] if fill_height is None else fill_height
+    counts = (_axis_count(0.0, dmax[0], dx32), _axis_count(0.0, dmax[1], dx32), _axis_count(0.0, fill, dx32))
+    sph = sphere_sdf(dmin, dmax, sdf_cell, center, radius)
+    parts = block_particles(dmin, counts, dx32, seed)
+    pts = np.stack([parts.x, parts.y, parts.z], axis=-1)
+    keep = sdf_sample(sph, pts) >= f32(0)
+    p = ParticleArrays.from_positions(parts.x[keep], parts.y[keep], parts.z[keep], particle_mass(dx32))
+    p.vx[:], p.vy[:], p.vz[:] = (f32(v) for v in velocity)
+    m = particle_mass(dx32)
+    walls = wall_boundary_particles(dmin, dmax, dx32, m)
+    geo = geometry_boundary_particles(sph, dmin, dmax, dx32, m)
+    sdf = merge_sdf(box_sdf(dmin, dmax, sdf_cell), sph)
+    return Scenario(f"tank_sphere_dx{dx*1e3:g}mm", p, concat_boundary(walls, geo), float(smoothing_length(dx32)),
+                    (0.0, 0.0, -9.81), dam_break_c0(fill), 0.25, 0.0, dmin, dmax, alpha=alpha, sdf=sdf,
+                    extras=dict(sphere_center=center, sphere_radius=radius, sphere_sdf=sph,
+                                n_geometry_boundary=len(geo), n_wall_boundary=len(walls)))
+
+
 def two_particles(h: float = 0.05) -> Scenario:
     """``kernel/tests/two_particle.rs:11-24``: two particles h apart on x."""
     p = ParticleArrays.from_positions([0.0, h], [0.0, 0.0], [0.0, 0.0], 0.001)

@@ -39,7 +39,8 @@ EXPORTS = (
     "sph_read_boundary_pressure", "sph_error_metrics", "sph_particle_count",
     "sph_save_checkpoint", "sph_restore_checkpoint", "sph_synchronize", "sph_health",
     "sph_last_error", "sph_stream", "sph_launch_count", "sph_grid_info", "sph_read_grid",
-    "sph_neighbors", "sph_grid_sort_noalloc",
+    "sph_neighbors", "sph_grid_sort_noalloc", "sph_set_geometry_sdf", "sph_surface_forces",
+    "sph_body_force",
 )
 
 
@@ -93,6 +94,16 @@ class SphStepProfile(C.Structure):
         return {k: float(getattr(self, k)) for k, _ in self._fields_}
 
 
+class SphSurfaceForce(C.Structure):
+    _fields_ = [("force", C.c_double * 3), ("moment", C.c_double * 3), ("force_f32", C.c_float * 3),
+                ("moment_f32", C.c_float * 3), ("nodes", C.c_uint32), ("active_nodes", C.c_uint32)]
+
+
+class SphBodyForce(C.Structure):
+    _fields_ = [(k, C.c_double * 3) for k in ("pressure_force", "pressure_moment", "repulsion_force",
+                                              "repulsion_moment", "viscous_force", "viscous_moment")]
+
+
 class SphGridInfo(C.Structure):
     _fields_ = [("dims", C.c_uint32 * 3), ("total_cells", C.c_uint32), ("cell_size", C.c_float),
                 ("grid_min", C.c_float * 3), ("boundary_candidates", C.c_uint64)]
@@ -139,13 +150,17 @@ def load_library(path: str | None = None):
     L.sph_grid_info.argtypes = [H, C.POINTER(SphGridInfo)]
     L.sph_read_grid.argtypes = [H, _U32P, _U32P, _U32P, _U32P, _U32P]
     L.sph_neighbors.argtypes = [H, C.c_uint32, _U32P, C.c_size_t, C.POINTER(C.c_size_t)]
+    L.sph_set_geometry_sdf.argtypes = [H, C.POINTER(SphSdfView)]
+    L.sph_surface_forces.argtypes = [H, C.POINTER(SphSurfaceForce)]
+    L.sph_body_force.argtypes = [H, C.c_uint32, C.c_uint32, C.POINTER(SphBodyForce)]
     for name in EXPORTS:
         fn = getattr(L, name)
         if getattr(fn, "restype", None) is C.c_int or name in (
                 "sph_create", "sph_step", "sph_step_auto", "sph_compute_timestep", "sph_step_profiled",
                 "sph_read_particles", "sph_read_boundary_pressure", "sph_error_metrics",
                 "sph_save_checkpoint", "sph_restore_checkpoint", "sph_synchronize", "sph_health",
-                "sph_grid_info", "sph_read_grid", "sph_neighbors"):
+                "sph_grid_info", "sph_read_grid", "sph_neighbors", "sph_set_geometry_sdf",
+                "sph_surface_forces", "sph_body_force"):
             fn.restype = C.c_int
     _lib = L
     return L
@@ -347,6 +362,27 @@ class CudaKernel(SimulationKernel):
             "cell_linear", "morton_key", "cell_count", "cell_start", "slot_id")]), "sph_read_grid")
         out.update(info)
         return out
+
+    def set_geometry_sdf(self, sdf: GridSDF) -> None:
+        """Register the obstacle SDF used by ``surface_forces``."""
+        self._geo = np.ascontiguousarray(sdf.distances, np.float32)
+        sv = SphSdfView((C.c_float * 3)(*map(float, sdf.origin)), float(sdf.cell_size),
+                        (C.c_uint32 * 3)(*map(int, sdf.dimensions)), _fp(self._geo))
+        self._check(self._lib.sph_set_geometry_sdf(self._h, C.byref(sv)), "sph_set_geometry_sdf")
+
+    def surface_forces(self) -> dict:
+        """``compute_surface_forces`` (force.rs:39-129) on the device."""
+        o = SphSurfaceForce()
+        self._check(self._lib.sph_surface_forces(self._h, C.byref(o)), "sph_surface_forces")
+        return dict(force=np.array(o.force), moment=np.array(o.moment),
+                    force_f32=np.array(o.force_f32, np.float32), moment_f32=np.array(o.moment_f32, np.float32),
+                    nodes=int(o.nodes), active_nodes=int(o.active_nodes))
+
+    def body_force(self, first: int, count: int) -> dict:
+        """Fluid reaction on boundary particles [first, first + count)."""
+        o = SphBodyForce()
+        self._check(self._lib.sph_body_force(self._h, int(first), int(count), C.byref(o)), "sph_body_force")
+        return {k: np.array(getattr(o, k)) for k, _ in SphBodyForce._fields_}
 
     def neighbors(self, pid: int, cap: int = 4096) -> np.ndarray:
         out = np.zeros(cap, np.uint32)
