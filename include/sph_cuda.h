@@ -160,6 +160,13 @@ typedef struct SphBodyForce {
   double viscous_force[3], viscous_moment[3];
 } SphBodyForce;
 
+/* Threads per block of the three neighbour kernels (32..512, multiple of 32). */
+typedef struct SphLaunch {
+  int32_t xsph_threads;
+  int32_t density_threads;
+  int32_t forces_threads;
+} SphLaunch;
+
 typedef struct SphGridInfo {
   uint32_t dims[3];
   uint32_t total_cells;
@@ -214,6 +221,32 @@ const char *sph_last_error(const SphHandle *h);
 void *sph_stream(SphHandle *h);
 /* Total kernels this handle has launched (graph replays counted per node). */
 uint64_t sph_launch_count(const SphHandle *h);
+
+/* ---- batches of independent simulations (no reference counterpart) -----
+ * `ninst` simulations on one device stepped by the same kernel launches
+ * (one launch per stage for the whole batch), each with its own grid,
+ * constants, walls and dt. Boundary-particle mode only; `boundaries` may be
+ * NULL or hold n = 0 entries. Every single-simulation entry point works on
+ * a batch handle: sph_step sets one dt for all instances, sph_step_auto
+ * computes one dt per instance on the device, sph_read_particles returns
+ * the instances one after another (see sph_batch_info), sph_error_metrics
+ * sums over all instances. */
+int sph_batch_create(int ninst, const SphParams *params, const SphParticlesView *particles,
+                     const SphBoundaryView *boundaries, SphHandle **out);
+/* Instance count, and per instance the first particle and particle count in
+ * the concatenated order (first/count may be NULL, else ninst entries). */
+int sph_batch_info(const SphHandle *h, int *ninst, size_t *first, size_t *count);
+/* Per-instance sph::compute_timestep on the device (ninst floats). */
+int sph_batch_timesteps(SphHandle *h, float *dt_out);
+/* Launch shapes of the neighbour kernels (graphs are recaptured). */
+int sph_set_launch(SphHandle *h, const SphLaunch *launch);
+int sph_get_launch(const SphHandle *h, SphLaunch *launch);
+/* Autotuner: times each kernel at 64/128/256/512 threads per block over
+ * `trial_steps` profiled steps (after one untimed step) and applies the
+ * fastest shape per kernel. Results are cached per process by device name
+ * and instance-size histogram; a cache hit runs no step. The trial steps
+ * advance the simulation: tune a scratch handle of the same workload. */
+int sph_autotune(SphHandle *h, int trial_steps, SphLaunch *best);
 
 /* ---- force extraction ------------------------------------------------- */
 /* Register the geometry SDF whose surface force sph_surface_forces returns

@@ -7,6 +7,8 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <new>
 #include <string>
 #include <vector>
@@ -34,8 +36,19 @@ struct SphHandle {
   int dev = 0;
   cudaStream_t st = nullptr;
   SphParams prm{};
-  SimConst k{};
+  SimConst k{};  // constants of instance 0 (the simulation, for a single one)
   int n = 0, nb = 0, C = 0;
+  // batch: instances, their constants on the device, the instance of every
+  // particle slot and boundary particle, (h, c, cfl) for the dt finalize
+  int ninst = 1;
+  std::vector<SimConst> ktab_h;
+  SimConst* ktab = nullptr;
+  uint16_t *inst_p = nullptr, *inst_b = nullptr;
+  float4* hcc = nullptr;
+  std::vector<size_t> poff, boff;
+  std::vector<double> init_e, init_m;
+  // launch shapes (threads per block of the neighbour kernels)
+  int bs_xsph = 256, bs_density = 256, bs_forces = 256;
   std::vector<float> temperature;
   double init_energy = 0.0, init_mass = 0.0;
   bool needs_init = true;
@@ -308,6 +321,15 @@ void build_boundary_lists(const SimConst& k, const SphBoundaryView* b, int C,
   for (uint64_t pr : pairs) list[head[pr >> 32]++] = (uint32_t)(pr & 0xffffffffu);
 }
 
+// Calls f with the constants provider of the handle: the by-value constants
+// of a single simulation, or the per-instance table of a batch (indexed by
+// particle slot, or by boundary particle when `boundary`).
+template <class F>
+void dispatch(SphHandle* h, bool boundary, F&& f) {
+  if (h->ninst == 1) f(sph::OneSim{h->k});
+  else f(sph::ManySim{h->ktab, boundary ? h->inst_b : h->inst_p});
+}
+
 // Sorting scratch + binning of posU into the cell tables (k_bin or the
 // xsph kernel fill `hist` first).
 void enqueue_scan_fill(SphHandle* h) {
@@ -323,46 +345,61 @@ void enqueue_scan_fill(SphHandle* h) {
 
 void enqueue_density_adami(SphHandle* h) {
   using namespace sph;
-  k_density<<<grid_for(h->n, 256), 256, 0, h->st>>>(h->k, h->n, h->dt, h->pos, h->rv, h->id, h->ctab,
-                                                    h->bc_start, h->bc_list, h->bpos, h->rf, h->pr,
-                                                    h->err, h->nbr, h->ncount, h->sdf, h->wall_tab);
+  int bs = h->bs_density;
+  dispatch(h, false, [&](auto kp) {
+    k_density<<<grid_for(h->n, bs), bs, 0, h->st>>>(kp, h->n, h->dt, h->pos, h->rv, h->id, h->ctab,
+                                                    h->bc_start, h->bc_list, h->bpos, h->rf, h->pr, h->err,
+                                                    h->nbr, h->ncount, h->sdf, h->wall_tab);
+  });
   h->launches += 1;
   if (h->nb > 0) {
-    k_adami<<<grid_for(h->nb, kAdamiWarps), kAdamiWarps * 32, 0, h->st>>>(
-        h->k, h->nb, h->bpos, h->bpress, h->pos, h->rf, h->pr, h->id, h->ctab, h->err);
+    dispatch(h, true, [&](auto kp) {
+      k_adami<<<grid_for(h->nb, kAdamiWarps), kAdamiWarps * 32, 0, h->st>>>(
+          kp, h->nb, h->bpos, h->bpress, h->pos, h->rf, h->pr, h->id, h->ctab, h->err);
+    });
     h->launches += 1;
   }
 }
 
 void enqueue_forces(SphHandle* h, float hdt_scale) {
   using namespace sph;
-  cudaMemsetAsync(h->red, 0, 2 * sizeof(float), h->st);
-  k_forces<<<grid_for(h->n, 256), 256, 0, h->st>>>(h->k, h->n, h->dt, hdt_scale, h->pos, h->vel, h->rf,
-                                                   h->pr, h->id, h->ctab, h->bc_start, h->bc_list,
-                                                   h->bpos, h->bpress, h->acc, h->velout, h->red,
-                                                   h->err, h->nbr, h->ncount, h->sdf, h->wall_tab);
+  cudaMemsetAsync(h->red, 0, 2 * sizeof(float) * h->ninst, h->st);
+  int bs = h->bs_forces;
+  dispatch(h, false, [&](auto kp) {
+    k_forces<<<grid_for(h->n, bs), bs, 0, h->st>>>(kp, h->n, h->dt, hdt_scale, h->pos, h->vel, h->rf, h->pr,
+                                                   h->id, h->ctab, h->bc_start, h->bc_list, h->bpos,
+                                                   h->bpress, h->acc, h->velout, h->red, h->err, h->nbr,
+                                                   h->ncount, h->sdf, h->wall_tab);
+  });
   h->launches += 1;
 }
 
-void enqueue_xsph_sort(SphHandle* h, bool use_list) {
+void enqueue_xsph(SphHandle* h, bool use_list) {
   using namespace sph;
-  k_xsph_drift<<<grid_for(h->n, 256), 256, 0, h->st>>>(h->k, h->n, h->dt, h->pos, h->velout, h->acc,
-                                                       h->id, h->ctab, h->rank_of_lin, h->posU,
-                                                       h->velU, h->idU, h->keyU, h->hist, h->err,
+  int bs = h->bs_xsph;
+  dispatch(h, false, [&](auto kp) {
+    k_xsph_drift<<<grid_for(h->n, bs), bs, 0, h->st>>>(kp, h->n, h->dt, h->pos, h->velout, h->acc, h->id,
+                                                       h->ctab, h->rank_of_lin, h->posU, h->velU, h->idU,
+                                                       h->keyU, h->hist, h->err,
                                                        use_list ? h->nbr : nullptr, h->ncount);
+  });
   h->launches += 1;
+}
+
+void enqueue_sort(SphHandle* h) {
+  using namespace sph;
   enqueue_scan_fill(h);
-  k_reorder<<<grid_for(h->n, 256), 256, 0, h->st>>>(h->n, h->tmp, h->tmpid, h->keyU, h->cstart,
-                                                    h->ccount, h->posU, h->velU, h->pos, h->vel, h->rv,
-                                                    h->id, h->err, nullptr, nullptr, nullptr, nullptr,
-                                                    nullptr);
+  k_reorder<<<grid_for(h->n, 256), 256, 0, h->st>>>(h->n, h->tmp, h->tmpid, h->keyU, h->cstart, h->ccount,
+                                                    h->posU, h->velU, h->pos, h->vel, h->rv, h->id, h->err,
+                                                    nullptr, nullptr, nullptr, nullptr, nullptr);
   h->launches += 1;
 }
 
 // lib.rs:287-335 after the bootstrap: kick1+XSPH+drift+clamp, grid + reorder,
 // density, boundary pressure, forces + kick2.
 void enqueue_body(SphHandle* h, bool use_list) {
-  enqueue_xsph_sort(h, use_list);
+  enqueue_xsph(h, use_list);
+  enqueue_sort(h);
   enqueue_density_adami(h);
   enqueue_forces(h, 1.0f);
 }
@@ -373,12 +410,21 @@ void enqueue_bootstrap(SphHandle* h) {
   enqueue_forces(h, 0.0f);
 }
 
+void enqueue_dt_finalize(SphHandle* h, float* out) {
+  sph::k_dt_finalize<<<grid_for(h->ninst, 128), 128, 0, h->st>>>(h->ninst, h->hcc, h->red, out);
+  h->launches += 1;
+}
+
+void enqueue_set_dt(SphHandle* h, float dt) {
+  sph::k_set_dt<<<1, 256, 0, h->st>>>(h->dt, h->ninst, dt);
+  h->launches += 1;
+}
+
 int capture(SphHandle* h, bool with_finalize, cudaGraphExec_t* out) {
   cudaGraph_t g = nullptr;
   uint64_t before = h->launches;
   SPH_TRY(h, cudaStreamBeginCapture(h->st, cudaStreamCaptureModeThreadLocal));
-  if (with_finalize)
-    sph::k_dt_finalize<<<1, 1, 0, h->st>>>(h->k.h, h->k.c, h->prm.cfl_number, h->red, h->dt);
+  if (with_finalize) enqueue_dt_finalize(h, h->dt);
   enqueue_body(h, true);
   cudaError_t e = cudaStreamEndCapture(h->st, &g);
   if (e != cudaSuccess) return cuda_status(h, e, "cudaStreamEndCapture");
@@ -387,6 +433,13 @@ int capture(SphHandle* h, bool with_finalize, cudaGraphExec_t* out) {
   e = cudaGraphInstantiate(out, g, 0);
   cudaGraphDestroy(g);
   return cuda_status(h, e, "cudaGraphInstantiate");
+}
+
+void drop_graphs(SphHandle* h) {
+  if (h->g_step) cudaGraphExecDestroy(h->g_step);
+  if (h->g_auto) cudaGraphExecDestroy(h->g_auto);
+  h->g_step = nullptr;
+  h->g_auto = nullptr;
 }
 
 int check_device_flags(SphHandle* h) {
@@ -402,20 +455,288 @@ int check_device_flags(SphHandle* h) {
 
 void ensure_red(SphHandle* h) {
   if (h->red_valid) return;
-  cudaMemsetAsync(h->red, 0, 2 * sizeof(float), h->st);
+  cudaMemsetAsync(h->red, 0, 2 * sizeof(float) * h->ninst, h->st);
   if (h->n > 0) {
-    sph::k_timestep_reduce<<<grid_for(h->n, 256), 256, 0, h->st>>>(h->k, h->n, h->velout, h->acc, h->red);
+    dispatch(h, false, [&](auto kp) {
+      sph::k_timestep_reduce<<<grid_for(h->n, 256), 256, 0, h->st>>>(kp, h->n, h->velout, h->acc, h->red);
+    });
     h->launches += 1;
   }
   h->red_valid = true;
 }
 
 void free_all(SphHandle* h) {
-  if (h->g_step) cudaGraphExecDestroy(h->g_step);
-  if (h->g_auto) cudaGraphExecDestroy(h->g_auto);
+  drop_graphs(h);
   for (void* p : h->allocs) cudaFree(p);
   h->allocs.clear();
   if (h->st) cudaStreamDestroy(h->st);
+}
+
+int check_views(const SphParams& P, const SphParticlesView* pv, const SphBoundaryView* bv) {
+  if (!pv) return SPH_ERR_INVALID_ARG;
+  if (!(P.h > 0.0f) || !std::isfinite(P.h) || !(P.speed_of_sound > 0.0f)) return SPH_ERR_INVALID_ARG;
+  for (int a = 0; a < 3; ++a)
+    if (!(P.domain_max[a] > P.domain_min[a])) return SPH_ERR_INVALID_ARG;
+  if (pv->n > 0x7fffffffull) return SPH_ERR_INVALID_ARG;
+  if (pv->n > 0 && (!pv->x || !pv->y || !pv->z || !pv->vx || !pv->vy || !pv->vz || !pv->ax || !pv->ay ||
+                    !pv->az || !pv->density || !pv->pressure || !pv->mass || !pv->temperature ||
+                    !pv->fluid_type))
+    return SPH_ERR_INVALID_ARG;
+  if (bv && bv->n > 0 && (!bv->x || !bv->y || !bv->z || !bv->mass)) return SPH_ERR_INVALID_ARG;
+  if (bv && bv->n > 0x7fffffffull) return SPH_ERR_INVALID_ARG;
+  if (P.boundary_mode != SPH_BOUNDARY_PARTICLES && P.boundary_mode != SPH_BOUNDARY_SDF)
+    return SPH_ERR_INVALID_ARG;
+  return SPH_OK;
+}
+
+// One handle for `ninst` independent simulations on one device. Each
+// instance keeps its own grid, constants, boundary lists and dt; instances
+// occupy disjoint ranges of the global cell ranks, so the global counting
+// sort keeps every instance in a fixed contiguous slot range.
+int create_impl(int ninst, const SphParams* PP, const SphParticlesView* pvs,
+                const SphBoundaryView* const* bvs, const SphSdfView* sdf, SphHandle** out) {
+  if (!out) return SPH_ERR_INVALID_ARG;
+  *out = nullptr;
+  if (ninst < 1 || ninst > 65535 || !PP || !pvs) return SPH_ERR_INVALID_ARG;
+  const bool sdf_mode = PP[0].boundary_mode == SPH_BOUNDARY_SDF;
+  uint64_t ntot = 0, nbtot = 0;
+  for (int q = 0; q < ninst; ++q) {
+    const SphBoundaryView* bv = bvs ? bvs[q] : nullptr;
+    int s = check_views(PP[q], &pvs[q], bv);
+    if (s != SPH_OK) return s;
+    if (PP[q].device != PP[0].device) return SPH_ERR_INVALID_ARG;
+    if ((PP[q].boundary_mode == SPH_BOUNDARY_SDF) != sdf_mode) return SPH_ERR_INVALID_ARG;
+    ntot += pvs[q].n;
+    if (!sdf_mode && bv) nbtot += bv->n;
+  }
+  if (ntot > 0x7fffffffull || nbtot > 0x7fffffffull) return SPH_ERR_INVALID_ARG;
+  uint64_t sdf_nodes = 0;
+  if (sdf_mode) {
+    if (ninst != 1) return SPH_ERR_INVALID_ARG;  // the SDF wall mode is single-simulation
+    if (!sdf || !sdf->distances || !(sdf->cell_size > 0.0f)) return SPH_ERR_INVALID_ARG;
+    if (sdf->dims[0] < 2 || sdf->dims[1] < 2 || sdf->dims[2] < 2) return SPH_ERR_INVALID_ARG;
+    sdf_nodes = (uint64_t)sdf->dims[0] * sdf->dims[1] * sdf->dims[2];
+  }
+  const SphParams& P0 = PP[0];
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0 || P0.device < 0 || P0.device >= ndev) {
+    cudaGetLastError();
+    return SPH_ERR_NO_DEVICE;
+  }
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, P0.device) != cudaSuccess || prop.major != 10) {
+    cudaGetLastError();
+    return SPH_ERR_NO_DEVICE;
+  }
+
+  SphHandle* h = new (std::nothrow) SphHandle();
+  if (!h) return SPH_ERR_OOM;
+  h->prm = P0;
+  h->dev = P0.device;
+  h->ninst = ninst;
+  h->n = (int)ntot;
+  h->nb = (int)nbtot;
+  auto fail = [&](int code) {
+    free_all(h);
+    delete h;
+    return code;
+  };
+  if (cudaSetDevice(h->dev) != cudaSuccess) return fail(SPH_ERR_NO_DEVICE);
+
+  // per-instance grids (neighbor.rs:29-46), constants and cell ranks: Morton
+  // order within an instance (21 bits per axis; the 30-bit key when all dims
+  // <= 1024) or linear order, instances one after another.
+  std::vector<uint32_t> lin_of_rank, rank_of_lin, bstart, blist;
+  std::vector<float4> hcc(ninst);
+  h->ktab_h.resize(ninst);
+  h->poff.assign(ninst + 1, 0);
+  h->boff.assign(ninst + 1, 0);
+  h->init_e.assign(ninst, 0.0);
+  h->init_m.assign(ninst, 0.0);
+  uint64_t C = 0;
+  bstart.push_back(0);
+  for (int q = 0; q < ninst; ++q) {
+    const SphParams& P = PP[q];
+    const SphParticlesView* pv = &pvs[q];
+    const SphBoundaryView* bv = (sdf_mode || !bvs) ? nullptr : bvs[q];
+    uint32_t dims[3];
+    float cell = 2.0f * P.h;
+    uint64_t Cq = 1;
+    for (int a = 0; a < 3; ++a) {
+      dims[a] = (uint32_t)fmaxf(ceilf((P.domain_max[a] - P.domain_min[a]) / cell), 1.0f);
+      Cq *= dims[a];
+      if (dims[a] > (1u << 21)) return fail(SPH_ERR_INVALID_ARG);
+    }
+    if (C + Cq > (1ull << 30)) return fail(SPH_ERR_INVALID_ARG);
+    SimConst k = make_const(P, dims);
+    k.inst = q;
+    k.coff = (int)C;
+    k.cfl = P.cfl_number;
+    if (sdf_mode) {
+      k.sdf_mode = 1;
+      for (int a = 0; a < 3; ++a) {
+        k.sdf_origin[a] = sdf->origin[a];
+        k.sdf_dims[a] = (int)sdf->dims[a];
+      }
+      k.sdf_cell = sdf->cell_size;
+      k.wall_mid = 1.5f * (P.h / 1.3f);
+    }
+    h->ktab_h[q] = k;
+    hcc[q] = make_float4(P.h, P.speed_of_sound, P.cfl_number, 0.0f);
+    std::vector<std::pair<uint64_t, uint32_t>> cells(Cq);
+    for (uint32_t cz = 0; cz < dims[2]; ++cz)
+      for (uint32_t cy = 0; cy < dims[1]; ++cy)
+        for (uint32_t cx = 0; cx < dims[0]; ++cx) {
+          uint32_t lin = cx + cy * dims[0] + cz * dims[0] * dims[1];
+          uint64_t key = P.cell_order == SPH_CELL_ORDER_LINEAR
+                             ? lin
+                             : (spread21(cx) | (spread21(cy) << 1) | (spread21(cz) << 2));
+          cells[lin] = {key, lin};
+        }
+    std::sort(cells.begin(), cells.end());
+    lin_of_rank.resize(C + Cq);
+    rank_of_lin.resize(C + Cq);
+    for (uint64_t r = 0; r < Cq; ++r) {
+      lin_of_rank[C + r] = (uint32_t)(C + cells[r].second);
+      rank_of_lin[C + cells[r].second] = (uint32_t)(C + r);
+    }
+    std::vector<uint32_t> s1, l1;
+    build_boundary_lists(k, bv, (int)Cq, s1, l1);
+    uint32_t base = (uint32_t)blist.size(), bbase = (uint32_t)h->boff[q];
+    for (uint64_t c = 1; c <= Cq; ++c) bstart.push_back(base + s1[c]);
+    for (uint32_t b : l1) blist.push_back(bbase + b);
+    h->poff[q + 1] = h->poff[q] + pv->n;
+    h->boff[q + 1] = h->boff[q] + (bv ? bv->n : 0);
+    // initial conservation totals, in the reference's order (lib.rs:152-156)
+    double m = 0.0, e = 0.0;
+    for (size_t i = 0; i < pv->n; ++i) m += (double)pv->mass[i];
+    for (size_t i = 0; i < pv->n; ++i) {
+      double mi = (double)pv->mass[i];
+      double vx = pv->vx[i], vy = pv->vy[i], vz = pv->vz[i];
+      e += 0.5 * mi * (vx * vx + vy * vy + vz * vz);
+      double x = pv->x[i], y = pv->y[i], z = pv->z[i];
+      e -= mi * ((double)P.gravity[0] * x + (double)P.gravity[1] * y + (double)P.gravity[2] * z);
+    }
+    h->init_m[q] = m;
+    h->init_e[q] = e;
+    C += Cq;
+  }
+  h->k = h->ktab_h[0];
+  h->C = (int)C;
+  h->boundary_candidates = blist.size();
+  for (int q = 0; q < ninst; ++q) {
+    h->init_mass += h->init_m[q];
+    h->init_energy += h->init_e[q];
+  }
+  std::vector<float2> wall_host;
+  if (sdf_mode) wall_host = make_wall_table(P0.h, &h->ktab_h[0].wall_inv_step);
+  h->k = h->ktab_h[0];
+
+  if (cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking) != cudaSuccess) return fail(SPH_ERR_CUDA);
+  size_t n = (size_t)h->n, nb = (size_t)h->nb;
+  h->nbsum = grid_for(h->C, sph::kScanTile);
+  h->nparts = std::max(1, std::min(grid_for((long long)n, sph::kMetricThreads), 1184));
+  cudaError_t e = cudaSuccess;
+#define ALLOC(ptr, cnt) \
+  if (e == cudaSuccess) e = dalloc(h, &h->ptr, (cnt))
+  ALLOC(pos, n); ALLOC(vel, n); ALLOC(velout, n); ALLOC(acc, n);
+  ALLOC(rv, n); ALLOC(rf, n); ALLOC(pr, n); ALLOC(id, n);
+  ALLOC(posU, n); ALLOC(velU, n); ALLOC(idU, n); ALLOC(keyU, n); ALLOC(tmp, n); ALLOC(tmpid, n);
+  ALLOC(hist, C); ALLOC(cstart, C); ALLOC(ccount, C); ALLOC(cursor, C); ALLOC(bsum, h->nbsum);
+  ALLOC(rank_of_lin, C); ALLOC(lin_of_rank, C); ALLOC(ctab, C);
+  ALLOC(bpos, nb); ALLOC(bpress, nb); ALLOC(bc_start, C + 1); ALLOC(bc_list, blist.size());
+  ALLOC(dt, ninst); ALLOC(dt_query, ninst); ALLOC(red, 2 * ninst); ALLOC(err, 1); ALLOC(hcc, ninst);
+  ALLOC(part_m, h->nparts); ALLOC(part_e, h->nparts); ALLOC(part_var, h->nparts); ALLOC(me, 2);
+  ALLOC(var, 1); ALLOC(bad, 1);
+  ALLOC(stage, 12 * n); ALLOC(stage_ft, n); ALLOC(diag, 2);
+  ALLOC(nbr, (size_t)sph::kNbrCap * n); ALLOC(ncount, n);
+  if (ninst > 1) {
+    ALLOC(ktab, ninst); ALLOC(inst_p, n); ALLOC(inst_b, nb);
+  }
+  if (sdf_mode) ALLOC(sdf, sdf_nodes);
+  if (sdf_mode) ALLOC(wall_tab, wall_host.size());
+#undef ALLOC
+  if (e != cudaSuccess) return fail(e == cudaErrorMemoryAllocation ? SPH_ERR_OOM : SPH_ERR_CUDA);
+
+  // upload (particles of instance q at [poff[q], poff[q+1]), ids global)
+  std::vector<float4> hpos(n), hvel(n), hacc(n), hb(nb);
+  std::vector<uint32_t> hid(n);
+  std::vector<float> hpr(n);
+  std::vector<uint16_t> hip(ninst > 1 ? n : 0), hib(ninst > 1 ? nb : 0);
+  h->temperature.resize(n);
+  for (int q = 0; q < ninst; ++q) {
+    const SphParticlesView* pv = &pvs[q];
+    size_t o = h->poff[q];
+    for (size_t i = 0; i < pv->n; ++i) {
+      hpos[o + i] = make_float4(pv->x[i], pv->y[i], pv->z[i], pv->mass[i]);
+      hvel[o + i] = make_float4(pv->vx[i], pv->vy[i], pv->vz[i], pv->density[i]);
+      hacc[o + i] = make_float4(pv->ax[i], pv->ay[i], pv->az[i], 0.0f);
+      hid[o + i] = (uint32_t)(o + i) | (pv->fluid_type[i] ? sph::kAirBit : 0u);
+      hpr[o + i] = pv->pressure[i];
+      h->temperature[o + i] = pv->temperature[i];
+      if (ninst > 1) hip[o + i] = (uint16_t)q;
+    }
+    const SphBoundaryView* bv = (sdf_mode || !bvs) ? nullptr : bvs[q];
+    size_t bo = h->boff[q];
+    for (size_t i = 0; bv && i < bv->n; ++i) {
+      hb[bo + i] = make_float4(bv->x[i], bv->y[i], bv->z[i], bv->mass[i]);
+      if (ninst > 1) hib[bo + i] = (uint16_t)q;
+    }
+  }
+  float4* accU = nullptr;
+  float* prU = nullptr;
+  auto up = [&](void* d, const void* src, size_t bytes) {
+    if (e == cudaSuccess && bytes) e = cudaMemcpyAsync(d, src, bytes, cudaMemcpyHostToDevice, h->st);
+  };
+  if (e == cudaSuccess) e = cudaMalloc(&accU, std::max<size_t>(1, n) * sizeof(float4));
+  if (e == cudaSuccess) e = cudaMalloc(&prU, std::max<size_t>(1, n) * sizeof(float));
+  up(h->posU, hpos.data(), n * sizeof(float4));
+  up(h->velU, hvel.data(), n * sizeof(float4));
+  up(accU, hacc.data(), n * sizeof(float4));
+  up(prU, hpr.data(), n * sizeof(float));
+  up(h->idU, hid.data(), n * sizeof(uint32_t));
+  up(h->bpos, hb.data(), nb * sizeof(float4));
+  up(h->rank_of_lin, rank_of_lin.data(), C * sizeof(uint32_t));
+  up(h->lin_of_rank, lin_of_rank.data(), C * sizeof(uint32_t));
+  up(h->bc_start, bstart.data(), (C + 1) * sizeof(uint32_t));
+  up(h->bc_list, blist.data(), blist.size() * sizeof(uint32_t));
+  up(h->hcc, hcc.data(), ninst * sizeof(float4));
+  if (ninst > 1) {
+    up(h->ktab, h->ktab_h.data(), ninst * sizeof(SimConst));
+    up(h->inst_p, hip.data(), n * sizeof(uint16_t));
+    up(h->inst_b, hib.data(), nb * sizeof(uint16_t));
+  }
+  if (sdf_mode) up(h->sdf, sdf->distances, sdf_nodes * sizeof(float));
+  if (sdf_mode) up(h->wall_tab, wall_host.data(), wall_host.size() * sizeof(float2));
+  if (e == cudaSuccess) e = cudaMemsetAsync(h->hist, 0, C * sizeof(uint32_t), h->st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(h->bpress, 0, std::max<size_t>(1, nb) * sizeof(float), h->st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(h->err, 0, sizeof(uint32_t), h->st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(h->ctab, 0, C * sizeof(uint2), h->st);
+  if (e == cudaSuccess && n > 0) {
+    using namespace sph;
+    dispatch(h, false, [&](auto kp) {
+      k_bin<<<grid_for(h->n, 256), 256, 0, h->st>>>(kp, h->n, h->posU, h->rank_of_lin, h->keyU, h->hist);
+    });
+    h->launches += 1;
+    enqueue_scan_fill(h);
+    k_reorder<<<grid_for(h->n, 256), 256, 0, h->st>>>(h->n, h->tmp, h->tmpid, h->keyU, h->cstart,
+                                                      h->ccount, h->posU, h->velU, h->pos, h->vel, h->rv,
+                                                      h->id, h->err, accU, h->acc, prU, h->pr, h->velout);
+    h->launches += 1;
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->st);
+  if (accU) cudaFree(accU);
+  if (prU) cudaFree(prU);
+  if (e != cudaSuccess) {
+    fprintf(stderr, "sph_create: %s\n", cudaGetErrorString(e));
+    return fail(e == cudaErrorMemoryAllocation ? SPH_ERR_OOM : SPH_ERR_CUDA);
+  }
+  ensure_red(h);
+  int st = check_device_flags(h);
+  if (st != SPH_OK) return fail(st);
+  *out = h;
+  return SPH_OK;
 }
 
 }  // namespace
@@ -440,198 +761,20 @@ int sph_create(const SphParams* params, const SphParticlesView* pv, const SphBou
   if (!out) return SPH_ERR_INVALID_ARG;
   *out = nullptr;
   if (!params || !pv) return SPH_ERR_INVALID_ARG;
-  const SphParams& P = *params;
-  if (!(P.h > 0.0f) || !std::isfinite(P.h) || !(P.speed_of_sound > 0.0f)) return SPH_ERR_INVALID_ARG;
-  for (int a = 0; a < 3; ++a)
-    if (!(P.domain_max[a] > P.domain_min[a])) return SPH_ERR_INVALID_ARG;
-  if (pv->n > 0x7fffffffull) return SPH_ERR_INVALID_ARG;
-  if (pv->n > 0 && (!pv->x || !pv->y || !pv->z || !pv->vx || !pv->vy || !pv->vz || !pv->ax || !pv->ay ||
-                    !pv->az || !pv->density || !pv->pressure || !pv->mass || !pv->temperature ||
-                    !pv->fluid_type))
-    return SPH_ERR_INVALID_ARG;
-  if (bv && bv->n > 0 && (!bv->x || !bv->y || !bv->z || !bv->mass)) return SPH_ERR_INVALID_ARG;
-  if (bv && bv->n > 0x7fffffffull) return SPH_ERR_INVALID_ARG;
-  if (P.boundary_mode != SPH_BOUNDARY_PARTICLES && P.boundary_mode != SPH_BOUNDARY_SDF)
-    return SPH_ERR_INVALID_ARG;
-  const bool sdf_mode = P.boundary_mode == SPH_BOUNDARY_SDF;
-  uint64_t sdf_nodes = 0;
-  if (sdf_mode) {
-    if (!sdf || !sdf->distances || !(sdf->cell_size > 0.0f)) return SPH_ERR_INVALID_ARG;
-    if (sdf->dims[0] < 2 || sdf->dims[1] < 2 || sdf->dims[2] < 2) return SPH_ERR_INVALID_ARG;
-    sdf_nodes = (uint64_t)sdf->dims[0] * sdf->dims[1] * sdf->dims[2];
-    bv = nullptr;  // walls come from the SDF
-  }
+  const SphBoundaryView* bvs[1] = {bv};
+  return create_impl(1, params, pv, bvs, sdf, out);
+}
 
-  int ndev = 0;
-  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0 || P.device < 0 || P.device >= ndev) {
-    cudaGetLastError();
-    return SPH_ERR_NO_DEVICE;
-  }
-  cudaDeviceProp prop;
-  if (cudaGetDeviceProperties(&prop, P.device) != cudaSuccess || prop.major != 10) {
-    cudaGetLastError();
-    return SPH_ERR_NO_DEVICE;
-  }
-
-  SphHandle* h = new (std::nothrow) SphHandle();
-  if (!h) return SPH_ERR_OOM;
-  h->prm = P;
-  h->dev = P.device;
-  h->n = (int)pv->n;
-  h->nb = bv ? (int)bv->n : 0;
-  auto fail = [&](int code) {
-    free_all(h);
-    delete h;
-    return code;
-  };
-  if (cudaSetDevice(h->dev) != cudaSuccess) return fail(SPH_ERR_NO_DEVICE);
-
-  // grid (neighbor.rs:29-46)
-  uint32_t dims[3];
-  float cell = 2.0f * P.h;
-  uint64_t C = 1;
-  for (int a = 0; a < 3; ++a) {
-    dims[a] = (uint32_t)fmaxf(ceilf((P.domain_max[a] - P.domain_min[a]) / cell), 1.0f);
-    C *= dims[a];
-  }
-  if (C > (1ull << 30) || dims[0] > (1u << 21) || dims[1] > (1u << 21) || dims[2] > (1u << 21))
-    return fail(SPH_ERR_INVALID_ARG);
-  h->C = (int)C;
-  h->k = make_const(P, dims);
-  if (sdf_mode) {
-    h->nb = 0;
-    h->k.sdf_mode = 1;
-    for (int a = 0; a < 3; ++a) {
-      h->k.sdf_origin[a] = sdf->origin[a];
-      h->k.sdf_dims[a] = (int)sdf->dims[a];
-    }
-    h->k.sdf_cell = sdf->cell_size;
-    h->k.wall_mid = 1.5f * (P.h / 1.3f);
-  }
-  std::vector<float2> wall_host;
-  if (sdf_mode) wall_host = make_wall_table(P.h, &h->k.wall_inv_step);
-
-  // cell ranks: Morton order (21 bits per axis; the 30-bit key when all
-  // dims <= 1024) or linear order.
-  std::vector<uint32_t> lin_of_rank(C), rank_of_lin(C);
-  {
-    std::vector<std::pair<uint64_t, uint32_t>> cells(C);
-    for (uint32_t cz = 0; cz < dims[2]; ++cz)
-      for (uint32_t cy = 0; cy < dims[1]; ++cy)
-        for (uint32_t cx = 0; cx < dims[0]; ++cx) {
-          uint32_t lin = cx + cy * dims[0] + cz * dims[0] * dims[1];
-          uint64_t key = P.cell_order == SPH_CELL_ORDER_LINEAR
-                             ? lin
-                             : (spread21(cx) | (spread21(cy) << 1) | (spread21(cz) << 2));
-          cells[lin] = {key, lin};
-        }
-    std::sort(cells.begin(), cells.end());
-    for (uint64_t r = 0; r < C; ++r) {
-      lin_of_rank[r] = cells[r].second;
-      rank_of_lin[cells[r].second] = (uint32_t)r;
-    }
-  }
-  std::vector<uint32_t> bstart, blist;
-  build_boundary_lists(h->k, bv, h->C, bstart, blist);
-  h->boundary_candidates = blist.size();
-
-  // host-side initial conservation totals, in the reference's order
-  h->temperature.assign(pv->temperature ? pv->temperature : nullptr,
-                        pv->temperature ? pv->temperature + pv->n : nullptr);
-  {
-    double m = 0.0, e = 0.0;
-    for (size_t i = 0; i < pv->n; ++i) m += (double)pv->mass[i];
-    for (size_t i = 0; i < pv->n; ++i) {
-      double mi = (double)pv->mass[i];
-      double vx = pv->vx[i], vy = pv->vy[i], vz = pv->vz[i];
-      e += 0.5 * mi * (vx * vx + vy * vy + vz * vz);
-      double x = pv->x[i], y = pv->y[i], z = pv->z[i];
-      e -= mi * ((double)P.gravity[0] * x + (double)P.gravity[1] * y + (double)P.gravity[2] * z);
-    }
-    h->init_mass = m;
-    h->init_energy = e;
-  }
-
-  if (cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking) != cudaSuccess) return fail(SPH_ERR_CUDA);
-  size_t n = (size_t)h->n, nb = (size_t)h->nb;
-  h->nbsum = grid_for(h->C, sph::kScanTile);
-  h->nparts = std::max(1, std::min(grid_for((long long)n, sph::kMetricThreads), 1184));
-  cudaError_t e = cudaSuccess;
-#define ALLOC(ptr, cnt) \
-  if (e == cudaSuccess) e = dalloc(h, &h->ptr, (cnt))
-  ALLOC(pos, n); ALLOC(vel, n); ALLOC(velout, n); ALLOC(acc, n);
-  ALLOC(rv, n); ALLOC(rf, n); ALLOC(pr, n); ALLOC(id, n);
-  ALLOC(posU, n); ALLOC(velU, n); ALLOC(idU, n); ALLOC(keyU, n); ALLOC(tmp, n); ALLOC(tmpid, n);
-  ALLOC(hist, C); ALLOC(cstart, C); ALLOC(ccount, C); ALLOC(cursor, C); ALLOC(bsum, h->nbsum);
-  ALLOC(rank_of_lin, C); ALLOC(lin_of_rank, C); ALLOC(ctab, C);
-  ALLOC(bpos, nb); ALLOC(bpress, nb); ALLOC(bc_start, C + 1); ALLOC(bc_list, blist.size());
-  ALLOC(dt, 1); ALLOC(dt_query, 1); ALLOC(red, 2); ALLOC(err, 1);
-  ALLOC(part_m, h->nparts); ALLOC(part_e, h->nparts); ALLOC(part_var, h->nparts); ALLOC(me, 2);
-  ALLOC(var, 1); ALLOC(bad, 1);
-  ALLOC(stage, 12 * n); ALLOC(stage_ft, n); ALLOC(diag, 2);
-  ALLOC(nbr, (size_t)sph::kNbrCap * n); ALLOC(ncount, n);
-  if (sdf_mode) ALLOC(sdf, sdf_nodes);
-  if (sdf_mode) ALLOC(wall_tab, wall_host.size());
-#undef ALLOC
-  if (e != cudaSuccess) return fail(e == cudaErrorMemoryAllocation ? SPH_ERR_OOM : SPH_ERR_CUDA);
-
-  // upload
-  std::vector<float4> hpos(n), hvel(n), hacc(n);
-  std::vector<uint32_t> hid(n);
-  for (size_t i = 0; i < n; ++i) {
-    hpos[i] = make_float4(pv->x[i], pv->y[i], pv->z[i], pv->mass[i]);
-    hvel[i] = make_float4(pv->vx[i], pv->vy[i], pv->vz[i], pv->density[i]);
-    hacc[i] = make_float4(pv->ax[i], pv->ay[i], pv->az[i], 0.0f);
-    hid[i] = (uint32_t)i | (pv->fluid_type[i] ? sph::kAirBit : 0u);
-  }
-  std::vector<float4> hb(nb);
-  for (size_t i = 0; i < nb; ++i) hb[i] = make_float4(bv->x[i], bv->y[i], bv->z[i], bv->mass[i]);
-  float4* accU = nullptr;
-  float* prU = nullptr;
-  auto up = [&](void* d, const void* s, size_t bytes) {
-    if (e == cudaSuccess && bytes) e = cudaMemcpyAsync(d, s, bytes, cudaMemcpyHostToDevice, h->st);
-  };
-  if (e == cudaSuccess) e = cudaMalloc(&accU, std::max<size_t>(1, n) * sizeof(float4));
-  if (e == cudaSuccess) e = cudaMalloc(&prU, std::max<size_t>(1, n) * sizeof(float));
-  up(h->posU, hpos.data(), n * sizeof(float4));
-  up(h->velU, hvel.data(), n * sizeof(float4));
-  up(accU, hacc.data(), n * sizeof(float4));
-  up(prU, pv->pressure, n * sizeof(float));
-  up(h->idU, hid.data(), n * sizeof(uint32_t));
-  up(h->bpos, hb.data(), nb * sizeof(float4));
-  up(h->rank_of_lin, rank_of_lin.data(), C * sizeof(uint32_t));
-  up(h->lin_of_rank, lin_of_rank.data(), C * sizeof(uint32_t));
-  up(h->bc_start, bstart.data(), (C + 1) * sizeof(uint32_t));
-  up(h->bc_list, blist.data(), blist.size() * sizeof(uint32_t));
-  if (sdf_mode) up(h->sdf, sdf->distances, sdf_nodes * sizeof(float));
-  if (sdf_mode) up(h->wall_tab, wall_host.data(), wall_host.size() * sizeof(float2));
-  if (e == cudaSuccess) e = cudaMemsetAsync(h->hist, 0, C * sizeof(uint32_t), h->st);
-  if (e == cudaSuccess) e = cudaMemsetAsync(h->bpress, 0, std::max<size_t>(1, nb) * sizeof(float), h->st);
-  if (e == cudaSuccess) e = cudaMemsetAsync(h->err, 0, sizeof(uint32_t), h->st);
-  if (e == cudaSuccess) e = cudaMemsetAsync(h->ctab, 0, C * sizeof(uint2), h->st);
-  if (e == cudaSuccess && n > 0) {
-    using namespace sph;
-    k_bin<<<grid_for(h->n, 256), 256, 0, h->st>>>(h->k, h->n, h->posU, h->rank_of_lin, h->keyU, h->hist);
-    h->launches += 1;
-    enqueue_scan_fill(h);
-    k_reorder<<<grid_for(h->n, 256), 256, 0, h->st>>>(h->n, h->tmp, h->tmpid, h->keyU, h->cstart,
-                                                      h->ccount, h->posU, h->velU, h->pos, h->vel, h->rv,
-                                                      h->id, h->err, accU, h->acc, prU, h->pr, h->velout);
-    h->launches += 1;
-    e = cudaGetLastError();
-  }
-  if (e == cudaSuccess) e = cudaStreamSynchronize(h->st);
-  if (accU) cudaFree(accU);
-  if (prU) cudaFree(prU);
-  if (e != cudaSuccess) {
-    fprintf(stderr, "sph_create: %s\n", cudaGetErrorString(e));
-    return fail(e == cudaErrorMemoryAllocation ? SPH_ERR_OOM : SPH_ERR_CUDA);
-  }
-  ensure_red(h);
-  int s = check_device_flags(h);
-  if (s != SPH_OK) return fail(s);
-  *out = h;
-  return SPH_OK;
+int sph_batch_create(int ninst, const SphParams* params, const SphParticlesView* particles,
+                     const SphBoundaryView* boundaries, SphHandle** out) {
+  if (!out) return SPH_ERR_INVALID_ARG;
+  *out = nullptr;
+  if (ninst < 1 || !params || !particles) return SPH_ERR_INVALID_ARG;
+  std::vector<const SphBoundaryView*> bvs(ninst, nullptr);
+  for (int q = 0; q < ninst && boundaries; ++q) bvs[q] = boundaries[q].n ? &boundaries[q] : nullptr;
+  for (int q = 0; q < ninst; ++q)
+    if (params[q].boundary_mode != SPH_BOUNDARY_PARTICLES) return SPH_ERR_INVALID_ARG;
+  return create_impl(ninst, params, particles, bvs.data(), nullptr, out);
 }
 
 void sph_destroy(SphHandle* h) {
@@ -647,8 +790,7 @@ int sph_step(SphHandle* h, float dt) {
   if (!std::isfinite(dt)) return set_err(h, SPH_ERR_INVALID_ARG, "dt must be finite");
   SPH_TRY(h, cudaSetDevice(h->dev));
   if (h->n == 0) return SPH_OK;
-  sph::k_set_dt<<<1, 1, 0, h->st>>>(h->dt, dt);
-  h->launches += 1;
+  enqueue_set_dt(h, dt);
   if (h->needs_init) {
     enqueue_bootstrap(h);
     h->needs_init = false;
@@ -677,8 +819,7 @@ int sph_step_auto(SphHandle* h, int nsteps, float* dt_out) {
   for (int s = 0; s < nsteps; ++s) {
     ensure_red(h);
     if (h->needs_init || !h->list_valid) {
-      sph::k_dt_finalize<<<1, 1, 0, h->st>>>(h->k.h, h->k.c, h->prm.cfl_number, h->red, h->dt);
-      h->launches += 1;
+      enqueue_dt_finalize(h, h->dt);
       if (h->needs_init) {
         enqueue_bootstrap(h);
         h->needs_init = false;
@@ -713,8 +854,7 @@ int sph_compute_timestep(SphHandle* h, float* dt_out) {
     return SPH_OK;
   }
   ensure_red(h);
-  sph::k_dt_finalize<<<1, 1, 0, h->st>>>(h->k.h, h->k.c, h->prm.cfl_number, h->red, h->dt_query);
-  h->launches += 1;
+  enqueue_dt_finalize(h, h->dt_query);
   SPH_TRY(h, cudaMemcpyAsync(dt_out, h->dt_query, sizeof(float), cudaMemcpyDeviceToHost, h->st));
   SPH_TRY(h, cudaStreamSynchronize(h->st));
   return check_device_flags(h);
@@ -726,8 +866,7 @@ int sph_step_profiled(SphHandle* h, float dt, SphStepProfile* prof) {
   SPH_TRY(h, cudaSetDevice(h->dev));
   std::memset(prof, 0, sizeof(*prof));
   if (h->n == 0) return SPH_OK;
-  sph::k_set_dt<<<1, 1, 0, h->st>>>(h->dt, dt);
-  h->launches += 1;
+  enqueue_set_dt(h, dt);
   if (h->needs_init) {
     enqueue_bootstrap(h);
     h->needs_init = false;
@@ -735,29 +874,28 @@ int sph_step_profiled(SphHandle* h, float dt, SphStepProfile* prof) {
   }
   cudaEvent_t ev[6];
   for (int i = 0; i < 6; ++i) SPH_TRY(h, cudaEventCreate(&ev[i]));
-  using namespace sph;
   cudaEventRecord(ev[0], h->st);
-  k_xsph_drift<<<grid_for(h->n, 256), 256, 0, h->st>>>(h->k, h->n, h->dt, h->pos, h->velout, h->acc,
-                                                       h->id, h->ctab, h->rank_of_lin, h->posU, h->velU,
-                                                       h->idU, h->keyU, h->hist, h->err,
-                                                       h->list_valid ? h->nbr : nullptr, h->ncount);
-  h->launches += 1;
+  enqueue_xsph(h, h->list_valid);
   cudaEventRecord(ev[1], h->st);
-  enqueue_scan_fill(h);
-  k_reorder<<<grid_for(h->n, 256), 256, 0, h->st>>>(h->n, h->tmp, h->tmpid, h->keyU, h->cstart, h->ccount,
-                                                    h->posU, h->velU, h->pos, h->vel, h->rv, h->id, h->err,
-                                                    nullptr, nullptr, nullptr, nullptr, nullptr);
-  h->launches += 1;
+  enqueue_sort(h);
   cudaEventRecord(ev[2], h->st);
-  k_density<<<grid_for(h->n, 256), 256, 0, h->st>>>(h->k, h->n, h->dt, h->pos, h->rv, h->id, h->ctab,
-                                                    h->bc_start, h->bc_list, h->bpos, h->rf, h->pr, h->err,
-                                                    h->nbr, h->ncount, h->sdf, h->wall_tab);
-  h->launches += 1;
-  cudaEventRecord(ev[3], h->st);
-  if (h->nb > 0) {
-    k_adami<<<grid_for(h->nb, kAdamiWarps), kAdamiWarps * 32, 0, h->st>>>(
-        h->k, h->nb, h->bpos, h->bpress, h->pos, h->rf, h->pr, h->id, h->ctab, h->err);
+  {
+    using namespace sph;
+    int bs = h->bs_density;
+    dispatch(h, false, [&](auto kp) {
+      k_density<<<grid_for(h->n, bs), bs, 0, h->st>>>(kp, h->n, h->dt, h->pos, h->rv, h->id, h->ctab,
+                                                      h->bc_start, h->bc_list, h->bpos, h->rf, h->pr,
+                                                      h->err, h->nbr, h->ncount, h->sdf, h->wall_tab);
+    });
     h->launches += 1;
+    cudaEventRecord(ev[3], h->st);
+    if (h->nb > 0) {
+      dispatch(h, true, [&](auto kp) {
+        k_adami<<<grid_for(h->nb, kAdamiWarps), kAdamiWarps * 32, 0, h->st>>>(
+            kp, h->nb, h->bpos, h->bpress, h->pos, h->rf, h->pr, h->id, h->ctab, h->err);
+      });
+      h->launches += 1;
+    }
   }
   cudaEventRecord(ev[4], h->st);
   enqueue_forces(h, 1.0f);
@@ -1003,6 +1141,114 @@ int sph_body_force(SphHandle* h, uint32_t first, uint32_t count, SphBodyForce* o
   for (int t = 0; t < 6; ++t)
     for (int a = 0; a < 3; ++a) dst[t][a] = v[3 * t + a];
   return check_device_flags(h);
+}
+
+int sph_batch_info(const SphHandle* h, int* ninst, size_t* first, size_t* count) {
+  if (!h || !ninst) return SPH_ERR_INVALID_ARG;
+  *ninst = h->ninst;
+  for (int q = 0; q < h->ninst; ++q) {
+    if (first) first[q] = h->poff[q];
+    if (count) count[q] = h->poff[q + 1] - h->poff[q];
+  }
+  return SPH_OK;
+}
+
+int sph_batch_timesteps(SphHandle* h, float* dt_out) {
+  if (!h || !dt_out) return SPH_ERR_INVALID_ARG;
+  SPH_TRY(h, cudaSetDevice(h->dev));
+  if (h->n == 0) return SPH_ERR_INVALID_ARG;
+  ensure_red(h);
+  enqueue_dt_finalize(h, h->dt_query);
+  SPH_TRY(h, cudaMemcpyAsync(dt_out, h->dt_query, sizeof(float) * h->ninst, cudaMemcpyDeviceToHost, h->st));
+  SPH_TRY(h, cudaStreamSynchronize(h->st));
+  return check_device_flags(h);
+}
+
+int sph_set_launch(SphHandle* h, const SphLaunch* l) {
+  if (!h || !l) return SPH_ERR_INVALID_ARG;
+  int v[3] = {l->xsph_threads, l->density_threads, l->forces_threads};
+  for (int x : v)
+    if (x < 32 || x > 512 || (x & 31)) return set_err(h, SPH_ERR_INVALID_ARG, "threads per block");
+  h->bs_xsph = v[0];
+  h->bs_density = v[1];
+  h->bs_forces = v[2];
+  drop_graphs(h);  // recaptured with the new shapes on the next step
+  return SPH_OK;
+}
+
+int sph_get_launch(const SphHandle* h, SphLaunch* l) {
+  if (!h || !l) return SPH_ERR_INVALID_ARG;
+  l->xsph_threads = h->bs_xsph;
+  l->density_threads = h->bs_density;
+  l->forces_threads = h->bs_forces;
+  return SPH_OK;
+}
+
+// Autotuner cache: (device name, instance count, log2 histogram of instance
+// sizes) -> best launch shapes.
+static std::mutex g_tune_mu;
+static std::map<std::string, SphLaunch> g_tune_cache;
+
+static std::string tune_key(SphHandle* h) {
+  cudaDeviceProp prop;
+  std::string key = cudaGetDeviceProperties(&prop, h->dev) == cudaSuccess ? prop.name : "?";
+  int hist[40] = {0};
+  for (int q = 0; q < h->ninst; ++q) {
+    size_t c = h->poff[q + 1] - h->poff[q];
+    int b = 0;
+    while ((c >> b) > 1 && b < 39) ++b;
+    hist[b]++;
+  }
+  key += "|" + std::to_string(h->ninst);
+  for (int b = 0; b < 40; ++b)
+    if (hist[b]) key += "|" + std::to_string(b) + ":" + std::to_string(hist[b]);
+  return key;
+}
+
+int sph_autotune(SphHandle* h, int trial_steps, SphLaunch* best) {
+  if (!h || !best || trial_steps < 1) return SPH_ERR_INVALID_ARG;
+  std::string key = tune_key(h);
+  {
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    auto it = g_tune_cache.find(key);
+    if (it != g_tune_cache.end()) {
+      *best = it->second;
+      return sph_set_launch(h, best);
+    }
+  }
+  const int cand[4] = {64, 128, 256, 512};
+  float t_best[3] = {1e30f, 1e30f, 1e30f};
+  int s_best[3] = {256, 256, 256};
+  float dt = 0.0f;
+  int st = sph_compute_timestep(h, &dt);
+  if (st != SPH_OK) return st;
+  // one untimed step so that every trial starts from a stepped state
+  SphStepProfile prof;
+  st = sph_step_profiled(h, dt, &prof);
+  if (st != SPH_OK) return st;
+  for (int c : cand) {
+    SphLaunch l{c, c, c};
+    st = sph_set_launch(h, &l);
+    if (st != SPH_OK) return st;
+    float acc[3] = {0.0f, 0.0f, 0.0f};
+    for (int r = 0; r < trial_steps; ++r) {
+      st = sph_step_profiled(h, dt, &prof);
+      if (st != SPH_OK) return st;
+      acc[0] += prof.xsph_drift_us;
+      acc[1] += prof.density_us;
+      acc[2] += prof.forces_us;
+    }
+    for (int a = 0; a < 3; ++a)
+      if (acc[a] < t_best[a]) { t_best[a] = acc[a]; s_best[a] = c; }
+  }
+  best->xsph_threads = s_best[0];
+  best->density_threads = s_best[1];
+  best->forces_threads = s_best[2];
+  {
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    g_tune_cache[key] = *best;
+  }
+  return sph_set_launch(h, best);
 }
 
 int sph_grid_info(SphHandle* h, SphGridInfo* out) {

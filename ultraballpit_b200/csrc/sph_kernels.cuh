@@ -62,6 +62,26 @@ struct SimConst {
   float sdf_origin[3];
   float sdf_cell;
   int sdf_dims[3];
+  // batch: this instance's index (dt and dt-maxima slots) and the offset of
+  // its cells in the global cell tables (0 for a single simulation)
+  int inst;
+  int coff;
+  float cfl;
+};
+
+// Constants provider of a single simulation: the constants ride in the
+// kernel parameter space.
+struct OneSim {
+  SimConst k;
+  __device__ __forceinline__ const SimConst& at(int) const { return k; }
+};
+
+// Constants provider of a batch: per-instance constants, and the instance
+// of every slot (particles of an instance occupy a fixed slot range).
+struct ManySim {
+  const SimConst* __restrict__ tab;
+  const uint16_t* __restrict__ inst;
+  __device__ __forceinline__ const SimConst& at(int i) const { return tab[__ldg(&inst[i])]; }
 };
 
 // ---------------------------------------------------------------------------
@@ -245,7 +265,7 @@ __device__ __forceinline__ void for_each_neighbor(float px, float py, float pz, 
         int nx = cx + dx;
         if (nx < 0 || nx >= k.dims[0]) continue;
         if (ey + (dx < 0 ? lo2[0] : (dx > 0 ? hi2[0] : 0.0f)) > k.radius_sq) continue;
-        uint2 se = __ldg(&ctab[row + nx]);
+        uint2 se = __ldg(&ctab[k.coff + row + nx]);
         int end = (int)(se.x + se.y);
         for (int s = (int)se.x; s < end; ++s) {
           if (s == self) continue;
@@ -287,14 +307,17 @@ __device__ __forceinline__ void visit_neighbors(int i, int n, float px, float py
 // kernels
 // ---------------------------------------------------------------------------
 
-__global__ void k_set_dt(float* dt, float value) { *dt = value; }
+__global__ void k_set_dt(float* dt, int ninst, float value) {
+  for (int q = threadIdx.x; q < ninst; q += blockDim.x) dt[q] = value;
+}
 
 // Kick 1 (lib.rs:301-305) + XSPH (sph.rs:236-280) + drift (lib.rs:313-317)
 // + domain clamp (boundary.rs:239-291) + binning of the new position
 // (neighbor.rs:89-101) into a rank-indexed histogram. Reads the sorted state,
 // writes the unsorted "U" arrays in the same slot order.
-__global__ void __launch_bounds__(256)
-k_xsph_drift(SimConst k, int n, const float* __restrict__ dtp, const float4* __restrict__ pos,
+template <class KP>
+__global__ void __launch_bounds__(512)
+k_xsph_drift(KP kp, int n, const float* __restrict__ dtp, const float4* __restrict__ pos,
              const float4* __restrict__ velout, const float4* __restrict__ acc,
              const uint32_t* __restrict__ id, const uint2* __restrict__ ctab,
              const uint32_t* __restrict__ rank_of_lin, float4* __restrict__ posU,
@@ -303,7 +326,8 @@ k_xsph_drift(SimConst k, int n, const float* __restrict__ dtp, const float4* __r
              const uint32_t* __restrict__ nbr, const uint32_t* __restrict__ ncount) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n || *err) return;
-  float dt = *dtp;
+  const SimConst& k = kp.at(i);
+  float dt = dtp[k.inst];
   float hdt = 0.5f * dt;
   float4 pi = pos[i];
   float4 vi = velout[i];
@@ -349,22 +373,24 @@ k_xsph_drift(SimConst k, int n, const float* __restrict__ dtp, const float4* __r
   int lin = cell_hash(axis_cell(x, k.gmin[0], k.cell, k.dims[0]),
                       axis_cell(y, k.gmin[1], k.cell, k.dims[1]),
                       axis_cell(z, k.gmin[2], k.cell, k.dims[2]), k);
-  uint32_t r = __ldg(&rank_of_lin[lin]);
+  uint32_t r = __ldg(&rank_of_lin[k.coff + lin]);
   keyU[i] = r;
   atomicAdd(&hist[r], 1u);
 }
 
 // Binning of an unsorted state (creation, bootstrap) without moving it.
-__global__ void k_bin(SimConst k, int n, const float4* __restrict__ posU,
+template <class KP>
+__global__ void k_bin(KP kp, int n, const float4* __restrict__ posU,
                       const uint32_t* __restrict__ rank_of_lin, uint32_t* __restrict__ keyU,
                       uint32_t* __restrict__ hist) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
+  const SimConst& k = kp.at(i);
   float4 p = posU[i];
   int lin = cell_hash(axis_cell(p.x, k.gmin[0], k.cell, k.dims[0]),
                       axis_cell(p.y, k.gmin[1], k.cell, k.dims[1]),
                       axis_cell(p.z, k.gmin[2], k.cell, k.dims[2]), k);
-  uint32_t r = __ldg(&rank_of_lin[lin]);
+  uint32_t r = __ldg(&rank_of_lin[k.coff + lin]);
   keyU[i] = r;
   atomicAdd(&hist[r], 1u);
 }
@@ -508,8 +534,9 @@ k_reorder(int n, const uint32_t* __restrict__ tmp, const uint32_t* __restrict__ 
 
 // Density summation + delta-SPH + Tait EOS (lib.rs:213-237; sph.rs:112-216,
 // 295-312). One thread per sorted particle.
-__global__ void __launch_bounds__(256)
-k_density(SimConst k, int n, const float* __restrict__ dtp, const float4* __restrict__ pos,
+template <class KP>
+__global__ void __launch_bounds__(512)
+k_density(KP kp, int n, const float* __restrict__ dtp, const float4* __restrict__ pos,
           const float2* __restrict__ rv, const uint32_t* __restrict__ id,
           const uint2* __restrict__ ctab, const uint32_t* __restrict__ bc_start,
           const uint32_t* __restrict__ bc_list, const float4* __restrict__ bpos,
@@ -518,7 +545,8 @@ k_density(SimConst k, int n, const float* __restrict__ dtp, const float4* __rest
           const float2* __restrict__ wall_tab) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n || *err) return;
-  float dt = *dtp;
+  const SimConst& k = kp.at(i);
+  float dt = dtp[k.inst];
   float4 pi = pos[i];
   float rho_old_i = rv[i].x;
   float rho = pi.w * k.norm_h3;
@@ -558,7 +586,7 @@ k_density(SimConst k, int n, const float* __restrict__ dtp, const float4* __rest
   int lin = cell_hash(axis_cell(pi.x, k.gmin[0], k.cell, k.dims[0]),
                       axis_cell(pi.y, k.gmin[1], k.cell, k.dims[1]),
                       axis_cell(pi.z, k.gmin[2], k.cell, k.dims[2]), k);
-  uint32_t b0 = __ldg(&bc_start[lin]), b1 = __ldg(&bc_start[lin + 1]);
+  uint32_t b0 = __ldg(&bc_start[k.coff + lin]), b1 = __ldg(&bc_start[k.coff + lin + 1]);
   for (uint32_t q = b0; q < b1; ++q) {
     float4 bp = __ldg(&bpos[__ldg(&bc_list[q])]);
     float dx = pi.x - bp.x, dy = pi.y - bp.y, dz = pi.z - bp.z;
@@ -584,8 +612,9 @@ k_density(SimConst k, int n, const float* __restrict__ dtp, const float4* __rest
 // range, a warp bitonic sort orders them by fluid index, and lane 0 sums
 // them in that order.
 constexpr int kAdamiWarps = 4;
+template <class KP>
 __global__ void __launch_bounds__(kAdamiWarps * 32)
-k_adami(SimConst k, int nb, const float4* __restrict__ bpos, float* __restrict__ bpress,
+k_adami(KP kp, int nb, const float4* __restrict__ bpos, float* __restrict__ bpress,
         const float4* __restrict__ pos, const float2* __restrict__ rf, const float* __restrict__ pr,
         const uint32_t* __restrict__ id, const uint2* __restrict__ ctab, uint32_t* __restrict__ err) {
   __shared__ uint32_t s_id[kAdamiWarps][kAdamiCap];
@@ -594,6 +623,7 @@ k_adami(SimConst k, int nb, const float4* __restrict__ bpos, float* __restrict__
   int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   int b = blockIdx.x * kAdamiWarps + warp;
   if (b >= nb || *err) return;
+  const SimConst& k = kp.at(b);
   float4 bp = bpos[b];
   int lo[3], hi[3];
   float bc[3] = {bp.x, bp.y, bp.z};
@@ -614,7 +644,7 @@ k_adami(SimConst k, int nb, const float4* __restrict__ bpos, float* __restrict__
     uint2 mine = make_uint2(0u, 0u);
     if (q < ncell) {
       int qx = q % nx, qy = (q / nx) % ny, qz = q / (nx * ny);
-      mine = __ldg(&ctab[cell_hash(lo[0] + qx, lo[1] + qy, lo[2] + qz, k)]);
+      mine = __ldg(&ctab[k.coff + cell_hash(lo[0] + qx, lo[1] + qy, lo[2] + qz, k)]);
     }
     unsigned occupied = __ballot_sync(0xffffffffu, mine.y > 0u);
     while (occupied) {
@@ -693,8 +723,9 @@ k_adami(SimConst k, int nb, const float4* __restrict__ bpos, float* __restrict__
 // Pressure force + Monaghan viscosity + gravity + boundary pressure force +
 // repulsion (lib.rs:247-282; sph.rs:322-508; boundary.rs:143-181), then
 // kick 2 (lib.rs:330-334) and the dt reduction inputs (sph.rs:597-616).
-__global__ void __launch_bounds__(256)
-k_forces(SimConst k, int n, const float* __restrict__ dtp, float hdt_scale,
+template <class KP>
+__global__ void __launch_bounds__(512)
+k_forces(KP kp, int n, const float* __restrict__ dtp, float hdt_scale,
          const float4* __restrict__ pos, const float4* __restrict__ vel,
          const float2* __restrict__ rf, const float* __restrict__ pr,
          const uint32_t* __restrict__ id, const uint2* __restrict__ ctab,
@@ -706,8 +737,11 @@ k_forces(SimConst k, int n, const float* __restrict__ dtp, float hdt_scale,
          const float2* __restrict__ wall_tab) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   float sig = 0.0f, amag = 0.0f;
+  int inst = -1;
   if (i < n && !*err) {
-    float hdt = (0.5f * *dtp) * hdt_scale;
+    const SimConst& k = kp.at(i);
+    inst = k.inst;
+    float hdt = (0.5f * dtp[k.inst]) * hdt_scale;
     float4 pi = pos[i];
     float4 vi = vel[i];
     float2 rfi = rf[i];
@@ -742,7 +776,7 @@ k_forces(SimConst k, int n, const float* __restrict__ dtp, float hdt_scale,
     int lin = cell_hash(axis_cell(pi.x, k.gmin[0], k.cell, k.dims[0]),
                         axis_cell(pi.y, k.gmin[1], k.cell, k.dims[1]),
                         axis_cell(pi.z, k.gmin[2], k.cell, k.dims[2]), k);
-    uint32_t b0 = __ldg(&bc_start[lin]), b1 = __ldg(&bc_start[lin + 1]);
+    uint32_t b0 = __ldg(&bc_start[k.coff + lin]), b1 = __ldg(&bc_start[k.coff + lin + 1]);
     bool air = (id[i] & kAirBit) != 0;
     if (b1 > b0) {
       float pic = fmaxf(pr[i], 0.0f);
@@ -821,56 +855,55 @@ k_forces(SimConst k, int n, const float* __restrict__ dtp, float hdt_scale,
     if (!(sig >= 0.0f)) sig = 0.0f;    // NaN never wins (sph.rs:606)
     if (!(amag >= 0.0f)) amag = 0.0f;  // (sph.rs:613)
   }
-  // block max, one atomic per block
-  for (int o = 16; o > 0; o >>= 1) {
-    sig = fmaxf(sig, __shfl_xor_sync(0xffffffffu, sig, o));
-    amag = fmaxf(amag, __shfl_xor_sync(0xffffffffu, amag, o));
-  }
-  __shared__ float s_sig[8], s_a[8];
-  int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  if (lane == 0) { s_sig[wid] = sig; s_a[wid] = amag; }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    float a = s_sig[0], b = s_a[0];
-    for (int w = 1; w < (int)(blockDim.x >> 5); ++w) { a = fmaxf(a, s_sig[w]); b = fmaxf(b, s_a[w]); }
-    atomic_max_pos(&red[0], a);
-    atomic_max_pos(&red[1], b);
+  // per-instance maxima: a warp whose lanes share one instance reduces with
+  // shuffles and issues one atomic pair; a mixed warp issues per lane
+  int inst0 = __shfl_sync(0xffffffffu, inst, 0);
+  bool uniform = __all_sync(0xffffffffu, inst == inst0 || inst < 0);
+  if (uniform) {
+    for (int o = 16; o > 0; o >>= 1) {
+      sig = fmaxf(sig, __shfl_xor_sync(0xffffffffu, sig, o));
+      amag = fmaxf(amag, __shfl_xor_sync(0xffffffffu, amag, o));
+    }
+    if ((threadIdx.x & 31) == 0 && inst0 >= 0) {
+      atomic_max_pos(&red[2 * inst0], sig);
+      atomic_max_pos(&red[2 * inst0 + 1], amag);
+    }
+  } else if (inst >= 0) {
+    atomic_max_pos(&red[2 * inst], sig);
+    atomic_max_pos(&red[2 * inst + 1], amag);
   }
 }
 
 // dt reduction over an arbitrary state (creation, restore): same maxima as
 // the k_forces epilogue.
-__global__ void k_timestep_reduce(SimConst k, int n, const float4* __restrict__ velout,
+template <class KP>
+__global__ void k_timestep_reduce(KP kp, int n, const float4* __restrict__ velout,
                                   const float4* __restrict__ acc, float* __restrict__ red) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
-  float sig = 0.0f, amag = 0.0f;
-  if (i < n) {
-    float4 v = velout[i];
-    float4 a = acc[i];
-    sig = sqrtf(v.x * v.x + v.y * v.y + v.z * v.z) + k.c;
-    amag = sqrtf(a.x * a.x + a.y * a.y + a.z * a.z);
-    if (!(sig >= 0.0f)) sig = 0.0f;
-    if (!(amag >= 0.0f)) amag = 0.0f;
-  }
-  for (int o = 16; o > 0; o >>= 1) {
-    sig = fmaxf(sig, __shfl_xor_sync(0xffffffffu, sig, o));
-    amag = fmaxf(amag, __shfl_xor_sync(0xffffffffu, amag, o));
-  }
-  if ((threadIdx.x & 31) == 0) {
-    atomic_max_pos(&red[0], sig);
-    atomic_max_pos(&red[1], amag);
-  }
+  if (i >= n) return;
+  const SimConst& k = kp.at(i);
+  float4 v = velout[i];
+  float4 a = acc[i];
+  float sig = sqrtf(v.x * v.x + v.y * v.y + v.z * v.z) + k.c;
+  float amag = sqrtf(a.x * a.x + a.y * a.y + a.z * a.z);
+  if (sig >= 0.0f) atomic_max_pos(&red[2 * k.inst], sig);
+  if (amag >= 0.0f) atomic_max_pos(&red[2 * k.inst + 1], amag);
 }
 
 // sph.rs:591-628 from the reduced maxima.
-__global__ void k_dt_finalize(float h, float c, float cfl, const float* __restrict__ red,
+// Per instance (h, c, cfl in hcc[q]): dt = compute_timestep from its maxima.
+__global__ void k_dt_finalize(int ninst, const float4* __restrict__ hcc, const float* __restrict__ red,
                               float* __restrict__ dt_out) {
-  float max_signal = fmaxf(c, red[0]);
-  float max_accel = red[1];
-  float dt_cfl = cfl * h / max_signal;
-  float dt_force = max_accel > 1.0e-12f ? 0.25f * sqrtf(h / max_accel) : 0.01f;
-  float dt = fminf(dt_cfl, dt_force);
-  *dt_out = fminf(fmaxf(dt, 1.0e-8f), 0.01f);
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < ninst; q += gridDim.x * blockDim.x) {
+    float4 p = hcc[q];
+    float h = p.x, c = p.y, cfl = p.z;
+    float max_signal = fmaxf(c, red[2 * q]);
+    float max_accel = red[2 * q + 1];
+    float dt_cfl = cfl * h / max_signal;
+    float dt_force = max_accel > 1.0e-12f ? 0.25f * sqrtf(h / max_accel) : 0.01f;
+    float dt = fminf(dt_cfl, dt_force);
+    dt_out[q] = fminf(fmaxf(dt, 1.0e-8f), 0.01f);
+  }
 }
 
 // ---- readback / metrics / checkpoint -------------------------------------

@@ -388,3 +388,48 @@ def water_box_2mm() -> Scenario:
                                       np.ones(nb), np.zeros(nb))
     return Scenario("water_box_2mm", p, b, float(h), (0.0, -9.81, 0.0), 10.0, 0.4, 0.001,
                     (0.0, 0.0, 0.0), (0.01, 0.01, 0.01))
+
+
+def batch_boxes(n_instances: int = 256, seed: int = 7, dx: float = 0.002, lo: int = 2000,
+                hi: int = 400_000, alpha: float = 0.02, dims_range=(0.05, 0.3),
+                fill_range=(0.3, 0.8)) -> list:
+    """Independent hydrostatic / dam-break boxes for a batch.
+
+    Per instance, drawn from ``seed``: box dims uniform in ``dims_range`` per
+    axis and a fill fraction uniform in ``fill_range``; even instances are
+    hydrostatic tanks (water fills the bottom ``fill`` of the height), odd
+    ones dam breaks (a full-height column over the first ``fill`` of the
+    length). Draws whose particle count falls outside [lo, hi] are redrawn
+    (the stated ranges alone give about 368k particles per instance at 2 mm,
+    far above the 2k-400k the workload names). Walls on all six faces,
+    h = 1.3 dx, c0 = 10 sqrt(2 g H) with H the water height."""
+    rng = np.random.default_rng(seed)
+    out = []
+    dx32 = f32(dx)
+    q = 0
+    while len(out) < n_instances:
+        L = rng.uniform(*dims_range, size=3)
+        fill = rng.uniform(*fill_range)
+        dam = (len(out) % 2) == 1
+        block = (L[0] * fill, L[1], L[2]) if dam else (L[0], L[1], L[2] * fill)
+        counts = tuple(_axis_count(0.0, block[k], dx32) for k in range(3))
+        npart = counts[0] * counts[1] * counts[2]
+        q += 1
+        if not (lo <= npart <= hi):
+            continue
+        dmax = tuple(float(f32(v)) for v in L)
+        parts = block_particles((0.0, 0.0, 0.0), counts, dx32, seed=int(rng.integers(1 << 31)))
+        walls = wall_boundary_particles((0.0, 0.0, 0.0), dmax, dx32, particle_mass(dx32))
+        height = float(block[2])
+        out.append(Scenario(f"box{len(out)}", parts, walls, float(smoothing_length(dx32)),
+                            (0.0, 0.0, -9.81), dam_break_c0(height), 0.25, 0.0, (0.0, 0.0, 0.0), dmax,
+                            alpha=alpha, extras=dict(kind="dam_break" if dam else "hydrostatic",
+                                                     fill=float(fill), dims=tuple(L), draws=q)))
+    return out
+
+
+def size_histogram(scenarios) -> dict:
+    """Instance particle counts in log2 bins (the autotuner's cache key)."""
+    counts = np.array([len(s.particles) for s in scenarios])
+    bins = np.floor(np.log2(np.maximum(counts, 1))).astype(int)
+    return {int(b): int(np.sum(bins == b)) for b in np.unique(bins)}

@@ -40,7 +40,8 @@ EXPORTS = (
     "sph_save_checkpoint", "sph_restore_checkpoint", "sph_synchronize", "sph_health",
     "sph_last_error", "sph_stream", "sph_launch_count", "sph_grid_info", "sph_read_grid",
     "sph_neighbors", "sph_grid_sort_noalloc", "sph_set_geometry_sdf", "sph_surface_forces",
-    "sph_body_force",
+    "sph_body_force", "sph_batch_create", "sph_batch_info", "sph_batch_timesteps", "sph_set_launch",
+    "sph_get_launch", "sph_autotune",
 )
 
 
@@ -104,6 +105,13 @@ class SphBodyForce(C.Structure):
                                               "repulsion_moment", "viscous_force", "viscous_moment")]
 
 
+class SphLaunch(C.Structure):
+    _fields_ = [("xsph_threads", C.c_int32), ("density_threads", C.c_int32), ("forces_threads", C.c_int32)]
+
+    def as_dict(self) -> dict:
+        return {k: int(getattr(self, k)) for k, _ in self._fields_}
+
+
 class SphGridInfo(C.Structure):
     _fields_ = [("dims", C.c_uint32 * 3), ("total_cells", C.c_uint32), ("cell_size", C.c_float),
                 ("grid_min", C.c_float * 3), ("boundary_candidates", C.c_uint64)]
@@ -150,6 +158,13 @@ def load_library(path: str | None = None):
     L.sph_grid_info.argtypes = [H, C.POINTER(SphGridInfo)]
     L.sph_read_grid.argtypes = [H, _U32P, _U32P, _U32P, _U32P, _U32P]
     L.sph_neighbors.argtypes = [H, C.c_uint32, _U32P, C.c_size_t, C.POINTER(C.c_size_t)]
+    L.sph_batch_create.argtypes = [C.c_int, C.POINTER(SphParams), C.POINTER(SphParticlesView),
+                                   C.POINTER(SphBoundaryView), C.POINTER(vp)]
+    L.sph_batch_info.argtypes = [H, C.POINTER(C.c_int), C.POINTER(C.c_size_t), C.POINTER(C.c_size_t)]
+    L.sph_batch_timesteps.argtypes = [H, _FP]
+    L.sph_set_launch.argtypes = [H, C.POINTER(SphLaunch)]
+    L.sph_get_launch.argtypes = [H, C.POINTER(SphLaunch)]
+    L.sph_autotune.argtypes = [H, C.c_int, C.POINTER(SphLaunch)]
     L.sph_set_geometry_sdf.argtypes = [H, C.POINTER(SphSdfView)]
     L.sph_surface_forces.argtypes = [H, C.POINTER(SphSurfaceForce)]
     L.sph_body_force.argtypes = [H, C.c_uint32, C.c_uint32, C.POINTER(SphBodyForce)]
@@ -160,7 +175,8 @@ def load_library(path: str | None = None):
                 "sph_read_particles", "sph_read_boundary_pressure", "sph_error_metrics",
                 "sph_save_checkpoint", "sph_restore_checkpoint", "sph_synchronize", "sph_health",
                 "sph_grid_info", "sph_read_grid", "sph_neighbors", "sph_set_geometry_sdf",
-                "sph_surface_forces", "sph_body_force"):
+                "sph_surface_forces", "sph_body_force", "sph_batch_create", "sph_batch_info",
+                "sph_batch_timesteps", "sph_set_launch", "sph_get_launch", "sph_autotune"):
             fn.restype = C.c_int
     _lib = L
     return L
@@ -200,6 +216,38 @@ class SimulationKernel(ABC):
 
     def restore_checkpoint(self) -> bool:
         return False
+
+
+def make_params(h, gravity, speed_of_sound, cfl_number, viscosity, domain_min, domain_max, *,
+                alpha=1.0, beta=2.0, boundary_mode=BOUNDARY_PARTICLES, cell_order=CELL_ORDER_MORTON,
+                flags=FLAGS_REFERENCE, device=0, sdf_wall_coef=0.981) -> SphParams:
+    prm = default_params()
+    prm.h = h
+    prm.gravity = (C.c_float * 3)(*map(float, gravity))
+    prm.speed_of_sound = speed_of_sound
+    prm.cfl_number = cfl_number
+    prm.viscosity = viscosity
+    prm.domain_min = (C.c_float * 3)(*map(float, domain_min))
+    prm.domain_max = (C.c_float * 3)(*map(float, domain_max))
+    prm.alpha, prm.beta = alpha, beta
+    prm.boundary_mode, prm.cell_order, prm.flags, prm.device = boundary_mode, cell_order, flags, device
+    prm.sdf_wall_coef = sdf_wall_coef
+    return prm
+
+
+def _particles_view(particles: ParticleArrays, keep: list):
+    arrs = [np.ascontiguousarray(getattr(particles, f), np.float32) for f in PARTICLE_FIELDS]
+    ft = np.ascontiguousarray(particles.fluid_type, np.uint8)
+    keep.extend(arrs + [ft])
+    return SphParticlesView(len(particles), *[_fp(a) for a in arrs], ft.ctypes.data_as(_U8P))
+
+
+def _boundary_view(boundary: BoundaryParticles | None, keep: list):
+    if boundary is None or len(boundary) == 0:
+        return SphBoundaryView(0, *([None] * 7))
+    arrs = [np.ascontiguousarray(getattr(boundary, f), np.float32) for f in BOUNDARY_FIELDS]
+    keep.extend(arrs)
+    return SphBoundaryView(len(boundary), *[_fp(a) for a in arrs])
 
 
 class CudaKernel(SimulationKernel):
@@ -390,3 +438,70 @@ class CudaKernel(SimulationKernel):
         self._check(self._lib.sph_neighbors(self._h, int(pid), _u32p(out), cap, C.byref(cnt)),
                     "sph_neighbors")
         return out[:min(cap, cnt.value)].copy()
+
+    # -- launch shapes ---------------------------------------------------------
+    def launch(self) -> dict:
+        l = SphLaunch()
+        self._check(self._lib.sph_get_launch(self._h, C.byref(l)), "sph_get_launch")
+        return l.as_dict()
+
+    def set_launch(self, xsph_threads: int, density_threads: int, forces_threads: int) -> None:
+        l = SphLaunch(xsph_threads, density_threads, forces_threads)
+        self._check(self._lib.sph_set_launch(self._h, C.byref(l)), "sph_set_launch")
+
+    def autotune(self, trial_steps: int = 3) -> dict:
+        """Native autotuner; advances this simulation by its trial steps."""
+        l = SphLaunch()
+        self._check(self._lib.sph_autotune(self._h, int(trial_steps), C.byref(l)), "sph_autotune")
+        return l.as_dict()
+
+
+class CudaBatch(CudaKernel):
+    """Many independent simulations stepped by the same kernel launches
+    (``sph_batch_create``). ``scenarios`` hold what ``CpuKernel::new`` takes
+    per instance (``domain.Scenario``); ``particles()`` returns the instances
+    one after another, ``instance(q)`` slices one out."""
+
+    def __init__(self, scenarios, device: int = 0, cell_order: int = CELL_ORDER_MORTON):
+        L = load_library()
+        self._lib = L
+        self._keep = []
+        nq = len(scenarios)
+        prms = (SphParams * nq)()
+        views = (SphParticlesView * nq)()
+        bviews = (SphBoundaryView * nq)()
+        for q, sc in enumerate(scenarios):
+            sc.particles.validate()
+            prms[q] = make_params(sc.h, sc.gravity, sc.speed_of_sound, sc.cfl_number, sc.viscosity,
+                                  sc.domain_min, sc.domain_max, alpha=sc.alpha, beta=sc.beta,
+                                  cell_order=cell_order, device=device)
+            views[q] = _particles_view(sc.particles, self._keep)
+            bviews[q] = _boundary_view(sc.boundary, self._keep)
+        handle = C.c_void_p()
+        st = L.sph_batch_create(nq, prms, views, bviews, C.byref(handle))
+        self._keep = []
+        if st != SPH_OK:
+            raise SphError(st, "sph_batch_create failed")
+        self._h = handle
+        self._cache = None
+        self._n = sum(len(sc.particles) for sc in scenarios)
+        self._nb = sum(len(sc.boundary) if sc.boundary is not None else 0 for sc in scenarios)
+        self.ninst = nq
+        first = (C.c_size_t * nq)()
+        count = (C.c_size_t * nq)()
+        ni = C.c_int()
+        self._check(L.sph_batch_info(self._h, C.byref(ni), first, count), "sph_batch_info")
+        self.first = np.array(first[:], np.int64)
+        self.count = np.array(count[:], np.int64)
+
+    def timesteps(self) -> np.ndarray:
+        out = np.zeros(self.ninst, np.float32)
+        self._check(self._lib.sph_batch_timesteps(self._h, _fp(out)), "sph_batch_timesteps")
+        return out
+
+    def instance(self, q: int) -> ParticleArrays:
+        p = self.particles()
+        a, b = int(self.first[q]), int(self.first[q] + self.count[q])
+        out = ParticleArrays(**{f: getattr(p, f)[a:b].copy() for f in PARTICLE_FIELDS})
+        out.fluid_type = p.fluid_type[a:b].copy()
+        return out
