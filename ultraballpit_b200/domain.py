@@ -392,7 +392,7 @@ def water_box_2mm() -> Scenario:
 
 def batch_boxes(n_instances: int = 256, seed: int = 7, dx: float = 0.002, lo: int = 2000,
                 hi: int = 400_000, alpha: float = 0.02, dims_range=(0.05, 0.3),
-                fill_range=(0.3, 0.8)) -> list:
+                fill_range=(0.3, 0.8), draw: str = "stated") -> list:
     """Independent hydrostatic / dam-break boxes for a batch.
 
     Per instance, drawn from ``seed``: box dims uniform in ``dims_range`` per
@@ -401,8 +401,12 @@ def batch_boxes(n_instances: int = 256, seed: int = 7, dx: float = 0.002, lo: in
     ones dam breaks (a full-height column over the first ``fill`` of the
     length). Draws whose particle count falls outside [lo, hi] are redrawn
     (the stated ranges alone give about 368k particles per instance at 2 mm,
-    far above the 2k-400k the workload names). Walls on all six faces,
-    h = 1.3 dx, c0 = 10 sqrt(2 g H) with H the water height."""
+    far above the 2k-400k the workload names). With ``draw="loguniform"`` a
+    target count is drawn log-uniformly in [lo, hi] instead and the drawn box
+    is scaled to hold it (box edges may then leave ``dims_range``); that
+    matches the workload's stated total of about 20M for 256 instances.
+    Walls on all six faces, h = 1.3 dx, c0 = 10 sqrt(2 g H) with H the water
+    height."""
     rng = np.random.default_rng(seed)
     out = []
     dx32 = f32(dx)
@@ -410,6 +414,9 @@ def batch_boxes(n_instances: int = 256, seed: int = 7, dx: float = 0.002, lo: in
     while len(out) < n_instances:
         L = rng.uniform(*dims_range, size=3)
         fill = rng.uniform(*fill_range)
+        if draw == "loguniform":
+            target = math.exp(rng.uniform(math.log(lo), math.log(hi)))
+            L = L * (target * dx ** 3 / (fill * L[0] * L[1] * L[2])) ** (1.0 / 3.0)
         dam = (len(out) % 2) == 1
         block = (L[0] * fill, L[1], L[2]) if dam else (L[0], L[1], L[2] * fill)
         counts = tuple(_axis_count(0.0, block[k], dx32) for k in range(3))
