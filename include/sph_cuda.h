@@ -212,6 +212,10 @@ size_t sph_particle_count(const SphHandle *h);
 int sph_save_checkpoint(SphHandle *h);
 int sph_restore_checkpoint(SphHandle *h);
 
+/* Multiply every particle's velocity by `factor` (no reference
+ * counterpart). 0 between steps is kinetic damping: relaxing an initial
+ * lattice into its equilibrium before a run. */
+int sph_scale_velocities(SphHandle *h, float factor);
 /* Wait for queued work; reports a deferred device-side error, if any. */
 int sph_synchronize(SphHandle *h);
 /* Count of particles with a non-finite position, velocity or density. */
@@ -233,6 +237,10 @@ uint64_t sph_launch_count(const SphHandle *h);
  * sums over all instances. */
 int sph_batch_create(int ninst, const SphParams *params, const SphParticlesView *particles,
                      const SphBoundaryView *boundaries, SphHandle **out);
+/* A batch in SDF wall mode: one SDF per instance (all instances with the
+ * same h, which fixes the shared wall table). */
+int sph_batch_create_sdf(int ninst, const SphParams *params, const SphParticlesView *particles,
+                         const SphSdfView *sdfs, SphHandle **out);
 /* Instance count, and per instance the first particle and particle count in
  * the concatenated order (first/count may be NULL, else ninst entries). */
 int sph_batch_info(const SphHandle *h, int *ninst, size_t *first, size_t *count);
@@ -247,6 +255,54 @@ int sph_get_launch(const SphHandle *h, SphLaunch *launch);
  * and instance-size histogram; a cache hit runs no step. The trial steps
  * advance the simulation: tune a scratch handle of the same workload. */
 int sph_autotune(SphHandle *h, int trial_steps, SphLaunch *best);
+
+/* ---- learned near-wall closure network (no reference counterpart) -----
+ * MLP 16 -> 64 -> 64 -> 4 with SiLU; BF16 operands on the tensor cores with
+ * FP32 accumulation, FP32 master weights and Adam state on the device.
+ * Parameters (5,508 floats): W1[64][16], b1[64], W2[64][64], b2[64],
+ * W3[4][64], b3[4]. Inputs x[n][16], targets t[n][4] (host, row-major). */
+#define SPH_MLP_PARAMS 5508
+typedef struct SphMlp SphMlp;
+/* Weights and biases uniform in +-1/sqrt(fan_in) from `seed`. */
+int sph_mlp_create(int device, uint64_t seed, SphMlp **out);
+void sph_mlp_destroy(SphMlp *m);
+int sph_mlp_set_params(SphMlp *m, const float *params); /* also resets Adam */
+int sph_mlp_get_params(SphMlp *m, float *params);
+int sph_mlp_forward(SphMlp *m, const float *x, size_t n, float *y);
+/* Mean squared error over n x 4 outputs and its gradient (no update). */
+int sph_mlp_loss_grad(SphMlp *m, const float *x, const float *t, size_t n, float *loss, float *grad);
+/* Adam (beta 0.9 / 0.999, eps 1e-8) on shuffled mini-batches of `batch`;
+ * epoch_loss (may be NULL) gets the mean training loss of each epoch. */
+int sph_mlp_train(SphMlp *m, const float *x, const float *t, size_t n, int batch, int epochs, float lr,
+                  uint64_t shuffle_seed, float *epoch_loss);
+
+/* ---- closure in the WCSPH step ------------------------------------------
+ * The closure acts on fluid particles within 2h of the geometry SDF (the
+ * merged walls and obstacles; SDF wall mode uses its own SDF). */
+/* Geometry SDF of the closure features: one simulation, or one per instance. */
+int sph_set_feature_sdf(SphHandle *h, const SphSdfView *sdf);
+int sph_batch_set_feature_sdfs(SphHandle *h, const SphSdfView *sdfs);
+/* mode 0: off (the plain step). 1: the density pass records the features of
+ * near-geometry particles (sph_closure_samples) without changing the step.
+ * 2: also evaluates the network (`params`, SPH_MLP_PARAMS floats) on the
+ * tensor cores after the density pass: density += y0 rho0 / 100 with the
+ * EOS re-evaluated, acceleration += (y1, y2, y3) |g| in the force kernel,
+ * y0 clamped to +-SPH_CLOSURE_MAX_DRHO_PCT and y1..3 to +-SPH_CLOSURE_MAX_ACC_G.
+ * Features (d = SDF distance, n = SDF gradient):
+ *   0 d/h, 1-3 n, 4 1 - Shepard kernel sum, 5 listed neighbours / 73,
+ *   6 |v|/c, 7 dt c/h, 8 h * Laplacian of the SDF (clamped to +-4),
+ *   9 wall-table kernel mass at d (SDF mode; else boundary density / rho0),
+ *   10 n.g/|g|, 11 (d/h)^2, 12 f8 f0, 13 f10 f0,
+ *   14 boundary particles in support / 30, 15 1. */
+#define SPH_CLOSURE_MAX_DRHO_PCT 3.0f
+#define SPH_CLOSURE_MAX_ACC_G 25.0f
+int sph_set_closure(SphHandle *h, int mode, const float *params);
+/* Samples of the last density pass: original particle ids, 16 features each
+ * (row-major), density before correction; *count gets the total. */
+int sph_closure_samples(SphHandle *h, size_t cap, uint32_t *ids, float *features, float *rho, size_t *count);
+/* Shepard interpolation of the current state at points pts[n][3]:
+ * out[n][7] = (rho, p, ax, ay, az, weight sum, neighbour count). */
+int sph_interpolate(SphHandle *h, const float *pts, size_t n, float *out);
 
 /* ---- force extraction ------------------------------------------------- */
 /* Register the geometry SDF whose surface force sph_surface_forces returns

@@ -396,11 +396,23 @@ class Kernel {
       sdf.assign(prm.sdf, prm.sdf + (size_t)prm.sdf_dims[0] * prm.sdf_dims[1] * prm.sdf_dims[2]);
       prm.sdf = sdf.data();
       wall = make_wall_table(prm.h);
+      wall_scale = wall_mass_scale();
     }
     if (prm.tier == 1 && prm.boundary_mode == 0) build_boundary_lists();
   }
 
   bool sdf_mode() const { return prm.boundary_mode == 1; }
+  // Wall layers carry the first water particle's mass (domain.rs:57-62),
+  // relative to rho0 (h / 1.3)^3; exactly 1 within 1e-5 of 1.
+  float wall_scale = 1.0f;
+  float wall_mass_scale() const {
+    size_t i = 0;
+    while (i < p.len() && p.fluid_type[i] != 0) ++i;
+    if (i == p.len()) return 1.0f;
+    double dx = (double)prm.h / 1.3;
+    double s = (double)p.mass[i] / (1000.0 * dx * dx * dx);
+    return std::fabs(s - 1.0) < 1e-5 ? 1.0f : (float)s;
+  }
   float wall_distance(size_t i) const {
     return sdf_sample_clamped(prm.sdf, prm.sdf_dims, prm.sdf_origin, prm.sdf_cell, p.x[i], p.y[i], p.z[i]);
   }
@@ -527,7 +539,7 @@ class Kernel {
         float d = wall_distance(i);
         if (d < support) {
           float rest = p.fluid_type[i] == 0 ? kWaterRho0 : kAirRho0;
-          rho += rest * wall_lookup(wall.phi, wall.inv_step, d);
+          rho += rest * wall_scale * wall_lookup(wall.phi, wall.inv_step, d);
         }
       }
       out[i] = rho;
@@ -732,7 +744,7 @@ class Kernel {
       float depth = -(d + mid);
       float g_dot_dr = g[0] * (depth * n[0]) + g[1] * (depth * n[1]) + g[2] * (depth * n[2]);
       float pw = fmaxf(pic + p.density[i] * g_dot_dr, 0.0f);
-      float coef = (pic / (p.density[i] * p.density[i]) + pw / (rest * rest)) * rest *
+      float coef = (pic / (p.density[i] * p.density[i]) + pw / (rest * rest)) * (rest * wall_scale) *
                    wall_lookup(wall.grad, wall.inv_step, d);
       p.ax[i] += coef * n[0];
       p.ay[i] += coef * n[1];

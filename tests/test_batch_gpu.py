@@ -56,3 +56,17 @@ def test_autotune_returns_valid_shapes_and_caches():
     assert k.launch() == best
     k2 = CudaBatch(scs)
     assert k2.autotune(2) == best  # cache hit: same histogram, same device
+
+
+def test_batch_sdf_mode_matches_single_runs():
+    from ultraballpit_b200 import closure
+    from ultraballpit_b200.kernel import BOUNDARY_SDF
+    scs = [closure.tank_pair(s, dx_coarse=0.008)[0] for s in (21, 22, 23)]
+    batch = CudaBatch(scs, boundary_mode=BOUNDARY_SDF)
+    singles = [CudaKernel(*sc.kernel_args(), alpha=sc.alpha, boundary_mode=BOUNDARY_SDF, sdf=sc.sdf)
+               for sc in scs]
+    batch.step_auto(10, want_dt=False)
+    for k in singles:
+        k.step_auto(10, want_dt=False)
+    for q, k in enumerate(singles):
+        _same(batch.instance(q), k.particles())

@@ -1,0 +1,161 @@
+"""The closure network's tensor-core kernels against the float64 oracle."""
+import numpy as np
+import pytest
+
+from oracle import mlp_oracle as ref
+from ultraballpit_b200.closure import ClosureNet
+
+pytestmark = pytest.mark.gpu
+
+
+def _data(n, seed):
+    rng = np.random.default_rng(seed)
+    x = rng.normal(size=(n, 16)).astype(np.float32)
+    t = np.stack([np.sin(x[:, 0]) + 0.5 * x[:, 1] * x[:, 2], np.tanh(x[:, 3] - x[:, 4]),
+                  0.3 * x[:, 5] ** 2 - 0.2, x[:, 6] * 0.1 + np.cos(x[:, 7])], axis=1).astype(np.float32)
+    return x, t
+
+
+def test_forward_matches_oracle():
+    net = ClosureNet(seed=3)
+    x, _ = _data(1000, 1)
+    y = net.forward(x)
+    yr, _ = ref.forward(net.params(), x)
+    assert np.max(np.abs(y - yr)) <= 2e-2 * max(1.0, np.max(np.abs(yr)))
+
+
+def test_gradients_match_oracle():
+    net = ClosureNet(seed=4)
+    x, t = _data(777, 2)  # not a multiple of the 16-sample tile
+    loss, g = net.loss_grad(x, t)
+    lr_, gr = ref.loss_grad(net.params(), x, t)
+    assert abs(loss - lr_) <= 1e-2 * lr_
+    o = 0
+    for name, shp in ref.SHAPES:
+        k = int(np.prod(shp))
+        a, b = g[o:o + k], gr[o:o + k]
+        rel = np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-12)
+        assert rel < 3e-2, (name, rel)
+        o += k
+
+
+def test_training_reduces_loss():
+    net = ClosureNet(seed=5)
+    x, t = _data(20000, 3)
+    l0, _ = net.loss_grad(x, t)
+    losses = net.train(x, t, batch=512, epochs=8, lr=3e-3, seed=1)
+    l1, _ = net.loss_grad(x, t)
+    assert losses[-1] < losses[0] and l1 < 0.25 * l0
+
+
+# ---- the closure inside the WCSPH step -------------------------------------------
+
+from ultraballpit_b200 import closure, domain  # noqa: E402
+from ultraballpit_b200.kernel import BOUNDARY_SDF, CudaKernel  # noqa: E402
+
+DT = 5e-5
+FIELDS = ("x", "y", "z", "vx", "vy", "vz", "ax", "ay", "az", "density", "pressure")
+
+
+def _tank(dx=0.004, seed=11):
+    return closure.tank_pair(seed, dx_coarse=dx)[0]
+
+
+def _sdf_kernel(sc):
+    return CudaKernel(*sc.kernel_args(), alpha=sc.alpha, boundary_mode=BOUNDARY_SDF, sdf=sc.sdf)
+
+
+def _same(a, b):
+    for f in FIELDS:
+        np.testing.assert_array_equal(getattr(a, f), getattr(b, f), err_msg=f)
+
+
+def test_capture_mode_and_zero_network_leave_the_step_unchanged():
+    sc = _tank()
+    plain = _sdf_kernel(sc)
+    cap = _sdf_kernel(sc)
+    cap.set_closure(1)
+    zero = _sdf_kernel(sc)
+    zero.set_closure(2, np.zeros(closure.N_PARAMS, np.float32))
+    for _ in range(10):
+        for k in (plain, cap, zero):
+            k.step(DT)
+    assert plain.health() == 0
+    _same(plain.particles(), cap.particles())
+    _same(plain.particles(), zero.particles())
+    ids, feat, rho = cap.closure_samples()
+    assert 0 < len(ids) < len(sc.particles)
+    assert np.all(np.isfinite(feat)) and np.all(feat[:, 15] == 1.0)
+    assert np.all(feat[:, 0] < 2.0)  # d < 2h
+    np.testing.assert_allclose(np.linalg.norm(feat[:, 1:4], axis=1), 1.0, atol=1e-4)
+
+
+def test_applied_density_correction_is_the_network_output():
+    sc = _tank(seed=12)
+    net = closure.ClosureNet(seed=7)
+    k = _sdf_kernel(sc)
+    k.set_closure(2, net.params())
+    k.step(DT)
+    k.step(DT)
+    ids, feat, rho_pre = k.closure_samples()
+    y = net.forward(feat)
+    rho = k.particles().density[ids]
+    y0 = np.clip(y[:, 0], -closure.CLAMP_DRHO_PCT, closure.CLAMP_DRHO_PCT).astype(np.float32)
+    np.testing.assert_array_equal(rho, (rho_pre + y0 * np.float32(1000.0) / np.float32(100.0)).astype(np.float32))
+
+
+def test_features_see_the_sphere_curvature():
+    coarse, _, geo = closure.tank_pair(14)
+    k = _sdf_kernel(coarse)
+    k.set_closure(1)
+    k.step(DT)
+    ids, feat, _ = k.closure_samples()
+    p = k.particles()
+    pos = np.stack([p.x[ids], p.y[ids], p.z[ids]], axis=1).astype(np.float64)
+    c, r, h = np.asarray(geo["center"]), geo["radius"], coarse.h
+    ds = np.linalg.norm(pos - c, axis=1) - r
+    # samples whose nearest surface is the sphere, far from the tank walls
+    wall = np.minimum.reduce([pos[:, 0], 0.1 - pos[:, 0], pos[:, 1], 0.1 - pos[:, 1], pos[:, 2]])
+    near = (ds > 0.2 * h) & (ds < 1.5 * h) & (wall > ds + 3 * h)
+    assert near.sum() > 20
+    expect = 2.0 * h / (r + ds[near])  # Laplacian of |x - c| - r is 2 / |x - c|
+    np.testing.assert_allclose(feat[near, 8], expect, rtol=0.25, atol=0.05)
+    np.testing.assert_allclose(feat[near, 0], ds[near] / h, atol=0.15)
+    # beside one flat wall the SDF is linear: zero curvature wherever the
+    # +-h stencil stays inside the SDF grid (the sampler clamps outside it)
+    # and away from the kinks where another wall becomes the nearest
+    dw = np.sort(np.stack([pos[:, 0], 0.1 - pos[:, 0], pos[:, 1], 0.1 - pos[:, 1], pos[:, 2]], axis=1), axis=1)
+    flat = (dw[:, 0] > 1.1 * h) & (dw[:, 0] < 1.6 * h) & (dw[:, 1] > dw[:, 0] + 2 * h) & (ds > 4 * h)
+    assert flat.sum() > 20 and np.all(np.abs(feat[flat, 8]) < 0.05), np.abs(feat[flat, 8]).max()
+
+
+def test_interpolation_matches_brute_force():
+    from oracle import oracle as orc
+    sc = _tank(seed=13)
+    k = _sdf_kernel(sc)
+    k.step(DT)
+    p = k.particles()
+    rng = np.random.default_rng(0)
+    pts = np.stack([rng.uniform(0.0, 0.1, 50), rng.uniform(0.0, 0.1, 50), rng.uniform(0.0, 0.15, 50)], 1)
+    out = k.interpolate(pts)
+    for q in range(len(pts)):
+        r = np.sqrt((p.x - pts[q, 0]) ** 2 + (p.y - pts[q, 1]) ** 2 + (p.z - pts[q, 2]) ** 2).astype(np.float32)
+        w = np.array([orc.wendland(float(v), sc.h) if v < 2 * sc.h else 0.0 for v in r])
+        if w.sum() == 0:
+            assert out[q, 6] == 0
+            continue
+        assert abs(out[q, 0] - (w * p.density).sum() / w.sum()) < 1e-3
+        assert abs(out[q, 1] - (w * p.pressure).sum() / w.sum()) < 1e-2 * max(1.0, abs(out[q, 1]))
+
+
+def test_trained_closure_reduces_near_wall_pressure_error():
+    """Small version of the training workload: five 4 mm / 2 mm tank pairs
+    for training, an unseen sixth tank for the evaluation against its 2 mm
+    run (time-averaged probe pressures near the sphere and the walls)."""
+    kw = dict(dx_coarse=0.004, dt_coarse=DT, t_snap=(0.02, 0.03, 0.04))
+    x, t, _ = closure.generate(range(100, 105), **kw)
+    net = closure.ClosureNet(seed=1)
+    losses = net.train(x, closure.prepare_targets(t), batch=256, epochs=20, lr=1e-3, seed=2)
+    assert losses[-1] < losses[0]
+    r = closure.compare(200, net.params(), steps=800, dt=DT)
+    assert r["closure"]["all"] < r["plain"]["all"], r

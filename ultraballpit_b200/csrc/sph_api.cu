@@ -13,6 +13,8 @@
 #include <string>
 #include <vector>
 
+#include <cuda_bf16.h>
+
 #include "sph_cuda.h"
 #include "sph_kernels.cuh"
 
@@ -78,9 +80,16 @@ struct SphHandle {
   float4* bpos = nullptr;
   float* bpress = nullptr;
   uint32_t *bc_start = nullptr, *bc_list = nullptr;
-  // SDF node grid and wall table (boundary_mode SPH_BOUNDARY_SDF)
+  // SDF node grid and wall table (boundary_mode SPH_BOUNDARY_SDF), or the
+  // geometry SDF(s) of the closure features
   float* sdf = nullptr;
   float2* wall_tab = nullptr;
+  // learned closure: 0 off, 1 capture features, 2 capture and apply
+  int cl_mode = 0;
+  uint32_t *cl_count = nullptr, *cl_slot = nullptr;
+  float *cl_feat = nullptr, *cl_rho = nullptr, *cl_wf = nullptr;
+  float4* corr = nullptr;
+  __nv_bfloat16* cl_wb = nullptr;
   // scalars
   float *dt = nullptr, *dt_query = nullptr, *red = nullptr;
   uint32_t* err = nullptr;
@@ -240,6 +249,20 @@ std::vector<float2> make_wall_table(float hf, float* inv_step) {
   return t;
 }
 
+// Mass of the homogenised wall layers relative to rho0 (h / 1.3)^3: the
+// walls carry the mass of the first water particle (the reference gives wall
+// particles the water particle mass, orchestrator/src/domain.rs:57-62).
+// Within 1e-5 of 1 (mass rho0 dx^3 with h = 1.3 dx, up to f32 rounding) it
+// is exactly 1.
+float wall_mass_scale(float hf, const SphParticlesView* pv) {
+  size_t i = 0;
+  while (i < pv->n && pv->fluid_type && pv->fluid_type[i] != 0) ++i;
+  if (i == pv->n || !pv->mass) return 1.0f;
+  double dx = (double)hf / 1.3;
+  double s = (double)pv->mass[i] / (1000.0 * dx * dx * dx);
+  return std::fabs(s - 1.0) < 1e-5 ? 1.0f : (float)s;
+}
+
 // GridSDF::sample and ::gradient (orchestrator geometry.rs:99-181), f32.
 float host_sdf_get(const SphSdfView& g, int i, int j, int k) {
   uint64_t idx = (uint64_t)((uint32_t)i * g.dims[1] * g.dims[2] + (uint32_t)j * g.dims[2] + (uint32_t)k);
@@ -343,15 +366,35 @@ void enqueue_scan_fill(SphHandle* h) {
   h->launches += 4;
 }
 
-void enqueue_density_adami(SphHandle* h) {
+void enqueue_density_only(SphHandle* h) {
   using namespace sph;
   int bs = h->bs_density;
+  sph::ClosureBufs cb{h->cl_count, h->cl_slot, h->cl_feat, h->cl_rho, h->corr, h->vel};
+  if (h->cl_mode) cudaMemsetAsync(h->cl_count, 0, sizeof(uint32_t), h->st);
   dispatch(h, false, [&](auto kp) {
-    k_density<<<grid_for(h->n, bs), bs, 0, h->st>>>(kp, h->n, h->dt, h->pos, h->rv, h->id, h->ctab,
-                                                    h->bc_start, h->bc_list, h->bpos, h->rf, h->pr, h->err,
-                                                    h->nbr, h->ncount, h->sdf, h->wall_tab);
+    using KPT = decltype(kp);
+    if (h->cl_mode)
+      k_density<KPT, 1><<<grid_for(h->n, bs), bs, 0, h->st>>>(kp, h->n, h->dt, h->pos, h->rv, h->id, h->ctab,
+                                                            h->bc_start, h->bc_list, h->bpos, h->rf, h->pr,
+                                                            h->err, h->nbr, h->ncount, h->sdf, h->wall_tab, cb);
+    else
+      k_density<KPT, 0><<<grid_for(h->n, bs), bs, 0, h->st>>>(kp, h->n, h->dt, h->pos, h->rv, h->id, h->ctab,
+                                                            h->bc_start, h->bc_list, h->bpos, h->rf, h->pr,
+                                                            h->err, h->nbr, h->ncount, h->sdf, h->wall_tab, cb);
   });
   h->launches += 1;
+  if (h->cl_mode == 2) {
+    dispatch(h, false, [&](auto kp) {
+      k_closure_apply<<<std::max(1, std::min(grid_for(h->n, 16 * kClWarps), 148 * 8)), kClWarps * 32, 0, h->st>>>(
+          kp, h->cl_wb, h->cl_wf, h->cl_count, h->cl_slot, h->cl_feat, h->cl_rho, h->id, h->rf, h->pr, h->corr);
+    });
+    h->launches += 1;
+  }
+}
+
+void enqueue_density_adami(SphHandle* h) {
+  using namespace sph;
+  enqueue_density_only(h);
   if (h->nb > 0) {
     dispatch(h, true, [&](auto kp) {
       k_adami<<<grid_for(h->nb, kAdamiWarps), kAdamiWarps * 32, 0, h->st>>>(
@@ -366,10 +409,19 @@ void enqueue_forces(SphHandle* h, float hdt_scale) {
   cudaMemsetAsync(h->red, 0, 2 * sizeof(float) * h->ninst, h->st);
   int bs = h->bs_forces;
   dispatch(h, false, [&](auto kp) {
-    k_forces<<<grid_for(h->n, bs), bs, 0, h->st>>>(kp, h->n, h->dt, hdt_scale, h->pos, h->vel, h->rf, h->pr,
-                                                   h->id, h->ctab, h->bc_start, h->bc_list, h->bpos,
-                                                   h->bpress, h->acc, h->velout, h->red, h->err, h->nbr,
-                                                   h->ncount, h->sdf, h->wall_tab);
+    using KPT = decltype(kp);
+    if (h->cl_mode)
+      k_forces<KPT, 1><<<grid_for(h->n, bs), bs, 0, h->st>>>(kp, h->n, h->dt, hdt_scale, h->pos, h->vel, h->rf,
+                                                           h->pr, h->id, h->ctab, h->bc_start, h->bc_list,
+                                                           h->bpos, h->bpress, h->acc, h->velout, h->red,
+                                                           h->err, h->nbr, h->ncount, h->sdf, h->wall_tab,
+                                                           h->corr);
+    else
+      k_forces<KPT, 0><<<grid_for(h->n, bs), bs, 0, h->st>>>(kp, h->n, h->dt, hdt_scale, h->pos, h->vel, h->rf,
+                                                           h->pr, h->id, h->ctab, h->bc_start, h->bc_list,
+                                                           h->bpos, h->bpress, h->acc, h->velout, h->red,
+                                                           h->err, h->nbr, h->ncount, h->sdf, h->wall_tab,
+                                                           h->corr);
   });
   h->launches += 1;
 }
@@ -494,7 +546,7 @@ int check_views(const SphParams& P, const SphParticlesView* pv, const SphBoundar
 // occupy disjoint ranges of the global cell ranks, so the global counting
 // sort keeps every instance in a fixed contiguous slot range.
 int create_impl(int ninst, const SphParams* PP, const SphParticlesView* pvs,
-                const SphBoundaryView* const* bvs, const SphSdfView* sdf, SphHandle** out) {
+                const SphBoundaryView* const* bvs, const SphSdfView* sdfs, SphHandle** out) {
   if (!out) return SPH_ERR_INVALID_ARG;
   *out = nullptr;
   if (ninst < 1 || ninst > 65535 || !PP || !pvs) return SPH_ERR_INVALID_ARG;
@@ -510,12 +562,20 @@ int create_impl(int ninst, const SphParams* PP, const SphParticlesView* pvs,
     if (!sdf_mode && bv) nbtot += bv->n;
   }
   if (ntot > 0x7fffffffull || nbtot > 0x7fffffffull) return SPH_ERR_INVALID_ARG;
+  // SDF wall mode: one SDF per instance (concatenated on the device), one
+  // wall table, so every instance must share the smoothing length.
   uint64_t sdf_nodes = 0;
+  std::vector<uint64_t> sdf_off(ninst + 1, 0);
   if (sdf_mode) {
-    if (ninst != 1) return SPH_ERR_INVALID_ARG;  // the SDF wall mode is single-simulation
-    if (!sdf || !sdf->distances || !(sdf->cell_size > 0.0f)) return SPH_ERR_INVALID_ARG;
-    if (sdf->dims[0] < 2 || sdf->dims[1] < 2 || sdf->dims[2] < 2) return SPH_ERR_INVALID_ARG;
-    sdf_nodes = (uint64_t)sdf->dims[0] * sdf->dims[1] * sdf->dims[2];
+    if (!sdfs) return SPH_ERR_INVALID_ARG;
+    for (int q = 0; q < ninst; ++q) {
+      const SphSdfView* sd = &sdfs[q];
+      if (!sd->distances || !(sd->cell_size > 0.0f)) return SPH_ERR_INVALID_ARG;
+      if (sd->dims[0] < 2 || sd->dims[1] < 2 || sd->dims[2] < 2) return SPH_ERR_INVALID_ARG;
+      if (PP[q].h != PP[0].h) return SPH_ERR_INVALID_ARG;
+      sdf_off[q + 1] = sdf_off[q] + (uint64_t)sd->dims[0] * sd->dims[1] * sd->dims[2];
+    }
+    sdf_nodes = sdf_off[ninst];
   }
   const SphParams& P0 = PP[0];
   int ndev = 0;
@@ -573,13 +633,17 @@ int create_impl(int ninst, const SphParams* PP, const SphParticlesView* pvs,
     k.coff = (int)C;
     k.cfl = P.cfl_number;
     if (sdf_mode) {
+      const SphSdfView* sd = &sdfs[q];
       k.sdf_mode = 1;
       for (int a = 0; a < 3; ++a) {
-        k.sdf_origin[a] = sdf->origin[a];
-        k.sdf_dims[a] = (int)sdf->dims[a];
+        k.sdf_origin[a] = sd->origin[a];
+        k.sdf_dims[a] = (int)sd->dims[a];
       }
-      k.sdf_cell = sdf->cell_size;
+      k.sdf_cell = sd->cell_size;
+      k.sdf_off = (long long)sdf_off[q];
       k.wall_mid = 1.5f * (P.h / 1.3f);
+      k.wall_scale = wall_mass_scale(P.h, pv);
+      k.feat_sdf = 1;
     }
     h->ktab_h[q] = k;
     hcc[q] = make_float4(P.h, P.speed_of_sound, P.cfl_number, 0.0f);
@@ -629,7 +693,11 @@ int create_impl(int ninst, const SphParams* PP, const SphParticlesView* pvs,
     h->init_energy += h->init_e[q];
   }
   std::vector<float2> wall_host;
-  if (sdf_mode) wall_host = make_wall_table(P0.h, &h->ktab_h[0].wall_inv_step);
+  if (sdf_mode) {
+    float inv = 0.0f;
+    wall_host = make_wall_table(P0.h, &inv);
+    for (int q = 0; q < ninst; ++q) h->ktab_h[q].wall_inv_step = inv;
+  }
   h->k = h->ktab_h[0];
 
   if (cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking) != cudaSuccess) return fail(SPH_ERR_CUDA);
@@ -706,7 +774,8 @@ int create_impl(int ninst, const SphParams* PP, const SphParticlesView* pvs,
     up(h->inst_p, hip.data(), n * sizeof(uint16_t));
     up(h->inst_b, hib.data(), nb * sizeof(uint16_t));
   }
-  if (sdf_mode) up(h->sdf, sdf->distances, sdf_nodes * sizeof(float));
+  for (int q = 0; sdf_mode && q < ninst; ++q)
+    up(h->sdf + sdf_off[q], sdfs[q].distances, (sdf_off[q + 1] - sdf_off[q]) * sizeof(float));
   if (sdf_mode) up(h->wall_tab, wall_host.data(), wall_host.size() * sizeof(float2));
   if (e == cudaSuccess) e = cudaMemsetAsync(h->hist, 0, C * sizeof(uint32_t), h->st);
   if (e == cudaSuccess) e = cudaMemsetAsync(h->bpress, 0, std::max<size_t>(1, nb) * sizeof(float), h->st);
@@ -775,6 +844,16 @@ int sph_batch_create(int ninst, const SphParams* params, const SphParticlesView*
   for (int q = 0; q < ninst; ++q)
     if (params[q].boundary_mode != SPH_BOUNDARY_PARTICLES) return SPH_ERR_INVALID_ARG;
   return create_impl(ninst, params, particles, bvs.data(), nullptr, out);
+}
+
+int sph_batch_create_sdf(int ninst, const SphParams* params, const SphParticlesView* particles,
+                         const SphSdfView* sdfs, SphHandle** out) {
+  if (!out) return SPH_ERR_INVALID_ARG;
+  *out = nullptr;
+  if (ninst < 1 || !params || !particles || !sdfs) return SPH_ERR_INVALID_ARG;
+  for (int q = 0; q < ninst; ++q)
+    if (params[q].boundary_mode != SPH_BOUNDARY_SDF) return SPH_ERR_INVALID_ARG;
+  return create_impl(ninst, params, particles, nullptr, sdfs, out);
 }
 
 void sph_destroy(SphHandle* h) {
@@ -879,23 +958,15 @@ int sph_step_profiled(SphHandle* h, float dt, SphStepProfile* prof) {
   cudaEventRecord(ev[1], h->st);
   enqueue_sort(h);
   cudaEventRecord(ev[2], h->st);
-  {
+  enqueue_density_only(h);
+  cudaEventRecord(ev[3], h->st);
+  if (h->nb > 0) {
     using namespace sph;
-    int bs = h->bs_density;
-    dispatch(h, false, [&](auto kp) {
-      k_density<<<grid_for(h->n, bs), bs, 0, h->st>>>(kp, h->n, h->dt, h->pos, h->rv, h->id, h->ctab,
-                                                      h->bc_start, h->bc_list, h->bpos, h->rf, h->pr,
-                                                      h->err, h->nbr, h->ncount, h->sdf, h->wall_tab);
+    dispatch(h, true, [&](auto kp) {
+      k_adami<<<grid_for(h->nb, kAdamiWarps), kAdamiWarps * 32, 0, h->st>>>(
+          kp, h->nb, h->bpos, h->bpress, h->pos, h->rf, h->pr, h->id, h->ctab, h->err);
     });
     h->launches += 1;
-    cudaEventRecord(ev[3], h->st);
-    if (h->nb > 0) {
-      dispatch(h, true, [&](auto kp) {
-        k_adami<<<grid_for(h->nb, kAdamiWarps), kAdamiWarps * 32, 0, h->st>>>(
-            kp, h->nb, h->bpos, h->bpress, h->pos, h->rf, h->pr, h->id, h->ctab, h->err);
-      });
-      h->launches += 1;
-    }
   }
   cudaEventRecord(ev[4], h->st);
   enqueue_forces(h, 1.0f);
@@ -1007,6 +1078,17 @@ int sph_restore_checkpoint(SphHandle* h) {
   h->list_valid = false;
   ensure_red(h);
   return cuda_status(h, cudaGetLastError(), "sph_restore_checkpoint");
+}
+
+int sph_scale_velocities(SphHandle* h, float factor) {
+  if (!h || !std::isfinite(factor)) return SPH_ERR_INVALID_ARG;
+  SPH_TRY(h, cudaSetDevice(h->dev));
+  if (h->n > 0) {
+    sph::k_scale_velocities<<<grid_for(h->n, 256), 256, 0, h->st>>>(h->n, h->velout, factor);
+    h->launches += 1;
+    SPH_TRY(h, cudaGetLastError());
+  }
+  return SPH_OK;
 }
 
 int sph_synchronize(SphHandle* h) {
@@ -1249,6 +1331,133 @@ int sph_autotune(SphHandle* h, int trial_steps, SphLaunch* best) {
     g_tune_cache[key] = *best;
   }
   return sph_set_launch(h, best);
+}
+
+static int upload_ktab(SphHandle* h) {
+  h->k = h->ktab_h[0];
+  drop_graphs(h);  // captured launches hold the old constants
+  if (h->ninst > 1)
+    SPH_TRY(h, cudaMemcpyAsync(h->ktab, h->ktab_h.data(), h->ninst * sizeof(SimConst), cudaMemcpyHostToDevice,
+                               h->st));
+  SPH_TRY(h, cudaStreamSynchronize(h->st));
+  return SPH_OK;
+}
+
+int sph_batch_set_feature_sdfs(SphHandle* h, const SphSdfView* sdfs) {
+  if (!h || !sdfs) return SPH_ERR_INVALID_ARG;
+  if (h->k.sdf_mode) return set_err(h, SPH_ERR_INVALID_ARG, "SDF wall mode uses its wall SDF for features");
+  SPH_TRY(h, cudaSetDevice(h->dev));
+  uint64_t total = 0;
+  for (int q = 0; q < h->ninst; ++q) {
+    const SphSdfView& g = sdfs[q];
+    if (!g.distances || !(g.cell_size > 0.0f) || g.dims[0] < 2 || g.dims[1] < 2 || g.dims[2] < 2)
+      return SPH_ERR_INVALID_ARG;
+    total += (uint64_t)g.dims[0] * g.dims[1] * g.dims[2];
+  }
+  float* d = nullptr;
+  cudaError_t e = dalloc(h, &d, total);
+  if (e != cudaSuccess) return cuda_status(h, e, "feature SDF allocation");
+  uint64_t off = 0;
+  for (int q = 0; q < h->ninst; ++q) {
+    const SphSdfView& g = sdfs[q];
+    uint64_t cnt = (uint64_t)g.dims[0] * g.dims[1] * g.dims[2];
+    SPH_TRY(h, cudaMemcpyAsync(d + off, g.distances, cnt * sizeof(float), cudaMemcpyHostToDevice, h->st));
+    SimConst& k = h->ktab_h[q];
+    k.feat_sdf = 1;
+    k.sdf_off = (long long)off;
+    k.sdf_cell = g.cell_size;
+    for (int a = 0; a < 3; ++a) {
+      k.sdf_origin[a] = g.origin[a];
+      k.sdf_dims[a] = (int)g.dims[a];
+    }
+    off += cnt;
+  }
+  h->sdf = d;
+  return upload_ktab(h);
+}
+
+int sph_set_feature_sdf(SphHandle* h, const SphSdfView* sdf) {
+  if (!h || !sdf || h->ninst != 1) return SPH_ERR_INVALID_ARG;
+  return sph_batch_set_feature_sdfs(h, sdf);
+}
+
+int sph_set_closure(SphHandle* h, int mode, const float* params) {
+  if (!h || mode < 0 || mode > 2 || (mode == 2 && !params)) return SPH_ERR_INVALID_ARG;
+  if (mode > 0 && !h->k.feat_sdf) return set_err(h, SPH_ERR_INVALID_ARG, "closure needs a geometry SDF");
+  SPH_TRY(h, cudaSetDevice(h->dev));
+  size_t n = (size_t)h->n;
+  if (mode > 0 && !h->cl_count) {
+    cudaError_t e = dalloc(h, &h->cl_count, 1);
+    if (e == cudaSuccess) e = dalloc(h, &h->cl_slot, n);
+    if (e == cudaSuccess) e = dalloc(h, &h->cl_feat, n * 16);
+    if (e == cudaSuccess) e = dalloc(h, &h->cl_rho, n);
+    if (e == cudaSuccess) e = dalloc(h, &h->corr, n);
+    if (e == cudaSuccess) e = dalloc(h, &h->cl_wf, sphmlp::kParams);
+    if (e == cudaSuccess) e = dalloc(h, &h->cl_wb, sphmlp::kBf16Count);
+    if (e != cudaSuccess) return cuda_status(h, e, "closure allocation");
+    SPH_TRY(h, cudaMemsetAsync(h->cl_count, 0, sizeof(uint32_t), h->st));
+    SPH_TRY(h, cudaMemsetAsync(h->corr, 0, std::max<size_t>(n, 1) * sizeof(float4), h->st));
+  }
+  if (mode == 2) {
+    std::vector<__nv_bfloat16> wb(sphmlp::kBf16Count);
+    for (int i = 0; i < sphmlp::kParams; ++i) {
+      int bi = sphmlp::bf16_index(i);
+      if (bi >= 0) wb[bi] = __float2bfloat16_rn(params[i]);
+    }
+    SPH_TRY(h, cudaMemcpyAsync(h->cl_wf, params, sphmlp::kParams * sizeof(float), cudaMemcpyHostToDevice, h->st));
+    SPH_TRY(h, cudaMemcpyAsync(h->cl_wb, wb.data(), wb.size() * sizeof(__nv_bfloat16), cudaMemcpyHostToDevice,
+                               h->st));
+    SPH_TRY(h, cudaStreamSynchronize(h->st));
+  }
+  h->cl_mode = mode;
+  drop_graphs(h);
+  return SPH_OK;
+}
+
+int sph_closure_samples(SphHandle* h, size_t cap, uint32_t* ids, float* features, float* rho, size_t* count) {
+  if (!h || !count || (cap && (!ids || !features || !rho))) return SPH_ERR_INVALID_ARG;
+  if (!h->cl_mode) return set_err(h, SPH_ERR_INVALID_ARG, "closure capture is off");
+  SPH_TRY(h, cudaSetDevice(h->dev));
+  uint32_t c = 0;
+  SPH_TRY(h, cudaMemcpyAsync(&c, h->cl_count, 4, cudaMemcpyDeviceToHost, h->st));
+  SPH_TRY(h, cudaStreamSynchronize(h->st));
+  *count = c;
+  size_t m = std::min<size_t>(cap, c);
+  if (m == 0) return SPH_OK;
+  std::vector<uint32_t> slots(m), all_ids((size_t)h->n);
+  SPH_TRY(h, cudaMemcpyAsync(slots.data(), h->cl_slot, m * 4, cudaMemcpyDeviceToHost, h->st));
+  SPH_TRY(h, cudaMemcpyAsync(all_ids.data(), h->id, (size_t)h->n * 4, cudaMemcpyDeviceToHost, h->st));
+  SPH_TRY(h, cudaMemcpyAsync(features, h->cl_feat, m * 16 * sizeof(float), cudaMemcpyDeviceToHost, h->st));
+  SPH_TRY(h, cudaMemcpyAsync(rho, h->cl_rho, m * sizeof(float), cudaMemcpyDeviceToHost, h->st));
+  SPH_TRY(h, cudaStreamSynchronize(h->st));
+  for (size_t q = 0; q < m; ++q) ids[q] = all_ids[slots[q]] & sph::kIdMask;
+  return SPH_OK;
+}
+
+int sph_interpolate(SphHandle* h, const float* pts, size_t npts, float* out) {
+  if (!h || (npts && (!pts || !out)) || h->ninst != 1 || npts > 0x7fffffffull) return SPH_ERR_INVALID_ARG;
+  if (npts == 0 || h->n == 0) {
+    if (npts) std::memset(out, 0, npts * 7 * sizeof(float));
+    return SPH_OK;
+  }
+  SPH_TRY(h, cudaSetDevice(h->dev));
+  std::vector<float4> p4(npts);
+  for (size_t q = 0; q < npts; ++q) p4[q] = make_float4(pts[3 * q], pts[3 * q + 1], pts[3 * q + 2], 0.0f);
+  float4* dp = nullptr;
+  float* dout = nullptr;
+  cudaError_t e = cudaMalloc((void**)&dp, npts * sizeof(float4));
+  if (e == cudaSuccess) e = cudaMalloc((void**)&dout, npts * 7 * sizeof(float));
+  if (e == cudaSuccess) e = cudaMemcpyAsync(dp, p4.data(), npts * sizeof(float4), cudaMemcpyHostToDevice, h->st);
+  if (e == cudaSuccess) {
+    sph::k_interpolate<<<grid_for((long long)npts, 128), 128, 0, h->st>>>(sph::OneSim{h->k}, (int)npts, dp, h->pos,
+                                                                          h->rf, h->pr, h->acc, h->ctab, dout);
+    h->launches += 1;
+    e = cudaMemcpyAsync(out, dout, npts * 7 * sizeof(float), cudaMemcpyDeviceToHost, h->st);
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->st);
+  if (dp) cudaFree(dp);
+  if (dout) cudaFree(dout);
+  return cuda_status(h, e, "sph_interpolate");
 }
 
 int sph_grid_info(SphHandle* h, SphGridInfo* out) {

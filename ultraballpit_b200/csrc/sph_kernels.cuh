@@ -20,6 +20,9 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include "sph_cuda.h"
+#include "sph_mlp.cuh"
+
 namespace sph {
 
 constexpr uint32_t kIdMask = 0x7fffffffu;
@@ -59,6 +62,9 @@ struct SimConst {
   int sdf_mode;
   float wall_inv_step;   // kWallN / 2h
   float wall_mid;        // 1.5 * (h / 1.3): depth of the middle wall layer
+  // wall particle mass / (rho0 (h / 1.3)^3): the homogenised wall layers
+  // carry the fluid's particle mass; exactly 1 for mass rho0 dx^3
+  float wall_scale;
   float sdf_origin[3];
   float sdf_cell;
   int sdf_dims[3];
@@ -67,6 +73,10 @@ struct SimConst {
   int inst;
   int coff;
   float cfl;
+  // geometry SDF for the closure features (boundary-particle mode) or the
+  // SDF walls, at sdf_off in the device SDF array
+  int feat_sdf;
+  long long sdf_off;
 };
 
 // Constants provider of a single simulation: the constants ride in the
@@ -175,7 +185,7 @@ __device__ __forceinline__ float sdf_sample_clamped(const float* __restrict__ d,
     fr[a] = g[a] - (float)i0[a];
   }
   size_t ny = (size_t)k.sdf_dims[1], nz = (size_t)k.sdf_dims[2];
-  size_t base = (size_t)i0[0] * ny * nz + (size_t)i0[1] * nz + (size_t)i0[2];
+  size_t base = (size_t)k.sdf_off + (size_t)i0[0] * ny * nz + (size_t)i0[1] * nz + (size_t)i0[2];
   size_t si = ny * nz, sj = nz;
   float c000 = __ldg(&d[base]), c001 = __ldg(&d[base + 1]);
   float c010 = __ldg(&d[base + sj]), c011 = __ldg(&d[base + sj + 1]);
@@ -534,7 +544,19 @@ k_reorder(int n, const uint32_t* __restrict__ tmp, const uint32_t* __restrict__ 
 
 // Density summation + delta-SPH + Tait EOS (lib.rs:213-237; sph.rs:112-216,
 // 295-312). One thread per sorted particle.
-template <class KP>
+// Closure sample buffers of the density pass (particles within 2h of the
+// geometry SDF): count, slot, 16 features, density before correction; and
+// the per-particle acceleration correction consumed by k_forces.
+struct ClosureBufs {
+  uint32_t* count;
+  uint32_t* slot;
+  float* feat;
+  float* rho;
+  float4* corr;
+  const float4* vel;
+};
+
+template <class KP, int CL>
 __global__ void __launch_bounds__(512)
 k_density(KP kp, int n, const float* __restrict__ dtp, const float4* __restrict__ pos,
           const float2* __restrict__ rv, const uint32_t* __restrict__ id,
@@ -542,11 +564,13 @@ k_density(KP kp, int n, const float* __restrict__ dtp, const float4* __restrict_
           const uint32_t* __restrict__ bc_list, const float4* __restrict__ bpos,
           float2* __restrict__ rf, float* __restrict__ pr, const uint32_t* __restrict__ err,
           uint32_t* __restrict__ nbr, uint32_t* __restrict__ ncount, const float* __restrict__ sdf,
-          const float2* __restrict__ wall_tab) {
+          const float2* __restrict__ wall_tab, ClosureBufs cb) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n || *err) return;
   const SimConst& k = kp.at(i);
   float dt = dtp[k.inst];
+  float ssum = 0.0f, rho_wall = 0.0f;  // closure: kernel sum, wall density
+  uint32_t nwall = 0;
   float4 pi = pos[i];
   float rho_old_i = rv[i].x;
   float rho = pi.w * k.norm_h3;
@@ -571,7 +595,9 @@ k_density(KP kp, int n, const float* __restrict__ dtp, const float4* __restrict_
       float density_diff = rho_old_i - rvj.x;
       diff_sum += rvj.y * density_diff * 2.0f * r_dot_grad / (d2 + k.eta_sq);
     }
-    rho += pj.w * w_c2(r, k);
+    float w = w_c2(r, k);
+    rho += pj.w * w;
+    if (CL) ssum += __ldg(&rv[s]).y * w;
   };
   if (listed <= kNbrCap) {
     for (uint32_t c = 0; c < listed; ++c) {
@@ -591,12 +617,17 @@ k_density(KP kp, int n, const float* __restrict__ dtp, const float4* __restrict_
     float4 bp = __ldg(&bpos[__ldg(&bc_list[q])]);
     float dx = pi.x - bp.x, dy = pi.y - bp.y, dz = pi.z - bp.z;
     float d2 = dx * dx + dy * dy + dz * dz;
-    if (d2 <= k.sup_d2) rho += bp.w * w_c2(sqrtf(d2), k);
+    if (d2 <= k.sup_d2) {
+      float wb = bp.w * w_c2(sqrtf(d2), k);
+      rho += wb;
+      if (CL) { rho_wall += wb; ++nwall; }
+    }
   }
   bool air = (id[i] & kAirBit) != 0;
   if (k.sdf_mode) {  // kernel mass of the wall half-space
     float d = sdf_sample_clamped(sdf, k, pi.x, pi.y, pi.z);
-    if (d < k.support) rho += (air ? kAirRho0 : kWaterRho0) * wall_lookup(wall_tab, k.wall_inv_step, d).x;
+    if (d < k.support)
+      rho += (air ? kAirRho0 : kWaterRho0) * k.wall_scale * wall_lookup(wall_tab, k.wall_inv_step, d).x;
   }
   if (delta) {
     float diffusion = k.delta_coef * diff_sum;
@@ -605,6 +636,111 @@ k_density(KP kp, int n, const float* __restrict__ dtp, const float4* __restrict_
   float p = tait(rho, air, k);
   rf[i] = make_float2(rho, p / (rho * rho));
   pr[i] = p;
+  if (CL) {
+    cb.corr[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    float d = sdf_sample_clamped(sdf, k, pi.x, pi.y, pi.z);
+    if (k.feat_sdf && d < k.support) {
+      // Geometry and kinematics only: the particle's own density is not a
+      // feature, so the correction cannot soften the equation of state.
+      float nx, ny, nz;
+      sdf_gradient_clamped(sdf, k, pi.x, pi.y, pi.z, nx, ny, nz);
+      float4 v = cb.vel[i];
+      float rest = air ? kAirRho0 : kWaterRho0;
+      float gm = sqrtf(k.grav[0] * k.grav[0] + k.grav[1] * k.grav[1] + k.grav[2] * k.grav[2]);
+      // h * Laplacian of the SDF (sum of the principal curvatures) by second
+      // differences at step h; the trilinear field is piecewise linear, so a
+      // step of one SDF cell would only see its kinks.
+      float lap = sdf_sample_clamped(sdf, k, pi.x + k.h, pi.y, pi.z) + sdf_sample_clamped(sdf, k, pi.x - k.h, pi.y, pi.z) +
+                  sdf_sample_clamped(sdf, k, pi.x, pi.y + k.h, pi.z) + sdf_sample_clamped(sdf, k, pi.x, pi.y - k.h, pi.z) +
+                  sdf_sample_clamped(sdf, k, pi.x, pi.y, pi.z + k.h) + sdf_sample_clamped(sdf, k, pi.x, pi.y, pi.z - k.h) -
+                  6.0f * d;
+      float f[16];
+      f[0] = d / k.h;
+      f[1] = nx; f[2] = ny; f[3] = nz;
+      f[4] = 1.0f - (rv[i].y * k.norm_h3 + ssum);
+      f[5] = (float)listed / 73.0f;
+      f[6] = sqrtf(v.x * v.x + v.y * v.y + v.z * v.z) / k.c;
+      f[7] = dt * k.c / k.h;
+      f[8] = fminf(fmaxf(lap / k.h, -4.0f), 4.0f);
+      f[9] = k.sdf_mode ? k.wall_scale * wall_lookup(wall_tab, k.wall_inv_step, d).x : rho_wall / rest;
+      f[10] = gm > 0.0f ? (k.grav[0] * nx + k.grav[1] * ny + k.grav[2] * nz) / gm : 0.0f;
+      f[11] = f[0] * f[0];
+      f[12] = f[8] * f[0];
+      f[13] = f[10] * f[0];
+      f[14] = (float)nwall / 30.0f;
+      f[15] = 1.0f;
+      uint32_t q = atomicAdd(cb.count, 1u);
+      cb.slot[q] = (uint32_t)i;
+      cb.rho[q] = rho;
+#pragma unroll
+      for (int a = 0; a < 16; ++a) cb.feat[(size_t)q * 16 + a] = f[a];
+    }
+  }
+}
+
+// Closure inference on the tensor cores for the particles the density pass
+// listed: y = MLP(features); density += y0 rho0 / 100 (EOS re-evaluated),
+// acceleration correction y1..3 |g| stored for k_forces. The outputs are
+// clamped to SPH_CLOSURE_MAX_DRHO_PCT percent of rho0 and
+// SPH_CLOSURE_MAX_ACC_G times |g| per component, so a network queried outside
+// its training data cannot inject an arbitrarily large correction.
+constexpr int kClWarps = 2;
+constexpr float kClosureMaxDrho = SPH_CLOSURE_MAX_DRHO_PCT;
+constexpr float kClosureMaxAcc = SPH_CLOSURE_MAX_ACC_G;
+struct ClSmem {
+  __nv_bfloat16 w1[64 * 16];
+  __nv_bfloat16 w2[64 * 64];
+  __nv_bfloat16 w3[16 * 64];
+  float b[sphmlp::kParamBias];
+  struct Tile {
+    __nv_bfloat16 x[16 * 16];
+    float z1[16 * 64];
+    __nv_bfloat16 h1[16 * 64];
+    float z2[16 * 64];
+    __nv_bfloat16 h2[16 * 64];
+    float y[16 * 4];
+  } t[kClWarps];
+};
+
+template <class KP>
+__global__ void __launch_bounds__(kClWarps * 32)
+k_closure_apply(KP kp, const __nv_bfloat16* __restrict__ wb, const float* __restrict__ wf,
+                const uint32_t* __restrict__ count, const uint32_t* __restrict__ slot,
+                const float* __restrict__ feat, const float* __restrict__ rho_pre,
+                const uint32_t* __restrict__ id, float2* __restrict__ rf, float* __restrict__ pr,
+                float4* __restrict__ corr) {
+  __shared__ ClSmem S;
+  int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  sphmlp::load_weights_smem(wb, wf, S.w1, S.w2, S.w3, S.b);
+  __syncthreads();
+  const uint32_t cnt = *count;
+  auto& T = S.t[warp];
+  for (uint32_t base = (blockIdx.x * kClWarps + warp) * 16; base < cnt; base += gridDim.x * kClWarps * 16) {
+    for (int q = lane; q < 256; q += 32) {
+      uint32_t r = base + (q >> 4);
+      T.x[q] = __float2bfloat16_rn(r < cnt ? feat[(size_t)r * 16 + (q & 15)] : 0.0f);
+    }
+    __syncwarp();
+    sphmlp::forward_tile(T.x, S.w1, S.w2, S.w3, S.b, T.z1, T.h1, T.z2, T.h2, T.y, lane);
+    if (lane < 16 && base + lane < cnt) {
+      uint32_t q = base + lane;
+      int i = (int)slot[q];
+      const SimConst& k = kp.at(i);
+      bool air = (id[i] & kAirBit) != 0;
+      float rest = air ? kAirRho0 : kWaterRho0;
+      float gm = sqrtf(k.grav[0] * k.grav[0] + k.grav[1] * k.grav[1] + k.grav[2] * k.grav[2]);
+      float y0 = fminf(fmaxf(T.y[lane * 4], -kClosureMaxDrho), kClosureMaxDrho);
+      float rho = rho_pre[q] + y0 * rest / 100.0f;
+      float p = tait(rho, air, k);
+      rf[i] = make_float2(rho, p / (rho * rho));
+      pr[i] = p;
+      float c1 = fminf(fmaxf(T.y[lane * 4 + 1], -kClosureMaxAcc), kClosureMaxAcc);
+      float c2 = fminf(fmaxf(T.y[lane * 4 + 2], -kClosureMaxAcc), kClosureMaxAcc);
+      float c3 = fminf(fmaxf(T.y[lane * 4 + 3], -kClosureMaxAcc), kClosureMaxAcc);
+      corr[i] = make_float4(c1 * gm, c2 * gm, c3 * gm, 1.0f);
+    }
+    __syncwarp();
+  }
 }
 
 // Adami boundary pressure (boundary.rs:87-131). One warp per boundary
@@ -723,7 +859,7 @@ k_adami(KP kp, int nb, const float4* __restrict__ bpos, float* __restrict__ bpre
 // Pressure force + Monaghan viscosity + gravity + boundary pressure force +
 // repulsion (lib.rs:247-282; sph.rs:322-508; boundary.rs:143-181), then
 // kick 2 (lib.rs:330-334) and the dt reduction inputs (sph.rs:597-616).
-template <class KP>
+template <class KP, int CL>
 __global__ void __launch_bounds__(512)
 k_forces(KP kp, int n, const float* __restrict__ dtp, float hdt_scale,
          const float4* __restrict__ pos, const float4* __restrict__ vel,
@@ -734,7 +870,7 @@ k_forces(KP kp, int n, const float* __restrict__ dtp, float hdt_scale,
          float4* __restrict__ acc, float4* __restrict__ velout, float* __restrict__ red,
          const uint32_t* __restrict__ err, const uint32_t* __restrict__ nbr,
          const uint32_t* __restrict__ ncount, const float* __restrict__ sdf,
-         const float2* __restrict__ wall_tab) {
+         const float2* __restrict__ wall_tab, const float4* __restrict__ corr) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   float sig = 0.0f, amag = 0.0f;
   int inst = -1;
@@ -816,7 +952,7 @@ k_forces(KP kp, int n, const float* __restrict__ dtp, float hdt_scale,
         float depth = -(d + k.wall_mid);
         float g_dot_dr = k.grav[0] * (depth * nx) + k.grav[1] * (depth * ny) + k.grav[2] * (depth * nz);
         float pw = fmaxf(pic + rho_i * g_dot_dr, 0.0f);
-        float coef = (pic / (rho_i * rho_i) + pw / (rest * rest)) * rest *
+        float coef = (pic / (rho_i * rho_i) + pw / (rest * rest)) * (rest * k.wall_scale) *
                      wall_lookup(wall_tab, k.wall_inv_step, d).y;
         ax += coef * nx;
         ay += coef * ny;
@@ -845,6 +981,10 @@ k_forces(KP kp, int n, const float* __restrict__ dtp, float hdt_scale,
           az += force_mag * dz * inv_r;
         }
       }
+    }
+    if (CL) {  // learned near-wall correction (k_closure_apply)
+      float4 cr = corr[i];
+      if (cr.w != 0.0f) { ax += cr.x; ay += cr.y; az += cr.z; }
     }
     float vx = vi.x + ax * hdt, vy = vi.y + ay * hdt, vz = vi.z + az * hdt;
     acc[i] = make_float4(ax, ay, az, 0.0f);
@@ -976,6 +1116,14 @@ __global__ void k_metrics_final(int nparts, const double* __restrict__ part_m,
     if (part_var[b] > v) v = part_var[b];
   }
   out_me[0] = m; out_me[1] = e; *out_var = v;
+}
+
+// velocity *= factor (the end-of-step velocity the next step starts from)
+__global__ void k_scale_velocities(int n, float4* __restrict__ velout, float factor) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float4 v = velout[i];
+  velout[i] = make_float4(v.x * factor, v.y * factor, v.z * factor, v.w);
 }
 
 // Count of particles with a non-finite position, velocity or density.
@@ -1290,6 +1438,52 @@ __global__ void k_sum_parts_f64(int parts, int cols, const double* __restrict__ 
   double s = 0.0;
   for (int p = 0; p < parts; ++p) s += in[(size_t)p * cols + c];
   out[c] = s;
+}
+
+}  // namespace sph
+
+namespace sph {
+
+// Shepard interpolation of the fluid state at arbitrary points (a fine run
+// sampled where coarse particles are): out[q] = (rho, p, ax, ay, az, wsum, n).
+template <class KP>
+__global__ void k_interpolate(KP kp, int npts, const float4* __restrict__ pts, const float4* __restrict__ pos,
+                              const float2* __restrict__ rf, const float* __restrict__ pr,
+                              const float4* __restrict__ acc, const uint2* __restrict__ ctab,
+                              float* __restrict__ out) {
+  int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= npts) return;
+  const SimConst& k = kp.at(0);
+  float4 x = pts[q];
+  float c3[3] = {x.x, x.y, x.z};
+  int lo[3], hi[3];
+  for (int a = 0; a < 3; ++a) {
+    lo[a] = axis_cell(c3[a] - k.reach, k.gmin[a], k.cell, k.dims[a]);
+    hi[a] = axis_cell(c3[a] + k.reach, k.gmin[a], k.cell, k.dims[a]);
+  }
+  double ws = 0.0, sr = 0.0, sp = 0.0, sa[3] = {0.0, 0.0, 0.0};
+  int cnt = 0;
+  for (int cz = lo[2]; cz <= hi[2]; ++cz)
+    for (int cy = lo[1]; cy <= hi[1]; ++cy)
+      for (int cx = lo[0]; cx <= hi[0]; ++cx) {
+        uint2 se = ctab[k.coff + cell_hash(cx, cy, cz, k)];
+        for (uint32_t s = se.x; s < se.x + se.y; ++s) {
+          float4 pj = pos[s];
+          float dx = x.x - pj.x, dy = x.y - pj.y, dz = x.z - pj.z;
+          float d2 = dx * dx + dy * dy + dz * dz;
+          if (!(d2 <= k.sup_d2)) continue;
+          double w = (double)w_c2(sqrtf(d2), k);
+          float4 a = acc[s];
+          ws += w; sr += w * rf[s].x; sp += w * pr[s];
+          sa[0] += w * a.x; sa[1] += w * a.y; sa[2] += w * a.z;
+          ++cnt;
+        }
+      }
+  float* o = out + (size_t)q * 7;
+  double iw = ws > 0.0 ? 1.0 / ws : 0.0;
+  o[0] = (float)(sr * iw); o[1] = (float)(sp * iw);
+  o[2] = (float)(sa[0] * iw); o[3] = (float)(sa[1] * iw); o[4] = (float)(sa[2] * iw);
+  o[5] = (float)ws; o[6] = (float)cnt;
 }
 
 }  // namespace sph

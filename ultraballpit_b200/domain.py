@@ -291,14 +291,40 @@ def dam_break(dx: float, seed: int = 1234, sphere: bool = False, alpha: float = 
         sdf=sdf, extras=extras)
 
 
+def lattice_kernel_sum(h: float, dx: float) -> float:
+    """S = sum over the cubic lattice of W_C2(|x_ijk|, h) dx^3, self included:
+    the summation density of an undisturbed lattice of mass rho0 dx^3 is
+    S rho0 (1.0096 at h = 1.3 dx)."""
+    m = int(math.ceil(2.0 * h / dx)) + 1
+    r = np.arange(-m, m + 1, dtype=np.float64) * dx
+    X, Y, Z = np.meshgrid(r, r, r, indexing="ij")
+    q = np.sqrt(X * X + Y * Y + Z * Z) / h
+    w = np.where(q < 2.0, (1.0 - 0.5 * q) ** 4 * (1.0 + 2.0 * q), 0.0)
+    return float(21.0 / (16.0 * math.pi * h ** 3) * w.sum() * dx ** 3)
+
+
 def tank_with_sphere(dx: float, domain_max=(0.12, 0.08, 0.08), center=(0.06, 0.04, 0.035),
                      radius: float = 0.02, fill_height: float | None = None, seed: int = 5,
-                     alpha: float = 0.02, sdf_cell: float = 0.002, velocity=(0.0, 0.0, 0.0)) -> Scenario:
+                     alpha: float = 0.02, sdf_cell: float = 0.002, velocity=(0.0, 0.0, 0.0),
+                     hydrostatic: bool = False, solid_gap: float = 0.0) -> Scenario:
     """A closed tank filled with water up to ``fill_height`` around a fixed
     sphere. Lattice points inside the solid (sphere SDF < 0) are skipped as
     ``place_fluid_particles`` does (domain.rs:127-130); the sphere becomes
     geometry boundary particles (domain.rs:351-402) and is merged into the
-    SDF. ``velocity`` is an initial uniform fluid velocity."""
+    SDF. ``velocity`` is an initial uniform fluid velocity. ``solid_gap``
+    (in units of dx) also skips lattice points closer than that to the
+    sphere: 0.5 gives the sphere the half-spacing gap the lattice keeps
+    from the flat walls.
+
+    ``hydrostatic`` starts the water at rest in its hydrostatic state. The
+    particle (and wall) mass is rho0 dx^3 / S with S = sum W(|x_ijk|) dx^3
+    over the full lattice (1.0096 at h = 1.3 dx), so the undisturbed
+    lattice sums to rho0 instead of S rho0; then, as the summation density
+    follows the spacing, the lattice is compressed vertically to the Tait
+    density of p = rho0 g (H - z): dz'/dz = rho0 / rho(z) = 1 - p / (7 B)
+    to first order, i.e. z' = z - rho0 g (H z - z^2 / 2) / (7 B) with
+    B = rho0 c0^2 / 7. Without it the column starts about 3 kPa above its
+    hydrostatic pressure, expands and rings for tenths of a second."""
     dmin = (0.0, 0.0, 0.0)
     dmax = tuple(float(v) for v in domain_max)
     dx32 = f32(dx)
@@ -306,16 +332,24 @@ def tank_with_sphere(dx: float, domain_max=(0.12, 0.08, 0.08), center=(0.06, 0.0
     counts = (_axis_count(0.0, dmax[0], dx32), _axis_count(0.0, dmax[1], dx32), _axis_count(0.0, fill, dx32))
     sph = sphere_sdf(dmin, dmax, sdf_cell, center, radius)
     parts = block_particles(dmin, counts, dx32, seed)
+    c0 = dam_break_c0(fill)
+    if hydrostatic:
+        top = counts[2] * float(dx32)
+        b = 1000.0 * c0 * c0 / 7.0
+        z = parts.z.astype(np.float64)
+        parts.z[:] = (z - 1000.0 * 9.81 * (top * z - 0.5 * z * z) / (7.0 * b)).astype(np.float32)
     pts = np.stack([parts.x, parts.y, parts.z], axis=-1)
-    keep = sdf_sample(sph, pts) >= f32(0)
-    p = ParticleArrays.from_positions(parts.x[keep], parts.y[keep], parts.z[keep], particle_mass(dx32))
-    p.vx[:], p.vy[:], p.vz[:] = (f32(v) for v in velocity)
+    keep = sdf_sample(sph, pts) >= f32(solid_gap * float(dx32))
     m = particle_mass(dx32)
+    if hydrostatic:
+        m = f32(float(m) / lattice_kernel_sum(float(smoothing_length(dx32)), float(dx32)))
+    p = ParticleArrays.from_positions(parts.x[keep], parts.y[keep], parts.z[keep], m)
+    p.vx[:], p.vy[:], p.vz[:] = (f32(v) for v in velocity)
     walls = wall_boundary_particles(dmin, dmax, dx32, m)
     geo = geometry_boundary_particles(sph, dmin, dmax, dx32, m)
     sdf = merge_sdf(box_sdf(dmin, dmax, sdf_cell), sph)
     return Scenario(f"tank_sphere_dx{dx*1e3:g}mm", p, concat_boundary(walls, geo), float(smoothing_length(dx32)),
-                    (0.0, 0.0, -9.81), dam_break_c0(fill), 0.25, 0.0, dmin, dmax, alpha=alpha, sdf=sdf,
+                    (0.0, 0.0, -9.81), c0, 0.25, 0.0, dmin, dmax, alpha=alpha, sdf=sdf,
                     extras=dict(sphere_center=center, sphere_radius=radius, sphere_sdf=sph,
                                 n_geometry_boundary=len(geo), n_wall_boundary=len(walls)))
 

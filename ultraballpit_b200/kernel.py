@@ -37,11 +37,14 @@ EXPORTS = (
     "sph_params_default", "sph_create", "sph_destroy", "sph_step", "sph_step_auto",
     "sph_compute_timestep", "sph_step_profiled", "sph_read_particles",
     "sph_read_boundary_pressure", "sph_error_metrics", "sph_particle_count",
-    "sph_save_checkpoint", "sph_restore_checkpoint", "sph_synchronize", "sph_health",
+    "sph_save_checkpoint", "sph_restore_checkpoint", "sph_scale_velocities", "sph_synchronize", "sph_health",
     "sph_last_error", "sph_stream", "sph_launch_count", "sph_grid_info", "sph_read_grid",
     "sph_neighbors", "sph_grid_sort_noalloc", "sph_set_geometry_sdf", "sph_surface_forces",
     "sph_body_force", "sph_batch_create", "sph_batch_info", "sph_batch_timesteps", "sph_set_launch",
-    "sph_get_launch", "sph_autotune",
+    "sph_get_launch", "sph_autotune", "sph_mlp_create", "sph_mlp_destroy", "sph_mlp_set_params",
+    "sph_mlp_get_params", "sph_mlp_forward", "sph_mlp_loss_grad", "sph_mlp_train",
+    "sph_set_feature_sdf", "sph_batch_set_feature_sdfs", "sph_set_closure", "sph_closure_samples",
+    "sph_interpolate", "sph_batch_create_sdf",
 )
 
 
@@ -147,6 +150,8 @@ def load_library(path: str | None = None):
     L.sph_particle_count.restype = C.c_size_t
     L.sph_save_checkpoint.argtypes = [H]
     L.sph_restore_checkpoint.argtypes = [H]
+    L.sph_scale_velocities.argtypes = [H, C.c_float]
+    L.sph_scale_velocities.restype = C.c_int
     L.sph_synchronize.argtypes = [H]
     L.sph_health.argtypes = [H, C.POINTER(C.c_uint64)]
     L.sph_last_error.argtypes = [H]
@@ -160,11 +165,22 @@ def load_library(path: str | None = None):
     L.sph_neighbors.argtypes = [H, C.c_uint32, _U32P, C.c_size_t, C.POINTER(C.c_size_t)]
     L.sph_batch_create.argtypes = [C.c_int, C.POINTER(SphParams), C.POINTER(SphParticlesView),
                                    C.POINTER(SphBoundaryView), C.POINTER(vp)]
+    L.sph_batch_create_sdf.argtypes = [C.c_int, C.POINTER(SphParams), C.POINTER(SphParticlesView),
+                                       C.POINTER(SphSdfView), C.POINTER(vp)]
+    L.sph_batch_create_sdf.restype = C.c_int
     L.sph_batch_info.argtypes = [H, C.POINTER(C.c_int), C.POINTER(C.c_size_t), C.POINTER(C.c_size_t)]
     L.sph_batch_timesteps.argtypes = [H, _FP]
     L.sph_set_launch.argtypes = [H, C.POINTER(SphLaunch)]
     L.sph_get_launch.argtypes = [H, C.POINTER(SphLaunch)]
     L.sph_autotune.argtypes = [H, C.c_int, C.POINTER(SphLaunch)]
+    L.sph_set_feature_sdf.argtypes = [H, C.POINTER(SphSdfView)]
+    L.sph_batch_set_feature_sdfs.argtypes = [H, C.POINTER(SphSdfView)]
+    L.sph_set_closure.argtypes = [H, C.c_int, _FP]
+    L.sph_closure_samples.argtypes = [H, C.c_size_t, _U32P, _FP, _FP, C.POINTER(C.c_size_t)]
+    L.sph_interpolate.argtypes = [H, _FP, C.c_size_t, _FP]
+    for f in ("sph_set_feature_sdf", "sph_batch_set_feature_sdfs", "sph_set_closure", "sph_closure_samples",
+              "sph_interpolate"):
+        getattr(L, f).restype = C.c_int
     L.sph_set_geometry_sdf.argtypes = [H, C.POINTER(SphSdfView)]
     L.sph_surface_forces.argtypes = [H, C.POINTER(SphSurfaceForce)]
     L.sph_body_force.argtypes = [H, C.c_uint32, C.c_uint32, C.POINTER(SphBodyForce)]
@@ -372,6 +388,11 @@ class CudaKernel(SimulationKernel):
         self._cache = None
         return prof.as_dict()
 
+    def scale_velocities(self, factor: float) -> None:
+        """velocity *= factor for every particle; 0 between steps is kinetic
+        damping (relaxing an initial lattice before a run)."""
+        self._check(self._lib.sph_scale_velocities(self._h, float(factor)), "sph_scale_velocities")
+
     def synchronize(self) -> None:
         self._check(self._lib.sph_synchronize(self._h), "sph_synchronize")
 
@@ -439,6 +460,44 @@ class CudaKernel(SimulationKernel):
                     "sph_neighbors")
         return out[:min(cap, cnt.value)].copy()
 
+    # -- learned closure ---------------------------------------------------------
+    @staticmethod
+    def _sdf_view(sdf: GridSDF, keep: list) -> SphSdfView:
+        d = np.ascontiguousarray(sdf.distances, np.float32)
+        keep.append(d)
+        return SphSdfView((C.c_float * 3)(*map(float, sdf.origin)), float(sdf.cell_size),
+                          (C.c_uint32 * 3)(*map(int, sdf.dimensions)), _fp(d))
+
+    def set_feature_sdf(self, sdf: GridSDF) -> None:
+        """Geometry SDF (walls and obstacles) of the closure features."""
+        keep = []
+        sv = self._sdf_view(sdf, keep)
+        self._check(self._lib.sph_set_feature_sdf(self._h, C.byref(sv)), "sph_set_feature_sdf")
+
+    def set_closure(self, mode: int, params=None) -> None:
+        """0 off, 1 record features, 2 record and apply ``params``."""
+        p = None if params is None else np.ascontiguousarray(params, np.float32)
+        self._check(self._lib.sph_set_closure(self._h, int(mode), None if p is None else _fp(p)), "sph_set_closure")
+
+    def closure_samples(self):
+        """(ids, features[n, 16], density before correction) of the last density pass."""
+        cnt = C.c_size_t()
+        self._check(self._lib.sph_closure_samples(self._h, 0, None, None, None, C.byref(cnt)), "sph_closure_samples")
+        n = cnt.value
+        ids = np.zeros(n, np.uint32)
+        feat = np.zeros((n, 16), np.float32)
+        rho = np.zeros(n, np.float32)
+        self._check(self._lib.sph_closure_samples(self._h, n, _u32p(ids), _fp(feat), _fp(rho), C.byref(cnt)),
+                    "sph_closure_samples")
+        return ids, feat, rho
+
+    def interpolate(self, pts) -> np.ndarray:
+        """Shepard interpolation at pts[n, 3]: columns rho, p, ax, ay, az, wsum, count."""
+        pts = np.ascontiguousarray(pts, np.float32)
+        out = np.zeros((pts.shape[0], 7), np.float32)
+        self._check(self._lib.sph_interpolate(self._h, _fp(pts), pts.shape[0], _fp(out)), "sph_interpolate")
+        return out
+
     # -- launch shapes ---------------------------------------------------------
     def launch(self) -> dict:
         l = SphLaunch()
@@ -462,7 +521,8 @@ class CudaBatch(CudaKernel):
     per instance (``domain.Scenario``); ``particles()`` returns the instances
     one after another, ``instance(q)`` slices one out."""
 
-    def __init__(self, scenarios, device: int = 0, cell_order: int = CELL_ORDER_MORTON):
+    def __init__(self, scenarios, device: int = 0, cell_order: int = CELL_ORDER_MORTON,
+                 boundary_mode: int = BOUNDARY_PARTICLES):
         L = load_library()
         self._lib = L
         self._keep = []
@@ -470,22 +530,29 @@ class CudaBatch(CudaKernel):
         prms = (SphParams * nq)()
         views = (SphParticlesView * nq)()
         bviews = (SphBoundaryView * nq)()
+        sviews = (SphSdfView * nq)()
         for q, sc in enumerate(scenarios):
             sc.particles.validate()
             prms[q] = make_params(sc.h, sc.gravity, sc.speed_of_sound, sc.cfl_number, sc.viscosity,
                                   sc.domain_min, sc.domain_max, alpha=sc.alpha, beta=sc.beta,
-                                  cell_order=cell_order, device=device)
+                                  cell_order=cell_order, device=device, boundary_mode=boundary_mode)
             views[q] = _particles_view(sc.particles, self._keep)
             bviews[q] = _boundary_view(sc.boundary, self._keep)
+            if boundary_mode == BOUNDARY_SDF:
+                sviews[q] = self._sdf_view(sc.sdf, self._keep)
         handle = C.c_void_p()
-        st = L.sph_batch_create(nq, prms, views, bviews, C.byref(handle))
+        if boundary_mode == BOUNDARY_SDF:
+            st = L.sph_batch_create_sdf(nq, prms, views, sviews, C.byref(handle))
+        else:
+            st = L.sph_batch_create(nq, prms, views, bviews, C.byref(handle))
         self._keep = []
         if st != SPH_OK:
             raise SphError(st, "sph_batch_create failed")
         self._h = handle
         self._cache = None
         self._n = sum(len(sc.particles) for sc in scenarios)
-        self._nb = sum(len(sc.boundary) if sc.boundary is not None else 0 for sc in scenarios)
+        self._nb = 0 if boundary_mode == BOUNDARY_SDF else sum(
+            len(sc.boundary) if sc.boundary is not None else 0 for sc in scenarios)
         self.ninst = nq
         first = (C.c_size_t * nq)()
         count = (C.c_size_t * nq)()
@@ -493,6 +560,11 @@ class CudaBatch(CudaKernel):
         self._check(L.sph_batch_info(self._h, C.byref(ni), first, count), "sph_batch_info")
         self.first = np.array(first[:], np.int64)
         self.count = np.array(count[:], np.int64)
+
+    def set_feature_sdfs(self, sdfs) -> None:
+        keep = []
+        arr = (SphSdfView * len(sdfs))(*[self._sdf_view(sd, keep) for sd in sdfs])
+        self._check(self._lib.sph_batch_set_feature_sdfs(self._h, arr), "sph_batch_set_feature_sdfs")
 
     def timesteps(self) -> np.ndarray:
         out = np.zeros(self.ninst, np.float32)
