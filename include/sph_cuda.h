@@ -285,16 +285,17 @@ int sph_batch_set_feature_sdfs(SphHandle *h, const SphSdfView *sdfs);
 /* mode 0: off (the plain step). 1: the density pass records the features of
  * near-geometry particles (sph_closure_samples) without changing the step.
  * 2: also evaluates the network (`params`, SPH_MLP_PARAMS floats) on the
- * tensor cores after the density pass: density += y0 rho0 / 100 with the
+ * tensor cores after the density pass: density += y0 rho0 SPH_CLOSURE_DRHO_UNIT with the
  * EOS re-evaluated, acceleration += (y1, y2, y3) |g| in the force kernel,
- * y0 clamped to +-SPH_CLOSURE_MAX_DRHO_PCT and y1..3 to +-SPH_CLOSURE_MAX_ACC_G.
+ * y0 clamped to +-SPH_CLOSURE_MAX_DRHO and y1..3 to +-SPH_CLOSURE_MAX_ACC_G.
  * Features (d = SDF distance, n = SDF gradient):
  *   0 d/h, 1-3 n, 4 1 - Shepard kernel sum, 5 listed neighbours / 73,
  *   6 |v|/c, 7 dt c/h, 8 h * Laplacian of the SDF (clamped to +-4),
  *   9 wall-table kernel mass at d (SDF mode; else boundary density / rho0),
  *   10 n.g/|g|, 11 (d/h)^2, 12 f8 f0, 13 f10 f0,
  *   14 boundary particles in support / 30, 15 1. */
-#define SPH_CLOSURE_MAX_DRHO_PCT 3.0f
+#define SPH_CLOSURE_DRHO_UNIT 1e-4f /* y0 in units of 0.01 % of rho0 */
+#define SPH_CLOSURE_MAX_DRHO 300.0f  /* 3 % of rho0 */
 #define SPH_CLOSURE_MAX_ACC_G 25.0f
 int sph_set_closure(SphHandle *h, int mode, const float *params);
 /* Samples of the last density pass: original particle ids, 16 features each

@@ -102,27 +102,31 @@ class ClosureNet:
 # ---------------------------------------------------------------------------
 
 RHO0, G = 1000.0, 9.81
+FILL = 0.16  # 40 layers at 4 mm, 80 at 2 mm
+SETTLE_S = 0.05  # kinetic-damping relaxation before every paired run
 TANK = (0.1, 0.1, 0.2)
 ALPHA = 0.02
 
 
-def tank_pair(seed: int, dx_coarse: float = 0.004, fill: float = 0.15, alpha: float = ALPHA):
-    """Hydrostatic tank 0.1 x 0.1 x 0.2 m filled to ``fill`` around a fixed
-    sphere of seeded radius in [0.01, 0.03] m at a seeded submerged position,
-    at dx and dx / 2. The runs use the SDF wall mode: the reference's
-    geometry particles (3 layers inward along -grad SDF) pile up inside a
-    sphere of only a few coarse spacings in radius."""
+def tank_pair(seed: int, dx_coarse: float = 0.004, fill: float = FILL, alpha: float = ALPHA):
+    """Hydrostatic tank 0.1 x 0.1 x 0.2 m filled to ``fill`` (a multiple of
+    both spacings, so both runs hold the same water) around a fixed sphere
+    of seeded radius in [0.01, 0.03] m at a seeded submerged position, at dx
+    and dx / 2; fluid, walls and sphere on one lattice (``tank_with_sphere``
+    with ``geometry="lattice"``). The seed also draws the speed U in
+    [0, 0.5] m/s the moving variant starts with (``settled_pair``)."""
     from . import domain
     rng = np.random.default_rng(seed)
     r = rng.uniform(0.01, 0.03)
     m = r + 0.008
     c = (rng.uniform(m, TANK[0] - m), rng.uniform(m, TANK[1] - m), rng.uniform(m, fill - m))
+    speed = rng.uniform(0.0, 0.5)
     out = []
     for dx in (dx_coarse, dx_coarse / 2):
         sc = domain.tank_with_sphere(dx, domain_max=TANK, center=c, radius=r, fill_height=fill, seed=seed,
-                                     alpha=alpha, hydrostatic=True)
+                                     alpha=alpha, hydrostatic=True, geometry="lattice")
         out.append(sc)
-    return out[0], out[1], dict(center=c, radius=r)
+    return out[0], out[1], dict(center=c, radius=r, speed=speed)
 
 
 def settle(sc, seconds: float = 0.05, dt: float = 5e-5, every: int = 20, device: int = 0):
@@ -149,21 +153,46 @@ def settle(sc, seconds: float = 0.05, dt: float = 5e-5, every: int = 20, device:
     return dataclasses.replace(sc, particles=q)
 
 
-def _kernel(sc, device=0):
-    """The tank in SDF wall mode (walls and sphere from the merged SDF, which
-    also gives the closure features)."""
+# Wall treatment of the closure tanks: "particles" (the reference's wall and
+# geometry boundary particles with Adami pressure) or "sdf" (the homogenised
+# SDF wall layers). The merged SDF gives the closure features either way.
+WALLS = "particles"
+
+
+def _kernel(sc, device=0, walls=None):
     from .kernel import BOUNDARY_SDF, CudaKernel
-    return CudaKernel(*sc.kernel_args(), alpha=sc.alpha, device=device, boundary_mode=BOUNDARY_SDF, sdf=sc.sdf)
+    if (walls or WALLS) == "sdf":
+        return CudaKernel(*sc.kernel_args(), alpha=sc.alpha, device=device, boundary_mode=BOUNDARY_SDF, sdf=sc.sdf)
+    k = CudaKernel(*sc.kernel_args(), alpha=sc.alpha, device=device)
+    k.set_feature_sdf(sc.sdf)
+    return k
+
+
+def settled_pair(seed: int, dx_coarse: float = 0.004, dt_coarse: float = 5e-5, settle_s: float = SETTLE_S,
+                 device: int = 0, moving: bool = False):
+    """tank_pair with both tanks relaxed (``settle``) for ``settle_s``; with
+    ``moving`` the water then starts at the seed's speed along +x."""
+    coarse_sc, fine_sc, geo = tank_pair(seed, dx_coarse)
+    if settle_s > 0:
+        coarse_sc = settle(coarse_sc, settle_s, dt_coarse, device=device)
+        fine_sc = settle(fine_sc, settle_s, dt_coarse / 2, device=device)
+    if moving:
+        for sc in (coarse_sc, fine_sc):
+            sc.particles.vx[:] = np.float32(geo["speed"])
+    return coarse_sc, fine_sc, geo
 
 
 def run_pair(seed: int, t_snap=(0.02, 0.03, 0.04, 0.05), dt_coarse: float = 5e-5, device: int = 0,
-             dx_coarse: float = 0.004):
-    """Samples (features, targets) of one tank pair at the snapshot times.
+             dx_coarse: float = 0.004, settle_s: float = SETTLE_S, moving: bool = False):
+    """Samples (features, targets) of one settled tank pair at the snapshot
+    times (seconds after the relaxation).
 
-    Targets: t0 = (rho_fine(x) - rho_coarse) / rho0 * 100 and
-    t1..3 = (a_fine(x) - a_coarse) / |g|, with the fine run (dx / 2,
-    dt / 2) interpolated at the coarse sample positions at the same time."""
-    coarse_sc, fine_sc, geo = tank_pair(seed, dx_coarse)
+    Targets in physical units: (p_f(x) - p_c(x), a_f(x) - a_c(x)), Pa and
+    m/s^2, with both runs Shepard-interpolated at the coarse sample
+    positions x at the same time (the fine run at dx / 2, dt / 2):
+    smoothing the coarse side too removes the sample particle's own noise,
+    which no feature can predict. Returned in network units (``to_units``)."""
+    coarse_sc, fine_sc, geo = settled_pair(seed, dx_coarse, dt_coarse, settle_s, device, moving)
     kc, kf = _kernel(coarse_sc, device), _kernel(fine_sc, device)
     kc.set_closure(1)
     X, T, step = [], [], 0
@@ -178,12 +207,11 @@ def run_pair(seed: int, t_snap=(0.02, 0.03, 0.04, 0.05), dt_coarse: float = 5e-5
         pc = kc.particles()
         pts = np.stack([pc.x[ids], pc.y[ids], pc.z[ids]], axis=1)
         fine = kf.interpolate(pts)
-        ok = fine[:, 6] > 0
-        acc_c = np.stack([pc.ax[ids], pc.ay[ids], pc.az[ids]], axis=1)
-        tgt = np.concatenate([((fine[:, 0] - rho_pre) / RHO0 * 100.0)[:, None],
-                              (fine[:, 2:5] - acc_c) / G], axis=1)
+        crs = kc.interpolate(pts)
+        ok = (fine[:, 6] > 0) & (crs[:, 6] > 0)
+        tgt = np.concatenate([(fine[:, 1] - crs[:, 1])[:, None], fine[:, 2:5] - crs[:, 2:5]], axis=1)
         X.append(feat[ok])
-        T.append(tgt[ok].astype(np.float32))
+        T.append(to_units(tgt[ok], coarse_sc.speed_of_sound))
     kc.close()
     kf.close()
     return np.concatenate(X), np.concatenate(T)
@@ -199,8 +227,20 @@ def generate(seeds, **kw):
     return np.concatenate(xs), np.concatenate(ts), np.concatenate(owners)
 
 
-# Output clamps of the step (SPH_CLOSURE_MAX_DRHO_PCT, SPH_CLOSURE_MAX_ACC_G).
-CLAMP_DRHO_PCT, CLAMP_ACC_G = 3.0, 25.0
+# Output units and clamps of the step: y0 in SPH_CLOSURE_DRHO_UNIT rho0
+# (clamped to SPH_CLOSURE_MAX_DRHO), y1..3 in |g| (SPH_CLOSURE_MAX_ACC_G).
+DRHO_UNIT, CLAMP_DRHO, CLAMP_ACC_G = 1e-4, 300.0, 25.0
+
+
+def to_units(raw, c: float) -> np.ndarray:
+    """(dp [Pa], da [m/s^2]) -> network outputs: a density change of
+    dp / c^2 (the Tait slope at rest) in units of DRHO_UNIT rho0, and
+    accelerations in units of |g|."""
+    raw = np.asarray(raw, np.float64)
+    out = np.empty_like(raw)
+    out[:, 0] = raw[:, 0] / (c * c * RHO0 * DRHO_UNIT)
+    out[:, 1:] = raw[:, 1:] / G
+    return out.astype(np.float32)
 
 
 def prepare_targets(t, lo: float = 1.0, hi: float = 99.0) -> np.ndarray:
@@ -212,7 +252,7 @@ def prepare_targets(t, lo: float = 1.0, hi: float = 99.0) -> np.ndarray:
     for j in range(t.shape[1]):
         a, b = np.percentile(t[:, j], [lo, hi])
         np.clip(t[:, j], a, b, out=t[:, j])
-    np.clip(t[:, 0], -CLAMP_DRHO_PCT, CLAMP_DRHO_PCT, out=t[:, 0])
+    np.clip(t[:, 0], -CLAMP_DRHO, CLAMP_DRHO, out=t[:, 0])
     np.clip(t[:, 1:], -CLAMP_ACC_G, CLAMP_ACC_G, out=t[:, 1:])
     return t
 
@@ -227,7 +267,7 @@ def split_by_tank(owners, frac: float = 0.1, seed: int = 0):
     return np.isin(owners, out)
 
 
-def probe_points(geo, h: float, fill: float = 0.15, tank=TANK, n_sphere: int = 256):
+def probe_points(geo, h: float, fill: float = FILL, tank=TANK, n_sphere: int = 256):
     """Fixed near-wall pressure probes at distance h from the geometry:
     a Fibonacci lattice on the sphere (radius r + h) and grids on the floor
     and the four side walls, each at least 2h from the other surfaces and
@@ -251,6 +291,18 @@ def probe_points(geo, h: float, fill: float = 0.15, tank=TANK, n_sphere: int = 2
     walls = np.concatenate(pts)
     walls = walls[np.linalg.norm(walls - c, axis=1) - r >= 2 * h]
     return sph.astype(np.float32), walls.astype(np.float32)
+
+
+def _sphere_force(k, sc) -> np.ndarray:
+    """Fluid force on the sphere: with boundary particles the FP64 reaction
+    (pressure + repulsion) on the sphere's particles, which is a pairwise
+    sum and so comparable across resolutions; in SDF wall mode the surface
+    integral of force.rs, whose 2h node shell makes it scale with h."""
+    ex = sc.extras
+    if (WALLS == "particles") and ex.get("n_geometry_boundary", 0):
+        f = k.body_force(ex["n_wall_boundary"], ex["n_geometry_boundary"])
+        return np.asarray(f["pressure_force"]) + np.asarray(f["repulsion_force"])
+    return k.surface_forces()["force"]
 
 
 def run_probes(sc, probes, steps: int, dt: float, every: int, start: int, mode: int = 0, params=None,
@@ -281,14 +333,14 @@ def run_probes(sc, probes, steps: int, dt: float, every: int, start: int, mode: 
         ok = out[:, 6] > 0
         acc[ok] += out[ok, 1]
         cnt[ok] += 1
-        forces.append(k.surface_forces()["force"])
+        forces.append(_sphere_force(k, sc))
     k.health()
     k.close()
     return acc / np.maximum(cnt, 1), cnt, np.mean(forces, axis=0), secs
 
 
 def compare(seed: int, params=None, steps: int = 800, dt: float = 5e-5, every: int = 20, start: int | None = None,
-            dx_coarse: float = 0.004, device: int = 0) -> dict:
+            dx_coarse: float = 0.004, device: int = 0, settle_s: float = SETTLE_S, moving: bool = False) -> dict:
     """The fine tank (dx / 2, dt / 2) judges the coarse tank without
     (``plain``) and, when ``params`` is given, with the closure
     (``closure``): near-wall pressure error = mean |p_c - p_f| / mean |p_f|
@@ -297,7 +349,7 @@ def compare(seed: int, params=None, steps: int = 800, dt: float = 5e-5, every: i
     |F_c - F_f| / |F_f| for the time-averaged pressure force on the sphere;
     ``speedup`` = fine stepping time / coarse stepping time."""
     start = steps // 2 if start is None else start
-    coarse, fine, geo = tank_pair(seed, dx_coarse)
+    coarse, fine, geo = settled_pair(seed, dx_coarse, dt, settle_s, device, moving)
     sph, walls = probe_points(geo, coarse.h)
     probes = np.concatenate([sph, walls])
     ns = len(sph)

@@ -679,13 +679,14 @@ k_density(KP kp, int n, const float* __restrict__ dtp, const float4* __restrict_
 }
 
 // Closure inference on the tensor cores for the particles the density pass
-// listed: y = MLP(features); density += y0 rho0 / 100 (EOS re-evaluated),
+// listed: y = MLP(features); density += y0 rho0 1e-4 (EOS re-evaluated),
 // acceleration correction y1..3 |g| stored for k_forces. The outputs are
-// clamped to SPH_CLOSURE_MAX_DRHO_PCT percent of rho0 and
+// clamped to SPH_CLOSURE_MAX_DRHO units (3 % of rho0) and
 // SPH_CLOSURE_MAX_ACC_G times |g| per component, so a network queried outside
 // its training data cannot inject an arbitrarily large correction.
 constexpr int kClWarps = 2;
-constexpr float kClosureMaxDrho = SPH_CLOSURE_MAX_DRHO_PCT;
+constexpr float kClosureMaxDrho = SPH_CLOSURE_MAX_DRHO;
+constexpr float kClosureDrhoUnit = SPH_CLOSURE_DRHO_UNIT;
 constexpr float kClosureMaxAcc = SPH_CLOSURE_MAX_ACC_G;
 struct ClSmem {
   __nv_bfloat16 w1[64 * 16];
@@ -730,7 +731,7 @@ k_closure_apply(KP kp, const __nv_bfloat16* __restrict__ wb, const float* __rest
       float rest = air ? kAirRho0 : kWaterRho0;
       float gm = sqrtf(k.grav[0] * k.grav[0] + k.grav[1] * k.grav[1] + k.grav[2] * k.grav[2]);
       float y0 = fminf(fmaxf(T.y[lane * 4], -kClosureMaxDrho), kClosureMaxDrho);
-      float rho = rho_pre[q] + y0 * rest / 100.0f;
+      float rho = rho_pre[q] + y0 * (rest * kClosureDrhoUnit);
       float p = tait(rho, air, k);
       rf[i] = make_float2(rho, p / (rho * rho));
       pr[i] = p;

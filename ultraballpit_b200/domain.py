@@ -182,6 +182,59 @@ def merge_sdf(a: GridSDF, b: GridSDF) -> GridSDF:
     return GridSDF(a.origin, a.cell_size, a.dimensions, np.minimum(a.distances, b.distances))
 
 
+def lattice_box_walls(domain_min, domain_max, dx, mass, n_layers: int = 3) -> BoundaryParticles:
+    """Walls of the domain box on the fluid lattice: per axis the lattice
+    ``lo + (i + 0.5) dx`` inside and ``n_layers`` sites beyond each face
+    (``lo - (l + 0.5) dx``, ``hi + (l + 0.5) dx``), every combination with a
+    coordinate outside the box. Unlike the reference's per-face layers
+    (domain.rs:162-348), which span only the box in the tangential
+    directions, this fills the edge and corner columns, so a particle in an
+    edge or corner sees as much wall mass as one beside a face. Normals
+    point from the site to the nearest point of the box."""
+    dx = f32(dx)
+    axes, inside = [], []
+    for k in range(3):
+        lo, hi = f32(domain_min[k]), f32(domain_max[k])
+        n = _axis_count(lo, hi, dx)
+        layers = (np.arange(n_layers, dtype=np.float32) + f32(0.5)) * dx
+        a = np.concatenate([(lo - layers[::-1]).astype(np.float32), _lattice(lo, n, dx),
+                            (hi + layers).astype(np.float32)])
+        axes.append(a)
+        inside.append((a > lo) & (a < hi))
+    X, Y, Z = np.meshgrid(*axes, indexing="ij")
+    I = np.meshgrid(*inside, indexing="ij")
+    sel = ~(I[0] & I[1] & I[2])
+    pts = np.stack([X[sel], Y[sel], Z[sel]], axis=-1).astype(np.float64)
+    lo = np.asarray(domain_min, np.float64)
+    hi = np.asarray(domain_max, np.float64)
+    nrm = np.clip(pts, lo, hi) - pts
+    nrm /= np.maximum(np.linalg.norm(nrm, axis=1, keepdims=True), 1e-30)
+    pts = pts.astype(np.float32)
+    return BoundaryParticles.from_arrays(pts[:, 0], pts[:, 1], pts[:, 2], np.full(len(pts), f32(mass)),
+                                         nrm[:, 0], nrm[:, 1], nrm[:, 2])
+
+
+def lattice_solid_particles(sdf: GridSDF, domain_min, domain_max, dx, mass,
+                            n_layers: int = 3) -> BoundaryParticles:
+    """Boundary particles at the fluid lattice's own sites (``lo + (i + 0.5)
+    dx``) inside the solid, within ``n_layers`` spacings of its surface
+    (-n_layers dx <= SDF < 0), normals from the SDF gradient. With the fluid
+    seeded at the sites where SDF >= 0, fluid and wall tile one lattice, so
+    the summation density starts uniform up to the surface; the reference's
+    layers along the inward normal (domain.rs:351-402) crowd together inside
+    a body only a few spacings in radius."""
+    dx = f32(dx)
+    n = [_axis_count(domain_min[k], domain_max[k], dx) for k in range(3)]
+    ax = [_lattice(domain_min[k], n[k], dx) for k in range(3)]
+    X, Y, Z = np.meshgrid(*ax, indexing="ij")
+    pts = np.stack([X.ravel(), Y.ravel(), Z.ravel()], axis=-1)
+    d = sdf_sample(sdf, pts)
+    p = pts[(d < f32(0)) & (d >= -f32(n_layers) * dx)]
+    nrm = sdf_gradient(sdf, p) if len(p) else np.zeros((0, 3), np.float32)
+    return BoundaryParticles.from_arrays(p[:, 0], p[:, 1], p[:, 2], np.full(len(p), f32(mass)),
+                                         nrm[:, 0], nrm[:, 1], nrm[:, 2])
+
+
 def geometry_boundary_particles(sdf: GridSDF, domain_min, domain_max, dx, mass,
                                 n_layers: int = 3) -> BoundaryParticles:
     """``domain.rs:351-402``: 3 layers along the inward normal at lattice points
@@ -306,7 +359,8 @@ def lattice_kernel_sum(h: float, dx: float) -> float:
 def tank_with_sphere(dx: float, domain_max=(0.12, 0.08, 0.08), center=(0.06, 0.04, 0.035),
                      radius: float = 0.02, fill_height: float | None = None, seed: int = 5,
                      alpha: float = 0.02, sdf_cell: float = 0.002, velocity=(0.0, 0.0, 0.0),
-                     hydrostatic: bool = False, solid_gap: float = 0.0) -> Scenario:
+                     hydrostatic: bool = False, solid_gap: float = 0.0,
+                     geometry: str = "offset") -> Scenario:
     """A closed tank filled with water up to ``fill_height`` around a fixed
     sphere. Lattice points inside the solid (sphere SDF < 0) are skipped as
     ``place_fluid_particles`` does (domain.rs:127-130); the sphere becomes
@@ -314,7 +368,11 @@ def tank_with_sphere(dx: float, domain_max=(0.12, 0.08, 0.08), center=(0.06, 0.0
     SDF. ``velocity`` is an initial uniform fluid velocity. ``solid_gap``
     (in units of dx) also skips lattice points closer than that to the
     sphere: 0.5 gives the sphere the half-spacing gap the lattice keeps
-    from the flat walls.
+    from the flat walls. ``geometry`` "offset" builds the boundary particles
+    as the reference does; "lattice" puts the box walls and the sphere on the
+    fluid lattice's own sites (``lattice_box_walls``,
+    ``lattice_solid_particles``) and splits fluid from solid on the bare
+    lattice, before jitter and compression.
 
     ``hydrostatic`` starts the water at rest in its hydrostatic state. The
     particle (and wall) mass is rho0 dx^3 / S with S = sum W(|x_ijk|) dx^3
@@ -333,20 +391,35 @@ def tank_with_sphere(dx: float, domain_max=(0.12, 0.08, 0.08), center=(0.06, 0.0
     sph = sphere_sdf(dmin, dmax, sdf_cell, center, radius)
     parts = block_particles(dmin, counts, dx32, seed)
     c0 = dam_break_c0(fill)
+    top = counts[2] * float(dx32)
+    kz = 1000.0 * 9.81 / (7.0 * (1000.0 * c0 * c0 / 7.0))
+
+    def zmap(z):  # hydrostatic compression, a constant shift above the fill
+        z = np.minimum(z.astype(np.float64), top) + np.maximum(z.astype(np.float64) - top, 0.0)
+        zc = np.minimum(z, top)
+        return (z - kz * (top * zc - 0.5 * zc * zc)).astype(np.float32)
+
     if hydrostatic:
-        top = counts[2] * float(dx32)
-        b = 1000.0 * c0 * c0 / 7.0
-        z = parts.z.astype(np.float64)
-        parts.z[:] = (z - 1000.0 * 9.81 * (top * z - 0.5 * z * z) / (7.0 * b)).astype(np.float32)
+        parts.z[:] = zmap(parts.z)
     pts = np.stack([parts.x, parts.y, parts.z], axis=-1)
+    if geometry == "lattice":  # fluid and solid split on the bare lattice
+        bare = block_particles(dmin, counts, dx32, None)
+        pts = np.stack([bare.x, bare.y, bare.z], axis=-1)
     keep = sdf_sample(sph, pts) >= f32(solid_gap * float(dx32))
     m = particle_mass(dx32)
     if hydrostatic:
         m = f32(float(m) / lattice_kernel_sum(float(smoothing_length(dx32)), float(dx32)))
     p = ParticleArrays.from_positions(parts.x[keep], parts.y[keep], parts.z[keep], m)
     p.vx[:], p.vy[:], p.vz[:] = (f32(v) for v in velocity)
-    walls = wall_boundary_particles(dmin, dmax, dx32, m)
-    geo = geometry_boundary_particles(sph, dmin, dmax, dx32, m)
+    if geometry == "lattice":
+        walls = lattice_box_walls(dmin, dmax, dx32, m)
+        geo = lattice_solid_particles(sph, dmin, dmax, dx32, m)
+    else:
+        walls = wall_boundary_particles(dmin, dmax, dx32, m)
+        geo = geometry_boundary_particles(sph, dmin, dmax, dx32, m)
+    if hydrostatic and geometry == "lattice":  # keep fluid and wall on one lattice
+        walls.z[:] = zmap(walls.z)
+        geo.z[:] = zmap(geo.z)
     sdf = merge_sdf(box_sdf(dmin, dmax, sdf_cell), sph)
     return Scenario(f"tank_sphere_dx{dx*1e3:g}mm", p, concat_boundary(walls, geo), float(smoothing_length(dx32)),
                     (0.0, 0.0, -9.81), c0, 0.25, 0.0, dmin, dmax, alpha=alpha, sdf=sdf,
