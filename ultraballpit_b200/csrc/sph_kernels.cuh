@@ -277,13 +277,22 @@ __device__ __forceinline__ void for_each_neighbor(float px, float py, float pz, 
         if (ey + (dx < 0 ? lo2[0] : (dx > 0 ? hi2[0] : 0.0f)) > k.radius_sq) continue;
         uint2 se = __ldg(&ctab[k.coff + row + nx]);
         int end = (int)(se.x + se.y);
-        for (int s = (int)se.x; s < end; ++s) {
-          if (s == self) continue;
-          float4 pj = __ldg(&pos[s]);
+        int s = (int)se.x;
+        auto test = [&](int t, const float4& pj) {
+          if (t == self) return;
           float ddx = px - pj.x, ddy = py - pj.y, ddz = pz - pj.z;
           float d2 = ddx * ddx + ddy * ddy + ddz * ddz;
-          if (d2 <= k.radius_sq) f(s, pj, ddx, ddy, ddz, d2);
+          if (d2 <= k.radius_sq) f(t, pj, ddx, ddy, ddz, d2);
+        };
+        // four candidate loads in flight before the (in-order) tests
+        for (; s + 3 < end; s += 4) {
+          float4 q0 = __ldg(&pos[s]), q1 = __ldg(&pos[s + 1]), q2 = __ldg(&pos[s + 2]), q3 = __ldg(&pos[s + 3]);
+          test(s, q0);
+          test(s + 1, q1);
+          test(s + 2, q2);
+          test(s + 3, q3);
         }
+        for (; s < end; ++s) test(s, __ldg(&pos[s]));
       }
     }
   }
