@@ -36,7 +36,45 @@ WORKLOADS = {
     "dam_break_4mm": dict(dx=0.004, sphere=False),          # 31,250 particles
     "batch_boxes_2mm": dict(batch=256),                     # 256 instances, about 51M particles
     "batch_boxes_2mm_loguniform": dict(batch=256, draw="loguniform"),  # 256 instances, about 20M
+    # 64 sphere-in-tank flows at 4 mm with the learned closure (about 8.6M particles)
+    "batch_closure_4mm": dict(batch=64, closure=True),
 }
+CLOSURE_WEIGHTS = os.path.join(ROOT, "ultraballpit_b200", "data", "closure_weights.npy")
+
+
+def pair_stats(sc, sample: int = 20000, seed: int = 0) -> dict:
+    """Mean in-support neighbours (interactions) and mean 27-cell candidates
+    after the kernel's cell culling, per particle, on a seeded sample of the
+    initial state (2h grid cells, as the kernels bin)."""
+    from scipy.spatial import cKDTree
+    p = sc.particles
+    pos = np.stack([p.x, p.y, p.z], axis=1).astype(np.float64)
+    rng = np.random.default_rng(seed)
+    pick = rng.choice(len(pos), min(sample, len(pos)), replace=False)
+    r = 2.0 * sc.h
+    inter = cKDTree(pos).query_ball_point(pos[pick], r, return_length=True) - 1
+    gmin = np.asarray(sc.domain_min, np.float64)
+    cell = 2.0 * sc.h
+    dims = np.maximum(np.ceil((np.asarray(sc.domain_max) - gmin) / cell), 1).astype(np.int64)
+    c = np.clip(np.floor((pos - gmin) / cell).astype(np.int64), 0, dims - 1)
+    lin = (c[:, 2] * dims[1] + c[:, 1]) * dims[0] + c[:, 0]
+    counts = np.bincount(lin, minlength=int(np.prod(dims)))
+    cq, pq = c[pick], pos[pick]
+    face = gmin + cq * cell
+    lo2 = np.maximum(pq - face, 0.0) ** 2
+    hi2 = np.maximum(face + cell - pq, 0.0) ** 2
+    cand = np.zeros(len(pick))
+    for dz in (-1, 0, 1):
+        for dy in (-1, 0, 1):
+            for dx in (-1, 0, 1):
+                d = np.array([dx, dy, dz])
+                e = sum(np.where(d[a] < 0, lo2[:, a], np.where(d[a] > 0, hi2[:, a], 0.0)) for a in range(3))
+                nc = cq + d
+                ok = np.all((nc >= 0) & (nc < dims), axis=1) & (e <= r * r)
+                l2 = (nc[:, 2] * dims[1] + nc[:, 1]) * dims[0] + nc[:, 0]
+                cand += np.where(ok, counts[np.where(ok, l2, 0)], 0)
+    return {"interactions_per_particle": float(inter.mean()), "candidates_per_particle": float(cand.mean() - 1),
+            "sample": f"{len(pick)} particles of the initial state"}
 
 
 def roofline_bytes():
@@ -198,6 +236,79 @@ def run_batch_arm(args):
         print(json.dumps(line), flush=True)
 
 
+def run_batch_closure_arm(args):
+    """Batched sphere-in-tank flows with the closure fused into the step
+    against the same instances solved one after another without it."""
+    import torch
+    from ultraballpit_b200 import closure_batch as cb
+    from ultraballpit_b200.kernel import CudaBatch, CudaKernel
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    w = WORKLOADS[args.workload]
+    weights = np.load(CLOSURE_WEIGHTS).astype(np.float32)
+    inst = cb.draw_instances(w["batch"], args.seed + rank)
+    scs = cb.settle_batch([cb.build(q, cb.DX) for q in inst], device=local)
+    for sc, q in zip(scs, inst):
+        sc.particles.vx[:] = np.float32(q["speed"])
+    dts = np.array([cb.dt_of(sc) for sc in scs], np.float32)
+    ntot = sum(len(s.particles) for s in scs)
+    b = CudaBatch(scs, device=local)
+    b.set_feature_sdfs([sc.sdf for sc in scs])
+    b.set_closure(2, weights)
+    stream = torch.cuda.ExternalStream(b.stream())
+    for _ in range(args.warmup):
+        b.step_each(dts)
+    torch.cuda.synchronize()
+    l0 = b.launch_count()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        e0.record(stream)
+        for _ in range(args.steps):
+            b.step_each(dts)
+        e1.record(stream)
+        e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    launches = b.launch_count() - l0
+    b.health()
+    b.close()
+    del b
+    seq_ms = 0.0
+    for sc, dt in zip(scs, dts):
+        k = CudaKernel(*sc.kernel_args(), alpha=sc.alpha, device=local)
+        st = torch.cuda.ExternalStream(k.stream())
+        for _ in range(args.warmup):
+            k.step(float(dt))
+        a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a0.record(st)
+        for _ in range(args.steps):
+            k.step(float(dt))
+        a1.record(st)
+        a1.synchronize()
+        seq_ms += a0.elapsed_time(a1)
+        k.close()
+    value = ntot * args.steps / (ms / 1e3)
+    seq_value = ntot * args.steps / (seq_ms / 1e3)
+    counts = [len(s.particles) for s in scs]
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32 (closure network bf16 operands, f32 accumulation)",
+        "data": "synthetic (seeded sphere-in-tank flows, host-built, relaxed on the device)",
+        "config": {"workload": args.workload, "instances": len(scs), "particles": ntot,
+                   "boundary_particles": sum(len(s.boundary) for s in scs),
+                   "instance_particles_min_max": [min(counts), max(counts)],
+                   "size_histogram_log2": np.bincount(np.log2(counts).astype(int)).tolist(),
+                   "dt": "per instance, dt c0 / h = %.4f" % cb.DT_C_OVER_H, "closure": "mode 2, shipped weights",
+                   "l2": "inputs larger than L2"},
+        "sequential_plain": {"value": seq_value, "unit": UNIT, "ms_per_step": seq_ms / args.steps,
+                             "how": "each instance alone through sph_create, closure off, graph-captured"},
+        "batched_closure_over_sequential_plain": value / seq_value,
+        "clocks": clk.summary(), "gpu_launches": launches,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def run_reference_arm(args):
     rank, world, _ = dist_env()
     if rank != 0:
@@ -294,6 +405,12 @@ def run_cuda_arm(args):
                 "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
                 "peak_source": peak_kind, "stage_us": {s.replace("_us", ""): round(avg[s], 2) for s in stage_keys},
                 "algorithmic_bytes_per_launch": bytes_of[dom]}
+    ps = pair_stats(sc)
+    roofline["pairs"] = dict(ps, **{
+        "density_candidate_tests_per_s": n * ps["candidates_per_particle"] / (avg["density_us"] * 1e-6),
+        "density_interactions_per_s": n * ps["interactions_per_particle"] / (avg["density_us"] * 1e-6),
+        "forces_interactions_per_s": n * ps["interactions_per_particle"] / (avg["forces_us"] * 1e-6),
+        "xsph_interactions_per_s": n * ps["interactions_per_particle"] / (avg["xsph_drift_us"] * 1e-6)})
     k.close()
     del k
 
@@ -361,6 +478,8 @@ def main():
         args.warmup = 3
     if args.impl == "reference":
         run_reference_arm(args)
+    elif WORKLOADS[args.workload].get("closure"):
+        run_batch_closure_arm(args)
     elif "batch" in WORKLOADS[args.workload]:
         run_batch_arm(args)
     else:

@@ -244,6 +244,8 @@ int sph_batch_create_sdf(int ninst, const SphParams *params, const SphParticlesV
 /* Instance count, and per instance the first particle and particle count in
  * the concatenated order (first/count may be NULL, else ninst entries). */
 int sph_batch_info(const SphHandle *h, int *ninst, size_t *first, size_t *count);
+/* One step with instance q advanced by dts[q] (ninst floats, host). */
+int sph_batch_step(SphHandle *h, const float *dts);
 /* Per-instance sph::compute_timestep on the device (ninst floats). */
 int sph_batch_timesteps(SphHandle *h, float *dt_out);
 /* Launch shapes of the neighbour kernels (graphs are recaptured). */
@@ -295,8 +297,8 @@ int sph_batch_set_feature_sdfs(SphHandle *h, const SphSdfView *sdfs);
  *   10 n.g/|g|, 11 (d/h)^2, 12 f8 f0, 13 f10 f0,
  *   14 boundary particles in support / 30, 15 1. */
 #define SPH_CLOSURE_DRHO_UNIT 1e-4f /* y0 in units of 0.01 % of rho0 */
-#define SPH_CLOSURE_MAX_DRHO 300.0f  /* 3 % of rho0 */
-#define SPH_CLOSURE_MAX_ACC_G 25.0f
+#define SPH_CLOSURE_MAX_DRHO 30.0f   /* 0.3 % of rho0 */
+#define SPH_CLOSURE_MAX_ACC_G 2.5f
 int sph_set_closure(SphHandle *h, int mode, const float *params);
 /* Samples of the last density pass: original particle ids, 16 features each
  * (row-major), density before correction; *count gets the total. */

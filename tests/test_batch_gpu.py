@@ -70,3 +70,28 @@ def test_batch_sdf_mode_matches_single_runs():
         k.step_auto(10, want_dt=False)
     for q, k in enumerate(singles):
         _same(batch.instance(q), k.particles())
+
+
+def test_batch_closure_with_per_instance_dt_matches_single_runs():
+    """Closure mode 2 on a batch stepped with one dt per instance
+    (sph_batch_step) == each instance alone with its own dt, bit for bit."""
+    from ultraballpit_b200 import closure
+    scs = [closure.tank_pair(s)[0] for s in (3, 4)]
+    w = closure.ClosureNet(seed=9).params()
+    dts = np.array([5e-5, 4e-5], np.float32)
+    b = CudaBatch(scs)
+    b.set_feature_sdfs([sc.sdf for sc in scs])
+    b.set_closure(2, w)
+    for _ in range(5):
+        b.step_each(dts)
+    for q, sc in enumerate(scs):
+        k = CudaKernel(*sc.kernel_args(), alpha=sc.alpha)
+        k.set_feature_sdf(sc.sdf)
+        k.set_closure(2, w)
+        for _ in range(5):
+            k.step(float(dts[q]))
+        got, ref = b.instance(q), k.particles()
+        for f in ("x", "y", "z", "vx", "vy", "vz", "ax", "ay", "az", "density", "pressure"):
+            np.testing.assert_array_equal(getattr(got, f), getattr(ref, f), err_msg=f"instance {q} {f}")
+        k.close()
+    b.close()

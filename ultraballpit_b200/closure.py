@@ -217,10 +217,12 @@ def run_pair(seed: int, t_snap=(0.02, 0.03, 0.04, 0.05), dt_coarse: float = 5e-5
     return np.concatenate(X), np.concatenate(T)
 
 
-def generate(seeds, **kw):
+def generate(seeds, moving=False, **kw):
+    """Samples of ``run_pair`` over ``seeds``; ``moving`` is a bool or a
+    function of the seed (True: the tank starts at the seed's speed)."""
     xs, ts, owners = [], [], []
     for s in seeds:
-        x, t = run_pair(s, **kw)
+        x, t = run_pair(s, moving=bool(moving(s) if callable(moving) else moving), **kw)
         xs.append(x)
         ts.append(t)
         owners.append(np.full(len(x), s))
@@ -229,7 +231,7 @@ def generate(seeds, **kw):
 
 # Output units and clamps of the step: y0 in SPH_CLOSURE_DRHO_UNIT rho0
 # (clamped to SPH_CLOSURE_MAX_DRHO), y1..3 in |g| (SPH_CLOSURE_MAX_ACC_G).
-DRHO_UNIT, CLAMP_DRHO, CLAMP_ACC_G = 1e-4, 300.0, 25.0
+DRHO_UNIT, CLAMP_DRHO, CLAMP_ACC_G = 1e-4, 30.0, 2.5
 
 
 def to_units(raw, c: float) -> np.ndarray:
@@ -341,20 +343,28 @@ def run_probes(sc, probes, steps: int, dt: float, every: int, start: int, mode: 
 
 def compare(seed: int, params=None, steps: int = 800, dt: float = 5e-5, every: int = 20, start: int | None = None,
             dx_coarse: float = 0.004, device: int = 0, settle_s: float = SETTLE_S, moving: bool = False) -> dict:
+    """``compare_scenarios`` on the settled tank pair of ``seed``."""
+    coarse, fine, geo = settled_pair(seed, dx_coarse, dt, settle_s, device, moving)
+    out = compare_scenarios(coarse, fine, geo, params, steps, dt, every, start, device)
+    out["seed"] = seed
+    return out
+
+
+def compare_scenarios(coarse, fine, geo, params=None, steps: int = 800, dt: float = 5e-5, every: int = 20,
+                      start: int | None = None, device: int = 0, fill: float = FILL, tank=TANK) -> dict:
     """The fine tank (dx / 2, dt / 2) judges the coarse tank without
     (``plain``) and, when ``params`` is given, with the closure
     (``closure``): near-wall pressure error = mean |p_c - p_f| / mean |p_f|
     over the probes on the sphere and on the walls, each pressure averaged
     over the snapshots of the second half of the run; force error =
-    |F_c - F_f| / |F_f| for the time-averaged pressure force on the sphere;
+    |F_c - F_f| / |F_f| for the time-averaged force on the sphere;
     ``speedup`` = fine stepping time / coarse stepping time."""
     start = steps // 2 if start is None else start
-    coarse, fine, geo = settled_pair(seed, dx_coarse, dt, settle_s, device, moving)
-    sph, walls = probe_points(geo, coarse.h)
+    sph, walls = probe_points(geo, coarse.h, fill=fill, tank=tank)
     probes = np.concatenate([sph, walls])
     ns = len(sph)
     pf, nf, ff, tf = run_probes(fine, probes, steps, dt, every, start, device=device, substeps=2)
-    out = dict(seed=seed, geo=geo, fine_seconds=tf, fine_force=ff, probes=(ns, len(walls)))
+    out = dict(geo=geo, fine_seconds=tf, fine_force=ff, probes=(ns, len(walls)))
     runs = [("plain", 1, None)] + ([("closure", 2, params)] if params is not None else [])
     for name, mode, prm in runs:
         pc, nc, fc, tc = run_probes(coarse, probes, steps, dt, every, start, mode=mode, params=prm, device=device)

@@ -864,12 +864,9 @@ void sph_destroy(SphHandle* h) {
   delete h;
 }
 
-int sph_step(SphHandle* h, float dt) {
-  if (!h) return SPH_ERR_INVALID_ARG;
-  if (!std::isfinite(dt)) return set_err(h, SPH_ERR_INVALID_ARG, "dt must be finite");
-  SPH_TRY(h, cudaSetDevice(h->dev));
-  if (h->n == 0) return SPH_OK;
-  enqueue_set_dt(h, dt);
+namespace {
+// sph_step after the step's dt is in device memory
+int step_enqueued_dt(SphHandle* h) {
   if (h->needs_init) {
     enqueue_bootstrap(h);
     h->needs_init = false;
@@ -889,6 +886,26 @@ int sph_step(SphHandle* h, float dt) {
   h->list_valid = true;
   h->red_valid = true;
   return cuda_status(h, cudaGetLastError(), "sph_step");
+}
+}  // namespace
+
+int sph_step(SphHandle* h, float dt) {
+  if (!h) return SPH_ERR_INVALID_ARG;
+  if (!std::isfinite(dt)) return set_err(h, SPH_ERR_INVALID_ARG, "dt must be finite");
+  SPH_TRY(h, cudaSetDevice(h->dev));
+  if (h->n == 0) return SPH_OK;
+  enqueue_set_dt(h, dt);
+  return step_enqueued_dt(h);
+}
+
+int sph_batch_step(SphHandle* h, const float* dts) {
+  if (!h || !dts) return SPH_ERR_INVALID_ARG;
+  for (int q = 0; q < h->ninst; ++q)
+    if (!std::isfinite(dts[q])) return set_err(h, SPH_ERR_INVALID_ARG, "dt must be finite");
+  SPH_TRY(h, cudaSetDevice(h->dev));
+  if (h->n == 0) return SPH_OK;
+  SPH_TRY(h, cudaMemcpyAsync(h->dt, dts, sizeof(float) * h->ninst, cudaMemcpyHostToDevice, h->st));
+  return step_enqueued_dt(h);
 }
 
 int sph_step_auto(SphHandle* h, int nsteps, float* dt_out) {

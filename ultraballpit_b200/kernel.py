@@ -44,7 +44,7 @@ EXPORTS = (
     "sph_get_launch", "sph_autotune", "sph_mlp_create", "sph_mlp_destroy", "sph_mlp_set_params",
     "sph_mlp_get_params", "sph_mlp_forward", "sph_mlp_loss_grad", "sph_mlp_train",
     "sph_set_feature_sdf", "sph_batch_set_feature_sdfs", "sph_set_closure", "sph_closure_samples",
-    "sph_interpolate", "sph_batch_create_sdf",
+    "sph_interpolate", "sph_batch_create_sdf", "sph_batch_step",
 )
 
 
@@ -150,6 +150,8 @@ def load_library(path: str | None = None):
     L.sph_particle_count.restype = C.c_size_t
     L.sph_save_checkpoint.argtypes = [H]
     L.sph_restore_checkpoint.argtypes = [H]
+    L.sph_batch_step.argtypes = [H, _FP]
+    L.sph_batch_step.restype = C.c_int
     L.sph_scale_velocities.argtypes = [H, C.c_float]
     L.sph_scale_velocities.restype = C.c_int
     L.sph_synchronize.argtypes = [H]
@@ -565,6 +567,14 @@ class CudaBatch(CudaKernel):
         keep = []
         arr = (SphSdfView * len(sdfs))(*[self._sdf_view(sd, keep) for sd in sdfs])
         self._check(self._lib.sph_batch_set_feature_sdfs(self._h, arr), "sph_batch_set_feature_sdfs")
+
+    def step_each(self, dts) -> None:
+        """One step with instance q advanced by dts[q]."""
+        d = np.ascontiguousarray(dts, np.float32)
+        if d.shape != (self.ninst,):
+            raise ValueError("one dt per instance")
+        self._check(self._lib.sph_batch_step(self._h, _fp(d)), "sph_batch_step")
+        self._cache = None
 
     def timesteps(self) -> np.ndarray:
         out = np.zeros(self.ninst, np.float32)
