@@ -3,7 +3,8 @@ simulations in one launch per stage, closure inference fused into the step).
 
     python -m ultraballpit_b200.closure_batch --weights W.npy --instances 64 --steps 1000 --compare 4 --out DIR
 
-1. ``draw_instances``: closed tanks with seeded dims in [0.1, 0.4] m, a fill
+1. ``draw_instances``: closed tanks with seeded dims in [0.1, 0.4] m (whole
+   4 mm spacings), a fill
    giving a log-uniform 4 mm particle count in [50k, 1M], a sphere of radius
    U[0.01, 0.04] m at a seeded submerged position and a start speed
    U[0, 0.5] m/s along +x; fluid, walls and sphere on one lattice with the
@@ -46,7 +47,9 @@ def draw_instances(n: int, seed: int, counts=(50_000, 1_000_000), dx: float = DX
     rng = np.random.default_rng(seed)
     out = []
     while len(out) < n:
-        dims = tuple(float(v) for v in rng.uniform(0.1, 0.4, 3))
+        # whole spacings (at dx and dx / 2), so the lattice meets every wall
+        # half a spacing from it
+        dims = tuple(round(float(v) / dx) * dx for v in rng.uniform(0.1, 0.4, 3))
         target = math.exp(rng.uniform(math.log(counts[0]), math.log(counts[1])))
         fill = round(target * dx ** 3 / (dims[0] * dims[1]) / dx) * dx
         r = float(rng.uniform(0.01, 0.04))
