@@ -314,12 +314,22 @@ __device__ __forceinline__ void visit_neighbors(int i, int n, float px, float py
                                                 const SimConst& k, F&& f) {
   uint32_t cnt = nbr ? __ldg(&ncount[i]) : 0xffffffffu;
   if (cnt <= kNbrCap) {
-    for (uint32_t c = 0; c < cnt; ++c) {
+    // two neighbours per iteration: both list entries and both positions are
+    // loaded before either is used (same order of f calls)
+    uint32_t c = 0;
+    for (; c + 1 < cnt; c += 2) {
+      int s0 = (int)__ldg(&nbr[(size_t)c * n + i]), s1 = (int)__ldg(&nbr[(size_t)(c + 1) * n + i]);
+      float4 p0 = __ldg(&pos[s0]), p1 = __ldg(&pos[s1]);
+      float ax = px - p0.x, ay = py - p0.y, az = pz - p0.z;
+      f(s0, p0, ax, ay, az, ax * ax + ay * ay + az * az);
+      float bx = px - p1.x, by = py - p1.y, bz = pz - p1.z;
+      f(s1, p1, bx, by, bz, bx * bx + by * by + bz * bz);
+    }
+    if (c < cnt) {
       int s = (int)__ldg(&nbr[(size_t)c * n + i]);
       float4 pj = __ldg(&pos[s]);
       float ddx = px - pj.x, ddy = py - pj.y, ddz = pz - pj.z;
-      float d2 = ddx * ddx + ddy * ddy + ddz * ddz;
-      f(s, pj, ddx, ddy, ddz, d2);
+      f(s, pj, ddx, ddy, ddz, ddx * ddx + ddy * ddy + ddz * ddz);
     }
   } else {
     for_each_neighbor(px, py, pz, i, pos, ctab, k, f);
@@ -613,7 +623,16 @@ k_density(KP kp, int n, const float* __restrict__ dtp, const float4* __restrict_
     if (CL) ssum += __ldg(&rv[s]).y * w;
   };
   if (listed <= kNbrCap) {
-    for (uint32_t c = 0; c < listed; ++c) {
+    uint32_t c = 0;
+    for (; c + 1 < listed; c += 2) {
+      int s0 = (int)nbr[(size_t)c * n + i], s1 = (int)nbr[(size_t)(c + 1) * n + i];
+      float4 p0 = __ldg(&pos[s0]), p1 = __ldg(&pos[s1]);
+      float ax = pi.x - p0.x, ay = pi.y - p0.y, az = pi.z - p0.z;
+      term(s0, p0, ax, ay, az, ax * ax + ay * ay + az * az);
+      float bx = pi.x - p1.x, by = pi.y - p1.y, bz = pi.z - p1.z;
+      term(s1, p1, bx, by, bz, bx * bx + by * by + bz * bz);
+    }
+    if (c < listed) {
       int s = (int)nbr[(size_t)c * n + i];
       float4 pj = __ldg(&pos[s]);
       float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
