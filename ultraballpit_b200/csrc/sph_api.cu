@@ -76,6 +76,8 @@ struct SphHandle {
   int nbsum = 0;
   // neighbour lists recorded by k_density: nbr[c * n + i], count per particle
   uint32_t *nbr = nullptr, *ncount = nullptr;
+  // XSPH gather records: (x, y, z, m), (v + a dt/2, rho) per particle
+  float4* xrec = nullptr;
   // boundary
   float4* bpos = nullptr;
   float* bpress = nullptr;
@@ -430,12 +432,14 @@ void enqueue_xsph(SphHandle* h, bool use_list) {
   using namespace sph;
   int bs = h->bs_xsph;
   dispatch(h, false, [&](auto kp) {
-    k_xsph_drift<<<grid_for(h->n, bs), bs, 0, h->st>>>(kp, h->n, h->dt, h->pos, h->velout, h->acc, h->id,
+    k_xsph_prep<<<grid_for(h->n, 256), 256, 0, h->st>>>(kp, h->n, h->dt, h->pos, h->velout, h->acc, h->xrec,
+                                                         h->err);
+    k_xsph_drift<<<grid_for(h->n, bs), bs, 0, h->st>>>(kp, h->n, h->dt, h->pos, h->velout, h->acc, h->xrec, h->id,
                                                        h->ctab, h->rank_of_lin, h->posU, h->velU, h->idU,
                                                        h->keyU, h->hist, h->err,
                                                        use_list ? h->nbr : nullptr, h->ncount);
   });
-  h->launches += 1;
+  h->launches += 2;
 }
 
 void enqueue_sort(SphHandle* h) {
@@ -717,7 +721,7 @@ int create_impl(int ninst, const SphParams* PP, const SphParticlesView* pvs,
   ALLOC(part_m, h->nparts); ALLOC(part_e, h->nparts); ALLOC(part_var, h->nparts); ALLOC(me, 2);
   ALLOC(var, 1); ALLOC(bad, 1);
   ALLOC(stage, 12 * n); ALLOC(stage_ft, n); ALLOC(diag, 2);
-  ALLOC(nbr, (size_t)sph::kNbrCap * n); ALLOC(ncount, n);
+  ALLOC(nbr, (size_t)sph::kNbrCap * n); ALLOC(ncount, n); ALLOC(xrec, 2 * n);
   if (ninst > 1) {
     ALLOC(ktab, ninst); ALLOC(inst_p, n); ALLOC(inst_b, nb);
   }

@@ -344,6 +344,25 @@ __global__ void k_set_dt(float* dt, int ninst, float value) {
   for (int q = threadIdx.x; q < ninst; q += blockDim.x) dt[q] = value;
 }
 
+// Gather records of k_xsph_drift, one 32-byte pair per particle:
+// rec[2i] = (x, y, z, m), rec[2i+1] = (v + a dt/2, rho), the half-kicked
+// velocity computed as the reference's kick 1 does (lib.rs:301-305). The
+// XSPH sum then gathers one sector per neighbour instead of three (it is
+// bound by L1 throughput; the other neighbour passes are latency-bound and
+// gain nothing from records).
+template <class KP>
+__global__ void __launch_bounds__(256)
+k_xsph_prep(KP kp, int n, const float* __restrict__ dtp, const float4* __restrict__ pos,
+            const float4* __restrict__ velout, const float4* __restrict__ acc, float4* __restrict__ rec,
+            const uint32_t* __restrict__ err) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n || *err) return;
+  float hdt = 0.5f * dtp[kp.at(i).inst];
+  float4 v = velout[i], a = acc[i];
+  rec[2 * i] = pos[i];
+  rec[2 * i + 1] = make_float4(v.x + a.x * hdt, v.y + a.y * hdt, v.z + a.z * hdt, v.w);
+}
+
 // Kick 1 (lib.rs:301-305) + XSPH (sph.rs:236-280) + drift (lib.rs:313-317)
 // + domain clamp (boundary.rs:239-291) + binning of the new position
 // (neighbor.rs:89-101) into a rank-indexed histogram. Reads the sorted state,
@@ -351,7 +370,7 @@ __global__ void k_set_dt(float* dt, int ninst, float value) {
 template <class KP>
 __global__ void __maxnreg__(40)
 k_xsph_drift(KP kp, int n, const float* __restrict__ dtp, const float4* __restrict__ pos,
-             const float4* __restrict__ velout, const float4* __restrict__ acc,
+             const float4* __restrict__ velout, const float4* __restrict__ acc, const float4* __restrict__ rec,
              const uint32_t* __restrict__ id, const uint2* __restrict__ ctab,
              const uint32_t* __restrict__ rank_of_lin, float4* __restrict__ posU,
              float4* __restrict__ velU, uint32_t* __restrict__ idU, uint32_t* __restrict__ keyU,
@@ -371,21 +390,41 @@ k_xsph_drift(KP kp, int n, const float* __restrict__ dtp, const float4* __restri
   float sx = 0.0f, sy = 0.0f, sz = 0.0f;
   if (k.flags & kFlagXsph) {
     float rho_i = vi.w;
-    visit_neighbors(i, n, pi.x, pi.y, pi.z, pos, ctab, nbr, ncount, k,
-                      [&](int s, const float4& pj, float dx, float dy, float dz, float d2) {
-                        float r = sqrtf(d2);
-                        float w = w_c2(r, k);
-                        float4 vj = __ldg(&velout[s]);
-                        float4 aj = __ldg(&acc[s]);
-                        float vjx = vj.x + aj.x * hdt;
-                        float vjy = vj.y + aj.y * hdt;
-                        float vjz = vj.z + aj.z * hdt;
-                        float rho_avg = 0.5f * (rho_i + vj.w);
-                        float factor = pj.w / fmaxf(rho_avg, 1.0f) * w;
-                        sx += factor * (vjx - vx);
-                        sy += factor * (vjy - vy);
-                        sz += factor * (vjz - vz);
-                      });
+    // vh = the neighbour's half-kicked velocity and density (k_xsph_prep)
+    auto term = [&](const float4& pj, const float4& vh, float dx, float dy, float dz, float d2) {
+      float r = sqrtf(d2);
+      float w = w_c2(r, k);
+      float rho_avg = 0.5f * (rho_i + vh.w);
+      float factor = pj.w / fmaxf(rho_avg, 1.0f) * w;
+      sx += factor * (vh.x - vx);
+      sy += factor * (vh.y - vy);
+      sz += factor * (vh.z - vz);
+    };
+    uint32_t cnt = nbr ? __ldg(&ncount[i]) : 0xffffffffu;
+    if (cnt <= kNbrCap) {
+      // one 32-byte record per neighbour, two neighbours in flight
+      uint32_t c = 0;
+      for (; c + 1 < cnt; c += 2) {
+        int s0 = (int)__ldg(&nbr[(size_t)c * n + i]), s1 = (int)__ldg(&nbr[(size_t)(c + 1) * n + i]);
+        float4 p0 = __ldg(&rec[2 * s0]), h0 = __ldg(&rec[2 * s0 + 1]);
+        float4 p1 = __ldg(&rec[2 * s1]), h1 = __ldg(&rec[2 * s1 + 1]);
+        float ax = pi.x - p0.x, ay = pi.y - p0.y, az = pi.z - p0.z;
+        term(p0, h0, ax, ay, az, ax * ax + ay * ay + az * az);
+        float bx = pi.x - p1.x, by = pi.y - p1.y, bz = pi.z - p1.z;
+        term(p1, h1, bx, by, bz, bx * bx + by * by + bz * bz);
+      }
+      if (c < cnt) {
+        int s = (int)__ldg(&nbr[(size_t)c * n + i]);
+        float4 pj = __ldg(&rec[2 * s]), vh = __ldg(&rec[2 * s + 1]);
+        float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
+        term(pj, vh, dx, dy, dz, dx * dx + dy * dy + dz * dz);
+      }
+    } else {
+      for_each_neighbor(pi.x, pi.y, pi.z, i, pos, ctab, k,
+                        [&](int s, const float4& pj, float dx, float dy, float dz, float d2) {
+                          term(pj, __ldg(&rec[2 * s + 1]), dx, dy, dz, d2);
+                        });
+    }
   }
   float dvx = 0.5f * sx, dvy = 0.5f * sy, dvz = 0.5f * sz;
   float x = pi.x + (vx + dvx) * dt;
