@@ -13,8 +13,8 @@
  *       fn restore_checkpoint(&mut self) -> bool;
  *   }
  *
- * A Rust `CudaKernel` implements that trait over an opaque SphHandle (the
- * binding is written out in INTEGRATION.md). Every entry point returns an
+ * A Rust `CudaKernel` implements that trait over an opaque SphHandle through
+ * a thin FFI module declaring these functions. Every entry point returns an
  * SphStatus (0 = ok) and never aborts; the handle is Send but not Sync:
  * calls on one handle must not overlap, and each call makes the handle's
  * device current, so the handle may move between host threads.

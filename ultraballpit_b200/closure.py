@@ -352,7 +352,7 @@ def compare(seed: int, params=None, steps: int = 800, dt: float = 5e-5, every: i
 
 def compare_scenarios(coarse, fine, geo, params=None, steps: int = 800, dt: float = 5e-5, every: int = 20,
                       start: int | None = None, device: int = 0, fill: float = FILL, tank=TANK) -> dict:
-    """The fine tank (dx / 2, dt / 2) judges the coarse tank without
+    """The fine tank (dx / 2, dt / 2) is the reference for the coarse tank without
     (``plain``) and, when ``params`` is given, with the closure
     (``closure``): near-wall pressure error = mean |p_c - p_f| / mean |p_f|
     over the probes on the sphere and on the walls, each pressure averaged

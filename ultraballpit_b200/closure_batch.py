@@ -18,7 +18,7 @@ simulations in one launch per stage, closure inference fused into the step).
    without it, and the instances one after another without it.
 4. For ``--compare`` instances (drawn among those with at most
    ``--compare-max`` particles, which bounds the 2 mm runs' cost): the
-   2 mm plain run (dt / 2) judges the 4 mm run without and with the closure
+   2 mm plain run (dt / 2) is the reference for the 4 mm run without and with the closure
    (``closure.compare_scenarios``: time-averaged near-wall probe pressure
    and the force on the sphere); GPU time of the 2 mm run against the
    instance's share of the batched closure run.
