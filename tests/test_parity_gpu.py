@@ -296,3 +296,22 @@ def test_surface_and_body_forces_on_sphere():
     gb, cb = gpu.body_force(first, nb_geo), cpu.body_force(first, nb_geo)
     for key in gb:
         np.testing.assert_allclose(gb[key], cb[key], rtol=1e-9, atol=1e-15, err_msg=key)
+
+
+def test_scale_velocities_scales_the_state_the_next_step_starts_from():
+    sc = domain.dam_break(0.004, seed=7, block=(0.04, 0.04, 0.04), domain_max=(0.08, 0.04, 0.04), with_sdf=False)
+    k = CudaKernel(*sc.kernel_args(), alpha=sc.alpha)
+    for _ in range(5):
+        k.step(k.compute_timestep())
+    p0 = k.particles()
+    k.scale_velocities(2.0)
+    p1 = k.particles()
+    for f in ("vx", "vy", "vz"):
+        np.testing.assert_array_equal(getattr(p1, f), getattr(p0, f) * np.float32(2.0))
+    np.testing.assert_array_equal(p1.x, p0.x)
+    k.scale_velocities(0.0)
+    p2 = k.particles()
+    assert not np.any(p2.vx) and not np.any(p2.vy) and not np.any(p2.vz)
+    k.step(k.compute_timestep())
+    assert k.health() == 0
+    k.close()

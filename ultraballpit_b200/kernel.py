@@ -394,6 +394,7 @@ class CudaKernel(SimulationKernel):
         """velocity *= factor for every particle; 0 between steps is kinetic
         damping (relaxing an initial lattice before a run)."""
         self._check(self._lib.sph_scale_velocities(self._h, float(factor)), "sph_scale_velocities")
+        self._cache = None
 
     def synchronize(self) -> None:
         self._check(self._lib.sph_synchronize(self._h), "sph_synchronize")
