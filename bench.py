@@ -176,8 +176,10 @@ def run_batch_arm(args):
     import torch
     from ultraballpit_b200 import domain
     from ultraballpit_b200.kernel import CudaBatch, CudaKernel
+    from ultraballpit_b200.replicas import Replicas
     rank, world, local = dist_env()
     torch.cuda.set_device(local)
+    rep = Replicas("nccl")
     w = WORKLOADS[args.workload]
     scs = domain.batch_boxes(w["batch"], seed=args.seed + rank, draw=w.get("draw", "stated"))
     ntot = sum(len(s.particles) for s in scs)
@@ -214,8 +216,9 @@ def run_batch_arm(args):
         a1.synchronize()
         seq_ms += a0.elapsed_time(a1)
         k.close()
-    value = ntot * args.steps / (ms / 1e3)
-    seq_value = ntot * args.steps / (seq_ms / 1e3)
+    value, ms = rep.whole_job_rate(ntot, args.steps, ms)
+    seq_value, seq_ms = rep.whole_job_rate(ntot, args.steps, seq_ms)
+    rep.close()
     counts = [len(s.particles) for s in scs]
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -242,8 +245,10 @@ def run_batch_closure_arm(args):
     import torch
     from ultraballpit_b200 import closure_batch as cb
     from ultraballpit_b200.kernel import CudaBatch, CudaKernel
+    from ultraballpit_b200.replicas import Replicas
     rank, world, local = dist_env()
     torch.cuda.set_device(local)
+    rep = Replicas("nccl")
     w = WORKLOADS[args.workload]
     weights = np.load(CLOSURE_WEIGHTS).astype(np.float32)
     inst = cb.draw_instances(w["batch"], args.seed + rank)
@@ -286,8 +291,9 @@ def run_batch_closure_arm(args):
         a1.synchronize()
         seq_ms += a0.elapsed_time(a1)
         k.close()
-    value = ntot * args.steps / (ms / 1e3)
-    seq_value = ntot * args.steps / (seq_ms / 1e3)
+    value, ms = rep.whole_job_rate(ntot, args.steps, ms)
+    seq_value, seq_ms = rep.whole_job_rate(ntot, args.steps, seq_ms)
+    rep.close()
     counts = [len(s.particles) for s in scs]
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -332,27 +338,15 @@ def run_reference_arm(args):
 
 def run_cuda_arm(args):
     import torch
+    from ultraballpit_b200.replicas import Replicas
     rank, world, local = dist_env()
     torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import torch.distributed as dist
-        from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=300),
-                                device_id=torch.device("cuda", local))
+    rep = Replicas("nccl")
     from ultraballpit_b200.kernel import CudaKernel
 
     def barrier():
-        if dist is not None:
-            dist.barrier()
+        rep.barrier()
         torch.cuda.synchronize()
-
-    def max_over_ranks(x: float) -> float:
-        if dist is None:
-            return x
-        t = torch.tensor([x], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
 
     sc = build_scenario(args.workload, seed=args.seed + rank)
     n = len(sc.particles)
@@ -373,8 +367,7 @@ def run_cuda_arm(args):
         e1.synchronize()
     launches = k.launch_count() - l0
     barrier()
-    ms = max_over_ranks(e0.elapsed_time(e1))
-    value = n * args.steps * world / (ms / 1e3)
+    value, ms = rep.whole_job_rate(n, args.steps, e0.elapsed_time(e1))
 
     # ---- per-kernel durations (profiled steps, events between stages) -----
     prof_steps = max(3, min(args.steps // 4, 50))
@@ -424,12 +417,13 @@ def run_cuda_arm(args):
         k2.error_metrics()
     final = k2.particles()
     torch.cuda.synchronize()
-    e2e_s = max_over_ranks(time.perf_counter() - t0)
+    e2e_s = rep.max(time.perf_counter() - t0)
+    n_all = rep.sum(n)
     assert len(final) == n
     k2.close()
     h2d_init = n * (13 * 4 + 1) + len(sc.boundary) * 7 * 4
     d2h_final = n * (13 * 4 + 1)
-    e2e = {"value": n * args.steps * world / e2e_s, "unit": UNIT,
+    e2e = {"value": n_all * args.steps / e2e_s, "unit": UNIT,
            "h2d_bytes_per_step": h2d_init / args.steps + 4,
            "d2h_bytes_per_step": d2h_final / args.steps + 4 + 12 + 4,
            "includes": "handle creation from host arrays, per step compute_timestep + step + "
@@ -443,9 +437,8 @@ def run_cuda_arm(args):
                "sample": f"{done} full steps of {args.workload} ({n} particles) on {threads} host threads, "
                          f"oracle tier G ({el:.1f} s)"}
 
-    if dist is not None:
-        dist.barrier()
-        dist.destroy_process_group()
+    rep.barrier()
+    rep.close()
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
