@@ -51,7 +51,8 @@ typedef enum SphStatus {
 
 typedef enum SphBoundaryMode {
   SPH_BOUNDARY_PARTICLES = 0, /* reference walls: frozen particles, Adami pressure */
-  SPH_BOUNDARY_SDF = 1        /* wall force from a trilinear SDF (no reference counterpart) */
+  SPH_BOUNDARY_SDF = 1        /* homogenised walls: the six faces of the domain box and an
+                                 obstacle given by a trilinear SDF (no reference counterpart) */
 } SphBoundaryMode;
 
 typedef enum SphCellOrder {
@@ -180,8 +181,10 @@ typedef struct SphGridInfo {
 void sph_params_default(SphParams *p);
 
 /* CpuKernel::new / GpuKernel::new (lib.rs:138-174, gpu/mod.rs:190-200).
- * `boundary` may be NULL (no walls); `sdf` is required for SPH_BOUNDARY_SDF
- * and ignored otherwise. */
+ * `boundary` may be NULL (no walls). With SPH_BOUNDARY_SDF the walls are
+ * the faces of the domain box (which must span at least 4h on every axis)
+ * plus the obstacle whose SDF `sdf` gives (NULL, or NULL distances: no
+ * obstacle); otherwise `sdf` is ignored. */
 int sph_create(const SphParams *params, const SphParticlesView *particles,
                const SphBoundaryView *boundary, const SphSdfView *sdf, SphHandle **out);
 void sph_destroy(SphHandle *h);
@@ -237,8 +240,9 @@ uint64_t sph_launch_count(const SphHandle *h);
  * sums over all instances. */
 int sph_batch_create(int ninst, const SphParams *params, const SphParticlesView *particles,
                      const SphBoundaryView *boundaries, SphHandle **out);
-/* A batch in SDF wall mode: one SDF per instance (all instances with the
- * same h, which fixes the shared wall table). */
+/* A batch in SDF wall mode: one obstacle SDF per instance (NULL distances:
+ * none; `sdfs` NULL: none anywhere), all instances with the same h, which
+ * fixes the shared wall table. */
 int sph_batch_create_sdf(int ninst, const SphParams *params, const SphParticlesView *particles,
                          const SphSdfView *sdfs, SphHandle **out);
 /* Instance count, and per instance the first particle and particle count in

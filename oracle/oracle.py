@@ -89,6 +89,8 @@ def lib():
         L.orc_body_force.argtypes = [vp, C.c_uint32, C.c_uint32, C.POINTER(C.c_double)]
         L.orc_wall_table.restype = C.c_int
         L.orc_wall_table.argtypes = [C.c_float, fp, fp, fp]
+        L.orc_wall_tables_box.restype = C.c_int
+        L.orc_wall_tables_box.argtypes = [C.c_float, fp, fp, fp, fp, fp, fp]
         L.orc_sdf_sample_clamped.restype = C.c_float
         L.orc_sdf_sample_clamped.argtypes = [fp, u32p, fp, C.c_float, fp]
         L.orc_sdf_gradient_clamped.argtypes = [fp, u32p, fp, C.c_float, fp, fp]
@@ -186,6 +188,23 @@ def wall_table(h):
     return phi, grad, float(inv[0])
 
 
+WALL_N2, WALL_N3 = 64, 24
+
+
+def wall_tables_box(h):
+    """Edge tables (phi2, grad2)[(N2 + 1), (N2 + 1)] and corner tables
+    (phi3, grad3)[(N3 + 1),] * 3 of the SDF-mode box walls, with their
+    inverse steps."""
+    n2, n3 = WALL_N2 + 1, WALL_N3 + 1
+    phi2, grad2 = np.zeros(n2 * n2, np.float32), np.zeros(n2 * n2, np.float32)
+    phi3, grad3 = np.zeros(n3 ** 3, np.float32), np.zeros(n3 ** 3, np.float32)
+    inv = np.zeros(2, np.float32)
+    code = lib().orc_wall_tables_box(h, _fp(phi2), _fp(grad2), _fp(phi3), _fp(grad3), _fp(inv[:1]), _fp(inv[1:]))
+    assert code == WALL_N2 * 1000 + WALL_N3
+    return (phi2.reshape(n2, n2), grad2.reshape(n2, n2), phi3.reshape(n3, n3, n3), grad3.reshape(n3, n3, n3),
+            float(inv[0]), float(inv[1]))
+
+
 def sdf_sample_clamped(sdf, pt) -> float:
     dims = np.asarray(sdf.dimensions, np.uint32)
     return lib().orc_sdf_sample_clamped(_fp(sdf.distances), _u32p(dims), _f3(sdf.origin), sdf.cell_size,
@@ -214,9 +233,7 @@ class OracleKernel:
                         domain_max=_f3(domain_max), alpha=alpha, beta=beta, tier=tier,
                         threads=threads, pow_mode=pow_mode, boundary_mode=boundary_mode,
                         sdf_wall_coef=sdf_wall_coef)
-        if boundary_mode == 1:
-            if sdf is None:
-                raise ValueError("boundary_mode 1 needs an sdf")
+        if boundary_mode == 1 and sdf is not None:  # the obstacle; the box faces are walls anyway
             self._sdf = np.ascontiguousarray(sdf.distances, np.float32)
             prm.sdf_origin = _f3(sdf.origin)
             prm.sdf_cell = float(sdf.cell_size)

@@ -278,9 +278,13 @@ struct OrcParams {
 // kWallN + 1 points on [0, 2h] in double, rounded to f32, linearly
 // interpolated in f32.
 constexpr int kWallN = 512;
+constexpr int kWallN2 = 64;
+constexpr int kWallN3 = 24;
 struct WallTable {
-  float inv_step = 0.0f;
-  std::vector<float> phi, grad;
+  float inv_step = 0.0f, inv2 = 0.0f, inv3 = 0.0f;
+  std::vector<float> phi, grad;     // one slab, kWallN + 1 distances
+  std::vector<float> phi2, grad2;   // edge column, (kWallN2 + 1)^2, gradient along the first face
+  std::vector<float> phi3, grad3;   // corner cube, (kWallN3 + 1)^3, gradient along the first face
 };
 
 inline WallTable make_wall_table(float hf) {
@@ -314,6 +318,65 @@ inline WallTable make_wall_table(float hf) {
     t.grad[k] = (float)(sg * vol);
   }
   t.inv_step = (float)((double)kWallN / sup);
+  // Edge column and corner cube of the box walls: the wall sites common to
+  // two (three) face slabs, counted once per slab, so the box walls are
+  // slabs - edges + corner. Edge averaged over 8 offsets along the edge.
+  auto w_and_dw = [&](double r, double& w, double& dw) {
+    double q = r / h, om = 1.0 - 0.5 * q;
+    w = C0 / (h * h * h) * om * om * om * om * (1.0 + 2.0 * q);
+    dw = C0 / (h * h * h * h) * 5.0 * q * om * om * om;
+  };
+  t.phi2.assign((kWallN2 + 1) * (kWallN2 + 1), 0.0f);
+  t.grad2.assign((kWallN2 + 1) * (kWallN2 + 1), 0.0f);
+  for (int i = 0; i <= kWallN2; ++i)
+    for (int j = 0; j <= kWallN2; ++j) {
+      double da = (double)i * (sup / kWallN2), db = (double)j * (sup / kWallN2);
+      double sw = 0.0, sg = 0.0;
+      for (int c = 0; c < 8; ++c) {
+        double oc = (c + 0.5) / 8.0 * dx;
+        for (int la = 0; la < 3; ++la)
+          for (int lb = 0; lb < 3; ++lb) {
+            double za = da + (la + 0.5) * dx, zb = db + (lb + 0.5) * dx;
+            for (int it = -M; it <= M; ++it) {
+              double T = it * dx + oc;
+              double r = std::sqrt(za * za + zb * zb + T * T);
+              if (r >= sup) continue;
+              double w, dw;
+              w_and_dw(r, w, dw);
+              sw += w;
+              sg += dw * (za / r);
+            }
+          }
+      }
+      double vol = dx * dx * dx / 8.0;
+      t.phi2[i * (kWallN2 + 1) + j] = (float)(sw * vol);
+      t.grad2[i * (kWallN2 + 1) + j] = (float)(sg * vol);
+    }
+  const int S = kWallN3 + 1;
+  t.phi3.assign(S * S * S, 0.0f);
+  t.grad3.assign(S * S * S, 0.0f);
+  for (int i = 0; i <= kWallN3; ++i)
+    for (int j = 0; j <= kWallN3; ++j)
+      for (int l = 0; l <= kWallN3; ++l) {
+        double da = (double)i * (sup / kWallN3), db = (double)j * (sup / kWallN3), dc = (double)l * (sup / kWallN3);
+        double sw = 0.0, sg = 0.0;
+        for (int la = 0; la < 3; ++la)
+          for (int lb = 0; lb < 3; ++lb)
+            for (int lc = 0; lc < 3; ++lc) {
+              double za = da + (la + 0.5) * dx, zb = db + (lb + 0.5) * dx, zc = dc + (lc + 0.5) * dx;
+              double r = std::sqrt(za * za + zb * zb + zc * zc);
+              if (r >= sup) continue;
+              double w, dw;
+              w_and_dw(r, w, dw);
+              sw += w;
+              sg += dw * (za / r);
+            }
+        double vol = dx * dx * dx;
+        t.phi3[(i * S + j) * S + l] = (float)(sw * vol);
+        t.grad3[(i * S + j) * S + l] = (float)(sg * vol);
+      }
+  t.inv2 = (float)((double)kWallN2 / sup);
+  t.inv3 = (float)((double)kWallN3 / sup);
   return t;
 }
 
@@ -324,6 +387,32 @@ inline float wall_lookup(const std::vector<float>& v, float inv_step, float d) {
   int i = (int)u;
   float f = u - (float)i;
   return v[i] + f * (v[i + 1] - v[i]);
+}
+
+// Bilinear / trilinear interpolation of the edge / corner tables.
+inline float wall_lookup2(const std::vector<float>& v, float inv, float da, float db) {
+  float u = fmaxf(da, 0.0f) * inv, w = fmaxf(db, 0.0f) * inv;
+  if (!(u < (float)kWallN2) || !(w < (float)kWallN2)) return 0.0f;
+  int i = (int)u, j = (int)w;
+  float fu = u - (float)i, fv = w - (float)j;
+  const float* t = v.data() + i * (kWallN2 + 1) + j;
+  float a = t[0], b = t[1], c = t[kWallN2 + 1], d = t[kWallN2 + 2];
+  float x0 = a + fv * (b - a), x1 = c + fv * (d - c);
+  return x0 + fu * (x1 - x0);
+}
+inline float wall_lookup3(const std::vector<float>& v, float inv, float da, float db, float dc) {
+  float u = fmaxf(da, 0.0f) * inv, w = fmaxf(db, 0.0f) * inv, x = fmaxf(dc, 0.0f) * inv;
+  if (!(u < (float)kWallN3) || !(w < (float)kWallN3) || !(x < (float)kWallN3)) return 0.0f;
+  int i = (int)u, j = (int)w, l = (int)x;
+  float fu = u - (float)i, fv = w - (float)j, fw = x - (float)l;
+  const int S = kWallN3 + 1;
+  const float* t = v.data() + (i * S + j) * S + l;
+  float c000 = t[0], c001 = t[1], c010 = t[S], c011 = t[S + 1];
+  float c100 = t[S * S], c101 = t[S * S + 1], c110 = t[S * S + S], c111 = t[S * S + S + 1];
+  float x00 = c000 + fw * (c001 - c000), x01 = c010 + fw * (c011 - c010);
+  float x10 = c100 + fw * (c101 - c100), x11 = c110 + fw * (c111 - c110);
+  float x0 = x00 + fv * (x01 - x00), x1 = x10 + fv * (x11 - x10);
+  return x0 + fu * (x1 - x0);
 }
 
 // GridSDF::sample (geometry.rs:99-150) with the grid coordinate clamped to
@@ -392,9 +481,11 @@ class Kernel {
     for (size_t i = 0; i < p.len(); ++i) m += (double)p.mass[i];
     initial_mass = m;
     initial_energy = total_energy();
-    if (prm.boundary_mode == 1 && prm.sdf) {
-      sdf.assign(prm.sdf, prm.sdf + (size_t)prm.sdf_dims[0] * prm.sdf_dims[1] * prm.sdf_dims[2]);
-      prm.sdf = sdf.data();
+    if (prm.boundary_mode == 1) {
+      if (prm.sdf) {
+        sdf.assign(prm.sdf, prm.sdf + (size_t)prm.sdf_dims[0] * prm.sdf_dims[1] * prm.sdf_dims[2]);
+        prm.sdf = sdf.data();
+      }
       wall = make_wall_table(prm.h);
       wall_scale = wall_mass_scale();
     }
@@ -402,6 +493,42 @@ class Kernel {
   }
 
   bool sdf_mode() const { return prm.boundary_mode == 1; }
+  bool has_geo() const { return prm.sdf != nullptr; }
+  // Tier S walls: the nearer face of the domain box on each axis (distance,
+  // inward normal sign, within 2h) and the obstacle SDF.
+  struct Faces {
+    float d[3], s[3];
+    bool on[3];
+  };
+  Faces box_faces(size_t i) const {
+    Faces b;
+    float pt[3] = {p.x[i], p.y[i], p.z[i]};
+    for (int a = 0; a < 3; ++a) {
+      float dl = pt[a] - prm.domain_min[a], dh = prm.domain_max[a] - pt[a];
+      if (dl <= dh) {
+        b.d[a] = dl;
+        b.s[a] = 1.0f;
+      } else {
+        b.d[a] = dh;
+        b.s[a] = -1.0f;
+      }
+      b.on[a] = b.d[a] < 2.0f * prm.h;
+    }
+    return b;
+  }
+  // Kernel mass of the walls: box faces (slabs - edges + corner), then the
+  // obstacle at SDF distance dgeo.
+  float sdf_wall_mass(const Faces& b, float dgeo) const {
+    float m = 0.0f;
+    for (int a = 0; a < 3; ++a)
+      if (b.on[a]) m += wall_lookup(wall.phi, wall.inv_step, b.d[a]);
+    for (int a = 0; a < 3; ++a)
+      for (int c = a + 1; c < 3; ++c)
+        if (b.on[a] && b.on[c]) m -= wall_lookup2(wall.phi2, wall.inv2, b.d[a], b.d[c]);
+    if (b.on[0] && b.on[1] && b.on[2]) m += wall_lookup3(wall.phi3, wall.inv3, b.d[0], b.d[1], b.d[2]);
+    if (has_geo() && dgeo < 2.0f * prm.h) m += wall_lookup(wall.phi, wall.inv_step, dgeo);
+    return m;
+  }
   // Wall layers carry the first water particle's mass (domain.rs:57-62),
   // relative to rho0 (h / 1.3)^3; exactly 1 within 1e-5 of 1.
   float wall_scale = 1.0f;
@@ -535,12 +662,12 @@ class Kernel {
         float r = sqrtf(dx * dx + dy * dy + dz * dz);
         if (r < support) rho += b.mass[bi] * wendland_c2(r, h);
       });
-      if (sdf_mode()) {  // tier S: kernel mass of the wall half-space
-        float d = wall_distance(i);
-        if (d < support) {
-          float rest = p.fluid_type[i] == 0 ? kWaterRho0 : kAirRho0;
-          rho += rest * wall_scale * wall_lookup(wall.phi, wall.inv_step, d);
-        }
+      if (sdf_mode()) {  // tier S: kernel mass of the walls (box faces, obstacle)
+        Faces bf = box_faces(i);
+        float dgeo = has_geo() ? wall_distance(i) : support;
+        float m = sdf_wall_mass(bf, dgeo);
+        float rest = p.fluid_type[i] == 0 ? kWaterRho0 : kAirRho0;
+        rho += rest * wall_scale * m;
       }
       out[i] = rho;
     });
@@ -725,27 +852,50 @@ class Kernel {
     else compute_repulsive_forces();
   }
 
-  // Tier S wall force, after gravity: the boundary pressure force of the
-  // homogenised wall layers along the SDF normal with the mirrored pressure
-  // p_w = max(max(p_i, 0) + rho_i g.(r_w - r_i), 0), r_w taken at the middle
-  // layer (d + 1.5 dx behind the particle, boundary.rs:117-119), then the
-  // near-wall repulsion.
+  // Tier S wall force, after gravity: the energy-consistent counterpart of the
+  // walls' kernel mass in rho_i, (p_i / rho_i^2) rho0 s grad(phi) per wall
+  // term (box faces per axis: slabs - edges + corner, then each face's
+  // repulsion; then the obstacle along its SDF normal and its repulsion).
   void compute_sdf_wall_forces() {
     float h = prm.h, support = 2.0f * h, r0 = 0.5f * h;
-    float mid = 1.5f * (h / 1.3f);
-    const float* g = prm.gravity;
     parallel_for(p.len(), nthreads(), 256, [&](size_t i) {
-      float d = wall_distance(i);
+      float rest = p.fluid_type[i] == 0 ? kWaterRho0 : kAirRho0;
+      float rho_i = p.density[i];
+      float pic = fmaxf(p.pressure[i], 0.0f);
+      float pic_over = pic / (rho_i * rho_i);
+      float cw = rest * wall_scale;
+      float base = pic_over * cw;
+      // box faces per axis: slabs - edges + corner, then each face's repulsion
+      Faces bf = box_faces(i);
+      float wa[3] = {0.0f, 0.0f, 0.0f};
+      for (int a = 0; a < 3; ++a)
+        if (bf.on[a]) wa[a] += base * wall_lookup(wall.grad, wall.inv_step, bf.d[a]) * bf.s[a];
+      for (int a = 0; a < 3; ++a)
+        for (int c = a + 1; c < 3; ++c)
+          if (bf.on[a] && bf.on[c]) {
+            wa[a] -= base * wall_lookup2(wall.grad2, wall.inv2, bf.d[a], bf.d[c]) * bf.s[a];
+            wa[c] -= base * wall_lookup2(wall.grad2, wall.inv2, bf.d[c], bf.d[a]) * bf.s[c];
+          }
+      if (bf.on[0] && bf.on[1] && bf.on[2]) {
+        wa[0] += base * wall_lookup3(wall.grad3, wall.inv3, bf.d[0], bf.d[1], bf.d[2]) * bf.s[0];
+        wa[1] += base * wall_lookup3(wall.grad3, wall.inv3, bf.d[1], bf.d[0], bf.d[2]) * bf.s[1];
+        wa[2] += base * wall_lookup3(wall.grad3, wall.inv3, bf.d[2], bf.d[0], bf.d[1]) * bf.s[2];
+      }
+      for (int a = 0; a < 3; ++a)
+        if (bf.d[a] < r0) {
+          float s = 1.0f - fmaxf(bf.d[a], 0.0f) / r0;
+          float fm = prm.sdf_wall_coef * s * s / r0;
+          wa[a] += fm * bf.s[a];
+        }
+      p.ax[i] += wa[0];
+      p.ay[i] += wa[1];
+      p.az[i] += wa[2];
+      // the obstacle along its SDF normal
+      float d = has_geo() ? wall_distance(i) : support;
       if (!(d < support)) return;
       float n[3];
       sdf_gradient_clamped(prm.sdf, prm.sdf_dims, prm.sdf_origin, prm.sdf_cell, p.x[i], p.y[i], p.z[i], n);
-      float rest = p.fluid_type[i] == 0 ? kWaterRho0 : kAirRho0;
-      float pic = fmaxf(p.pressure[i], 0.0f);
-      float depth = -(d + mid);
-      float g_dot_dr = g[0] * (depth * n[0]) + g[1] * (depth * n[1]) + g[2] * (depth * n[2]);
-      float pw = fmaxf(pic + p.density[i] * g_dot_dr, 0.0f);
-      float coef = (pic / (p.density[i] * p.density[i]) + pw / (rest * rest)) * (rest * wall_scale) *
-                   wall_lookup(wall.grad, wall.inv_step, d);
+      float coef = base * wall_lookup(wall.grad, wall.inv_step, d);
       p.ax[i] += coef * n[0];
       p.ay[i] += coef * n[1];
       p.az[i] += coef * n[2];
@@ -1164,6 +1314,18 @@ int orc_wall_table(float h, float* phi, float* grad, float* inv_step) {
   std::memcpy(grad, t.grad.data(), t.grad.size() * 4);
   *inv_step = t.inv_step;
   return kWallN;
+}
+// Edge ((kWallN2 + 1)^2) and corner ((kWallN3 + 1)^3) tables; returns
+// kWallN2 * 1000 + kWallN3.
+int orc_wall_tables_box(float h, float* phi2, float* grad2, float* phi3, float* grad3, float* inv2, float* inv3) {
+  WallTable t = make_wall_table(h);
+  std::memcpy(phi2, t.phi2.data(), t.phi2.size() * 4);
+  std::memcpy(grad2, t.grad2.data(), t.grad2.size() * 4);
+  std::memcpy(phi3, t.phi3.data(), t.phi3.size() * 4);
+  std::memcpy(grad3, t.grad3.data(), t.grad3.size() * 4);
+  *inv2 = t.inv2;
+  *inv3 = t.inv3;
+  return kWallN2 * 1000 + kWallN3;
 }
 float orc_sdf_sample_clamped(const float* d, const uint32_t* dims, const float* origin, float cell,
                              const float* pt) {

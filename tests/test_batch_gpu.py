@@ -63,7 +63,7 @@ def test_batch_sdf_mode_matches_single_runs():
     from ultraballpit_b200.kernel import BOUNDARY_SDF
     scs = [closure.tank_pair(s, dx_coarse=0.008)[0] for s in (21, 22, 23)]
     batch = CudaBatch(scs, boundary_mode=BOUNDARY_SDF)
-    singles = [CudaKernel(*sc.kernel_args(), alpha=sc.alpha, boundary_mode=BOUNDARY_SDF, sdf=sc.sdf)
+    singles = [CudaKernel(*sc.kernel_args(), alpha=sc.alpha, boundary_mode=BOUNDARY_SDF, sdf=sc.obstacle_sdf)
                for sc in scs]
     batch.step_auto(10, want_dt=False)
     for k in singles:

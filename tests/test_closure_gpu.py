@@ -62,7 +62,7 @@ def _tank(dx=0.004, seed=11):
 
 
 def _sdf_kernel(sc):
-    return CudaKernel(*sc.kernel_args(), alpha=sc.alpha, boundary_mode=BOUNDARY_SDF, sdf=sc.sdf)
+    return CudaKernel(*sc.kernel_args(), alpha=sc.alpha, boundary_mode=BOUNDARY_SDF, sdf=sc.obstacle_sdf)
 
 
 def _same(a, b):

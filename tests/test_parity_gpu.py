@@ -260,9 +260,9 @@ def test_sdf_mode_bit_exact_with_sphere():
     from ultraballpit_b200.kernel import BOUNDARY_SDF
     sc = domain.dam_break(0.004, seed=31, sphere=True)
     args = sc.kernel_args()
-    gpu = CudaKernel(*args, alpha=sc.alpha, boundary_mode=BOUNDARY_SDF, sdf=sc.sdf)
+    gpu = CudaKernel(*args, alpha=sc.alpha, boundary_mode=BOUNDARY_SDF, sdf=sc.obstacle_sdf)
     cpu = orc.OracleKernel(*args, alpha=sc.alpha, tier=1, threads=8, pow_mode=1, boundary_mode=1,
-                           sdf=sc.sdf)
+                           sdf=sc.obstacle_sdf)
     for _ in range(20):
         dt = cpu.compute_timestep(sc.cfl_number)
         assert gpu.compute_timestep() == dt
@@ -314,4 +314,28 @@ def test_scale_velocities_scales_the_state_the_next_step_starts_from():
     assert not np.any(p2.vx) and not np.any(p2.vy) and not np.any(p2.vz)
     k.step(k.compute_timestep())
     assert k.health() == 0
+    k.close()
+
+
+def test_sdf_mode_tank_at_rest_stays_quiet_at_edges_and_corners():
+    """A closed tank at rest in SDF wall mode: the box faces' slabs, edges and
+    corners, and the energy-consistent wall force, keep the water near the
+    edges and corners as quiet as the rest (no relaxation first)."""
+    from ultraballpit_b200 import closure
+    from ultraballpit_b200.kernel import BOUNDARY_SDF
+    sc = domain.tank_with_sphere(0.004, domain_max=closure.TANK, center=(0.05, 0.05, -1.0), radius=0.01,
+                                 fill_height=closure.FILL, seed=3, hydrostatic=True, geometry="lattice")
+    k = CudaKernel(*sc.kernel_args(), alpha=sc.alpha, boundary_mode=BOUNDARY_SDF)
+    for _ in range(600):
+        k.step(5e-5)
+    assert k.health() == 0
+    p = k.particles()
+    pos = np.stack([p.x, p.y, p.z], 1).astype(np.float64)
+    v = np.sqrt(p.vx.astype(np.float64) ** 2 + p.vy ** 2 + p.vz ** 2)
+    dw = np.sort(np.stack([pos[:, 0], 0.1 - pos[:, 0], pos[:, 1], 0.1 - pos[:, 1], pos[:, 2]], 1), 1)
+    h = sc.h
+    for name, m in (("wall", (dw[:, 0] < 2 * h) & (dw[:, 1] >= 2 * h)),
+                    ("edge", (dw[:, 1] < 2 * h) & (dw[:, 2] >= 2 * h)), ("corner", dw[:, 2] < 2 * h)):
+        assert v[m].mean() < 0.12, (name, v[m].mean())
+    assert p.z.max() < closure.FILL + 0.01
     k.close()

@@ -162,7 +162,8 @@ WALLS = "particles"
 def _kernel(sc, device=0, walls=None):
     from .kernel import BOUNDARY_SDF, CudaKernel
     if (walls or WALLS) == "sdf":
-        return CudaKernel(*sc.kernel_args(), alpha=sc.alpha, device=device, boundary_mode=BOUNDARY_SDF, sdf=sc.sdf)
+        return CudaKernel(*sc.kernel_args(), alpha=sc.alpha, device=device, boundary_mode=BOUNDARY_SDF,
+                          sdf=sc.obstacle_sdf)
     k = CudaKernel(*sc.kernel_args(), alpha=sc.alpha, device=device)
     k.set_feature_sdf(sc.sdf)
     return k

@@ -251,6 +251,73 @@ std::vector<float2> make_wall_table(float hf, float* inv_step) {
   return t;
 }
 
+// Edge and corner tables of the SDF wall (appended to the slab table at
+// kWallOff2 and kWallOff3): where the 3-layer slabs of two (three) box faces
+// meet, their common wall sites (depths (la + 0.5) dx, (lb + 0.5) dx
+// [, (lc + 0.5) dx] beyond the faces) are counted once per slab, so the box
+// walls are sum(slabs) - sum(edge columns) + corner cube. Edge: W and the
+// gradient along the first face's normal, averaged over 8 offsets along the
+// edge, at (d_a, d_b) on a (kWallN2 + 1)^2 grid of [0, 2h]^2. Corner: the 27
+// sites, at (d_a, d_b, d_c) on a (kWallN3 + 1)^3 grid.
+std::vector<float2> make_wall_tables(float hf, float* inv1, float* inv2, float* inv3) {
+  std::vector<float2> t = make_wall_table(hf, inv1);
+  t.resize(sph::kWallTabSize);
+  const double h = hf, dx = h / 1.3, sup = 2.0 * h;
+  const double C0 = 21.0 / (16.0 * 3.14159265358979323846);
+  const int M = (int)std::ceil(sup / dx) + 1;
+  auto w_and_dw = [&](double r, double& w, double& dw) {  // W and -dW/dr
+    double q = r / h, om = 1.0 - 0.5 * q;
+    w = C0 / (h * h * h) * om * om * om * om * (1.0 + 2.0 * q);
+    dw = C0 / (h * h * h * h) * 5.0 * q * om * om * om;
+  };
+  const int N2 = sph::kWallN2, N3 = sph::kWallN3;
+  for (int i = 0; i <= N2; ++i)
+    for (int j = 0; j <= N2; ++j) {
+      double da = (double)i * (sup / N2), db = (double)j * (sup / N2);
+      double sw = 0.0, sg = 0.0;
+      for (int c = 0; c < 8; ++c) {
+        double oc = (c + 0.5) / 8.0 * dx;
+        for (int la = 0; la < 3; ++la)
+          for (int lb = 0; lb < 3; ++lb) {
+            double za = da + (la + 0.5) * dx, zb = db + (lb + 0.5) * dx;
+            for (int it = -M; it <= M; ++it) {
+              double T = it * dx + oc;
+              double r = std::sqrt(za * za + zb * zb + T * T);
+              if (r >= sup) continue;
+              double w, dw;
+              w_and_dw(r, w, dw);
+              sw += w;
+              sg += dw * (za / r);
+            }
+          }
+      }
+      double vol = dx * dx * dx / 8.0;
+      t[sph::kWallOff2 + i * (N2 + 1) + j] = make_float2((float)(sw * vol), (float)(sg * vol));
+    }
+  for (int i = 0; i <= N3; ++i)
+    for (int j = 0; j <= N3; ++j)
+      for (int l = 0; l <= N3; ++l) {
+        double da = (double)i * (sup / N3), db = (double)j * (sup / N3), dc = (double)l * (sup / N3);
+        double sw = 0.0, sg = 0.0;
+        for (int la = 0; la < 3; ++la)
+          for (int lb = 0; lb < 3; ++lb)
+            for (int lc = 0; lc < 3; ++lc) {
+              double za = da + (la + 0.5) * dx, zb = db + (lb + 0.5) * dx, zc = dc + (lc + 0.5) * dx;
+              double r = std::sqrt(za * za + zb * zb + zc * zc);
+              if (r >= sup) continue;
+              double w, dw;
+              w_and_dw(r, w, dw);
+              sw += w;
+              sg += dw * (za / r);
+            }
+        double vol = dx * dx * dx;
+        t[sph::kWallOff3 + (i * (N3 + 1) + j) * (N3 + 1) + l] = make_float2((float)(sw * vol), (float)(sg * vol));
+      }
+  *inv2 = (float)((double)N2 / sup);
+  *inv3 = (float)((double)N3 / sup);
+  return t;
+}
+
 // Mass of the homogenised wall layers relative to rho0 (h / 1.3)^3: the
 // walls carry the mass of the first water particle (the reference gives wall
 // particles the water particle mass, orchestrator/src/domain.rs:57-62).
@@ -566,18 +633,24 @@ int create_impl(int ninst, const SphParams* PP, const SphParticlesView* pvs,
     if (!sdf_mode && bv) nbtot += bv->n;
   }
   if (ntot > 0x7fffffffull || nbtot > 0x7fffffffull) return SPH_ERR_INVALID_ARG;
-  // SDF wall mode: one SDF per instance (concatenated on the device), one
-  // wall table, so every instance must share the smoothing length.
+  // SDF wall mode: the domain box faces are walls; an instance's obstacle SDF
+  // (optional: distances may be NULL) is concatenated on the device; one wall
+  // table, so every instance must share the smoothing length.
   uint64_t sdf_nodes = 0;
   std::vector<uint64_t> sdf_off(ninst + 1, 0);
   if (sdf_mode) {
-    if (!sdfs) return SPH_ERR_INVALID_ARG;
     for (int q = 0; q < ninst; ++q) {
-      const SphSdfView* sd = &sdfs[q];
-      if (!sd->distances || !(sd->cell_size > 0.0f)) return SPH_ERR_INVALID_ARG;
-      if (sd->dims[0] < 2 || sd->dims[1] < 2 || sd->dims[2] < 2) return SPH_ERR_INVALID_ARG;
       if (PP[q].h != PP[0].h) return SPH_ERR_INVALID_ARG;
-      sdf_off[q + 1] = sdf_off[q] + (uint64_t)sd->dims[0] * sd->dims[1] * sd->dims[2];
+      for (int a = 0; a < 3; ++a)
+        if (!(PP[q].domain_max[a] - PP[q].domain_min[a] >= 4.0f * PP[q].h)) return SPH_ERR_INVALID_ARG;
+      const SphSdfView* sd = sdfs ? &sdfs[q] : nullptr;
+      uint64_t nodes = 0;
+      if (sd && sd->distances) {
+        if (!(sd->cell_size > 0.0f)) return SPH_ERR_INVALID_ARG;
+        if (sd->dims[0] < 2 || sd->dims[1] < 2 || sd->dims[2] < 2) return SPH_ERR_INVALID_ARG;
+        nodes = (uint64_t)sd->dims[0] * sd->dims[1] * sd->dims[2];
+      }
+      sdf_off[q + 1] = sdf_off[q] + nodes;
     }
     sdf_nodes = sdf_off[ninst];
   }
@@ -637,15 +710,17 @@ int create_impl(int ninst, const SphParams* PP, const SphParticlesView* pvs,
     k.coff = (int)C;
     k.cfl = P.cfl_number;
     if (sdf_mode) {
-      const SphSdfView* sd = &sdfs[q];
+      const SphSdfView* sd = sdfs ? &sdfs[q] : nullptr;
       k.sdf_mode = 1;
-      for (int a = 0; a < 3; ++a) {
-        k.sdf_origin[a] = sd->origin[a];
-        k.sdf_dims[a] = (int)sd->dims[a];
+      k.has_geo = (sd && sd->distances) ? 1 : 0;
+      if (k.has_geo) {
+        for (int a = 0; a < 3; ++a) {
+          k.sdf_origin[a] = sd->origin[a];
+          k.sdf_dims[a] = (int)sd->dims[a];
+        }
+        k.sdf_cell = sd->cell_size;
       }
-      k.sdf_cell = sd->cell_size;
       k.sdf_off = (long long)sdf_off[q];
-      k.wall_mid = 1.5f * (P.h / 1.3f);
       k.wall_scale = wall_mass_scale(P.h, pv);
       k.feat_sdf = 1;
     }
@@ -699,8 +774,13 @@ int create_impl(int ninst, const SphParams* PP, const SphParticlesView* pvs,
   std::vector<float2> wall_host;
   if (sdf_mode) {
     float inv = 0.0f;
-    wall_host = make_wall_table(P0.h, &inv);
-    for (int q = 0; q < ninst; ++q) h->ktab_h[q].wall_inv_step = inv;
+    float inv2 = 0.0f, inv3 = 0.0f;
+    wall_host = make_wall_tables(P0.h, &inv, &inv2, &inv3);
+    for (int q = 0; q < ninst; ++q) {
+      h->ktab_h[q].wall_inv_step = inv;
+      h->ktab_h[q].wall_inv2 = inv2;
+      h->ktab_h[q].wall_inv3 = inv3;
+    }
   }
   h->k = h->ktab_h[0];
 
@@ -725,7 +805,7 @@ int create_impl(int ninst, const SphParams* PP, const SphParticlesView* pvs,
   if (ninst > 1) {
     ALLOC(ktab, ninst); ALLOC(inst_p, n); ALLOC(inst_b, nb);
   }
-  if (sdf_mode) ALLOC(sdf, sdf_nodes);
+  if (sdf_mode) ALLOC(sdf, std::max<uint64_t>(sdf_nodes, 1));
   if (sdf_mode) ALLOC(wall_tab, wall_host.size());
 #undef ALLOC
   if (e != cudaSuccess) return fail(e == cudaErrorMemoryAllocation ? SPH_ERR_OOM : SPH_ERR_CUDA);
@@ -779,7 +859,8 @@ int create_impl(int ninst, const SphParams* PP, const SphParticlesView* pvs,
     up(h->inst_b, hib.data(), nb * sizeof(uint16_t));
   }
   for (int q = 0; sdf_mode && q < ninst; ++q)
-    up(h->sdf + sdf_off[q], sdfs[q].distances, (sdf_off[q + 1] - sdf_off[q]) * sizeof(float));
+    if (sdf_off[q + 1] > sdf_off[q])
+      up(h->sdf + sdf_off[q], sdfs[q].distances, (sdf_off[q + 1] - sdf_off[q]) * sizeof(float));
   if (sdf_mode) up(h->wall_tab, wall_host.data(), wall_host.size() * sizeof(float2));
   if (e == cudaSuccess) e = cudaMemsetAsync(h->hist, 0, C * sizeof(uint32_t), h->st);
   if (e == cudaSuccess) e = cudaMemsetAsync(h->bpress, 0, std::max<size_t>(1, nb) * sizeof(float), h->st);
@@ -854,7 +935,7 @@ int sph_batch_create_sdf(int ninst, const SphParams* params, const SphParticlesV
                          const SphSdfView* sdfs, SphHandle** out) {
   if (!out) return SPH_ERR_INVALID_ARG;
   *out = nullptr;
-  if (ninst < 1 || !params || !particles || !sdfs) return SPH_ERR_INVALID_ARG;
+  if (ninst < 1 || !params || !particles) return SPH_ERR_INVALID_ARG;
   for (int q = 0; q < ninst; ++q)
     if (params[q].boundary_mode != SPH_BOUNDARY_SDF) return SPH_ERR_INVALID_ARG;
   return create_impl(ninst, params, particles, nullptr, sdfs, out);

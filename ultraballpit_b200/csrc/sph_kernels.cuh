@@ -65,10 +65,11 @@ struct SimConst {
   // SDF wall mode (boundary_mode 1): node grid geometry
   int sdf_mode;
   float wall_inv_step;   // kWallN / 2h
-  float wall_mid;        // 1.5 * (h / 1.3): depth of the middle wall layer
   // wall particle mass / (rho0 (h / 1.3)^3): the homogenised wall layers
   // carry the fluid's particle mass; exactly 1 for mass rho0 dx^3
   float wall_scale;
+  float wall_inv2, wall_inv3;  // kWallN2 / 2h, kWallN3 / 2h: edge and corner tables
+  int has_geo;                 // SDF mode: an obstacle SDF is present
   float sdf_origin[3];
   float sdf_cell;
   int sdf_dims[3];
@@ -159,11 +160,23 @@ __device__ __forceinline__ float tait(float rho, bool air, const SimConst& k) {
 }
 
 // ---- SDF wall (boundary_mode 1; no reference counterpart) -----------------
-// The SDF wall stands in for the reference's 3 layers of wall particles,
-// homogenised along the wall: wall_tab holds, at kWallN + 1 distances on
-// [0, 2h], the lateral-average lattice sums (phi = sum W dx^3, grad =
-// sum -dW/dn dx^3) built on the host; linear interpolation in f32.
+// The walls stand in for the reference's 3 layers of wall particles on every
+// face of the domain box (domain.rs:162-348) plus those of an obstacle given
+// by its SDF, homogenised along each wall. wall_tab holds lattice sums built
+// on the host (phi = sum W dx^3, grad = sum (-dW/dr)(z_a / r) dx^3 along the
+// first argument's normal a):
+//   [0, kWallN]           one 3-layer slab at distance d (lateral average),
+//   kWallOff2 + ...       the edge column where two slabs meet, at (d_a, d_b)
+//                         (average along the edge),
+//   kWallOff3 + ...       the corner cube of three slabs, at (d_a, d_b, d_c),
+// on [0, 2h] per argument, interpolated (bi-, tri-)linearly in f32. The box
+// walls are the union of the face slabs: singles - edges + corner.
 constexpr int kWallN = 512;
+constexpr int kWallN2 = 64;
+constexpr int kWallN3 = 24;
+constexpr int kWallOff2 = kWallN + 1;
+constexpr int kWallOff3 = kWallOff2 + (kWallN2 + 1) * (kWallN2 + 1);
+constexpr int kWallTabSize = kWallOff3 + (kWallN3 + 1) * (kWallN3 + 1) * (kWallN3 + 1);
 __device__ __forceinline__ float2 wall_lookup(const float2* __restrict__ tab, float inv_step, float d) {
   float u = fmaxf(d, 0.0f) * inv_step;
   if (!(u < (float)kWallN)) return make_float2(0.0f, 0.0f);
@@ -171,6 +184,83 @@ __device__ __forceinline__ float2 wall_lookup(const float2* __restrict__ tab, fl
   float f = u - (float)i;
   float2 a = __ldg(&tab[i]), b = __ldg(&tab[i + 1]);
   return make_float2(a.x + f * (b.x - a.x), a.y + f * (b.y - a.y));
+}
+
+__device__ __forceinline__ float2 wall_lookup2(const float2* __restrict__ tab, float inv, float da, float db) {
+  float u = fmaxf(da, 0.0f) * inv, v = fmaxf(db, 0.0f) * inv;
+  if (!(u < (float)kWallN2) || !(v < (float)kWallN2)) return make_float2(0.0f, 0.0f);
+  int i = (int)u, j = (int)v;
+  float fu = u - (float)i, fv = v - (float)j;
+  const float2* t = tab + kWallOff2 + i * (kWallN2 + 1) + j;
+  float2 a = __ldg(t), b = __ldg(t + 1), c = __ldg(t + kWallN2 + 1), d = __ldg(t + kWallN2 + 2);
+  float x0 = a.x + fv * (b.x - a.x), x1 = c.x + fv * (d.x - c.x);
+  float y0 = a.y + fv * (b.y - a.y), y1 = c.y + fv * (d.y - c.y);
+  return make_float2(x0 + fu * (x1 - x0), y0 + fu * (y1 - y0));
+}
+
+__device__ __forceinline__ float2 wall_lookup3(const float2* __restrict__ tab, float inv, float da, float db,
+                                               float dc) {
+  float u = fmaxf(da, 0.0f) * inv, v = fmaxf(db, 0.0f) * inv, w = fmaxf(dc, 0.0f) * inv;
+  if (!(u < (float)kWallN3) || !(v < (float)kWallN3) || !(w < (float)kWallN3)) return make_float2(0.0f, 0.0f);
+  int i = (int)u, j = (int)v, l = (int)w;
+  float fu = u - (float)i, fv = v - (float)j, fw = w - (float)l;
+  const int S = kWallN3 + 1;
+  const float2* t = tab + kWallOff3 + (i * S + j) * S + l;
+  float2 c000 = __ldg(t), c001 = __ldg(t + 1), c010 = __ldg(t + S), c011 = __ldg(t + S + 1);
+  float2 c100 = __ldg(t + S * S), c101 = __ldg(t + S * S + 1), c110 = __ldg(t + S * S + S),
+         c111 = __ldg(t + S * S + S + 1);
+  float x00 = c000.x + fw * (c001.x - c000.x), x01 = c010.x + fw * (c011.x - c010.x);
+  float x10 = c100.x + fw * (c101.x - c100.x), x11 = c110.x + fw * (c111.x - c110.x);
+  float y00 = c000.y + fw * (c001.y - c000.y), y01 = c010.y + fw * (c011.y - c010.y);
+  float y10 = c100.y + fw * (c101.y - c100.y), y11 = c110.y + fw * (c111.y - c110.y);
+  float x0 = x00 + fv * (x01 - x00), x1 = x10 + fv * (x11 - x10);
+  float y0 = y00 + fv * (y01 - y00), y1 = y10 + fv * (y11 - y10);
+  return make_float2(x0 + fu * (x1 - x0), y0 + fu * (y1 - y0));
+}
+
+// The nearer face of the domain box on each axis: distance, inward normal
+// sign (+1 at the lower face, -1 at the upper) and whether it is within 2h.
+// Domains narrower than 4h, where both faces of an axis could be, are not
+// supported by the SDF wall mode.
+struct BoxFaces {
+  float d[3], s[3];
+  bool on[3];
+};
+__device__ __forceinline__ BoxFaces box_faces(const SimConst& k, float px, float py, float pz) {
+  BoxFaces b;
+  float p[3] = {px, py, pz};
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    float dl = p[a] - k.dmin[a], dh = k.dmax[a] - p[a];
+    if (dl <= dh) {
+      b.d[a] = dl;
+      b.s[a] = 1.0f;
+    } else {
+      b.d[a] = dh;
+      b.s[a] = -1.0f;
+    }
+    b.on[a] = b.d[a] < k.support;
+  }
+  return b;
+}
+
+// Kernel mass of the SDF-mode walls at a particle, in units of the wall
+// particle mass density: box faces (singles - edges + corner), then the
+// obstacle at SDF distance dgeo.
+__device__ __forceinline__ float sdf_wall_mass(const SimConst& k, const float2* __restrict__ tab,
+                                               const BoxFaces& b, float dgeo) {
+  float m = 0.0f;
+#pragma unroll
+  for (int a = 0; a < 3; ++a)
+    if (b.on[a]) m += wall_lookup(tab, k.wall_inv_step, b.d[a]).x;
+#pragma unroll
+  for (int a = 0; a < 3; ++a)
+#pragma unroll
+    for (int c = a + 1; c < 3; ++c)
+      if (b.on[a] && b.on[c]) m -= wall_lookup2(tab, k.wall_inv2, b.d[a], b.d[c]).x;
+  if (b.on[0] && b.on[1] && b.on[2]) m += wall_lookup3(tab, k.wall_inv3, b.d[0], b.d[1], b.d[2]).x;
+  if (k.has_geo && dgeo < k.support) m += wall_lookup(tab, k.wall_inv_step, dgeo).x;
+  return m;
 }
 
 // GridSDF::sample (orchestrator geometry.rs:99-150) with the grid coordinate
@@ -216,6 +306,28 @@ __device__ __forceinline__ void sdf_gradient_clamped(const float* __restrict__ d
   float mag = sqrtf(gx * gx + gy * gy + gz * gz);
   if (mag > 1e-8f) { nx = gx / mag; ny = gy / mag; nz = gz / mag; }
   else { nx = 0.0f; ny = 0.0f; nz = 0.0f; }
+}
+
+// Distance to the nearest wall of the SDF mode (a box face or the obstacle)
+// and its inward normal: the closure features' SDF in that mode.
+__device__ __forceinline__ float wall_distance(const SimConst& k, const float* __restrict__ sdf, float px,
+                                               float py, float pz) {
+  BoxFaces b = box_faces(k, px, py, pz);
+  float d = fminf(fminf(b.d[0], b.d[1]), b.d[2]);
+  if (k.has_geo) d = fminf(d, sdf_sample_clamped(sdf, k, px, py, pz));
+  return d;
+}
+__device__ __forceinline__ void wall_normal(const SimConst& k, const float* __restrict__ sdf, float px,
+                                            float py, float pz, float& nx, float& ny, float& nz) {
+  BoxFaces b = box_faces(k, px, py, pz);
+  int a = b.d[0] <= b.d[1] ? (b.d[0] <= b.d[2] ? 0 : 2) : (b.d[1] <= b.d[2] ? 1 : 2);
+  if (k.has_geo && sdf_sample_clamped(sdf, k, px, py, pz) < b.d[a]) {
+    sdf_gradient_clamped(sdf, k, px, py, pz, nx, ny, nz);
+    return;
+  }
+  nx = a == 0 ? b.s[0] : 0.0f;
+  ny = a == 1 ? b.s[1] : 0.0f;
+  nz = a == 2 ? b.s[2] : 0.0f;
 }
 
 __device__ __forceinline__ uint32_t spread10(uint32_t v) {
@@ -695,10 +807,12 @@ k_density(KP kp, int n, const float* __restrict__ dtp, const float4* __restrict_
     }
   }
   bool air = (id[i] & kAirBit) != 0;
-  if (k.sdf_mode) {  // kernel mass of the wall half-space
-    float d = sdf_sample_clamped(sdf, k, pi.x, pi.y, pi.z);
-    if (d < k.support)
-      rho += (air ? kAirRho0 : kWaterRho0) * k.wall_scale * wall_lookup(wall_tab, k.wall_inv_step, d).x;
+  float wall_m = 0.0f;
+  if (k.sdf_mode) {  // kernel mass of the walls: box faces and obstacle
+    BoxFaces bf = box_faces(k, pi.x, pi.y, pi.z);
+    float dgeo = k.has_geo ? sdf_sample_clamped(sdf, k, pi.x, pi.y, pi.z) : k.support;
+    wall_m = sdf_wall_mass(k, wall_tab, bf, dgeo);
+    rho += (air ? kAirRho0 : kWaterRho0) * k.wall_scale * wall_m;
   }
   if (delta) {
     float diffusion = k.delta_coef * diff_sum;
@@ -709,21 +823,28 @@ k_density(KP kp, int n, const float* __restrict__ dtp, const float4* __restrict_
   pr[i] = p;
   if (CL) {
     cb.corr[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-    float d = sdf_sample_clamped(sdf, k, pi.x, pi.y, pi.z);
+    // feature SDF: the given geometry SDF, or in SDF wall mode the distance
+    // to the nearest wall (box face or obstacle)
+    auto fsdf = [&](float x, float y, float z) {
+      return k.sdf_mode ? wall_distance(k, sdf, x, y, z) : sdf_sample_clamped(sdf, k, x, y, z);
+    };
+    float d = k.feat_sdf ? fsdf(pi.x, pi.y, pi.z) : k.support;
     if (k.feat_sdf && d < k.support) {
       // Geometry and kinematics only: the particle's own density is not a
       // feature, so the correction cannot soften the equation of state.
       float nx, ny, nz;
-      sdf_gradient_clamped(sdf, k, pi.x, pi.y, pi.z, nx, ny, nz);
+      if (k.sdf_mode)
+        wall_normal(k, sdf, pi.x, pi.y, pi.z, nx, ny, nz);
+      else
+        sdf_gradient_clamped(sdf, k, pi.x, pi.y, pi.z, nx, ny, nz);
       float4 v = cb.vel[i];
       float rest = air ? kAirRho0 : kWaterRho0;
       float gm = sqrtf(k.grav[0] * k.grav[0] + k.grav[1] * k.grav[1] + k.grav[2] * k.grav[2]);
       // h * Laplacian of the SDF (sum of the principal curvatures) by second
       // differences at step h; the trilinear field is piecewise linear, so a
       // step of one SDF cell would only see its kinks.
-      float lap = sdf_sample_clamped(sdf, k, pi.x + k.h, pi.y, pi.z) + sdf_sample_clamped(sdf, k, pi.x - k.h, pi.y, pi.z) +
-                  sdf_sample_clamped(sdf, k, pi.x, pi.y + k.h, pi.z) + sdf_sample_clamped(sdf, k, pi.x, pi.y - k.h, pi.z) +
-                  sdf_sample_clamped(sdf, k, pi.x, pi.y, pi.z + k.h) + sdf_sample_clamped(sdf, k, pi.x, pi.y, pi.z - k.h) -
+      float lap = fsdf(pi.x + k.h, pi.y, pi.z) + fsdf(pi.x - k.h, pi.y, pi.z) + fsdf(pi.x, pi.y + k.h, pi.z) +
+                  fsdf(pi.x, pi.y - k.h, pi.z) + fsdf(pi.x, pi.y, pi.z + k.h) + fsdf(pi.x, pi.y, pi.z - k.h) -
                   6.0f * d;
       float f[16];
       f[0] = d / k.h;
@@ -733,7 +854,7 @@ k_density(KP kp, int n, const float* __restrict__ dtp, const float4* __restrict_
       f[6] = sqrtf(v.x * v.x + v.y * v.y + v.z * v.z) / k.c;
       f[7] = dt * k.c / k.h;
       f[8] = fminf(fmaxf(lap / k.h, -4.0f), 4.0f);
-      f[9] = k.sdf_mode ? k.wall_scale * wall_lookup(wall_tab, k.wall_inv_step, d).x : rho_wall / rest;
+      f[9] = k.sdf_mode ? k.wall_scale * wall_m : rho_wall / rest;
       f[10] = gm > 0.0f ? (k.grav[0] * nx + k.grav[1] * ny + k.grav[2] * nz) / gm : 0.0f;
       f[11] = f[0] * f[0];
       f[12] = f[8] * f[0];
@@ -1012,20 +1133,52 @@ k_forces(KP kp, int n, const float* __restrict__ dtp, float hdt_scale,
     ax += fvx; ay += fvy; az += fvz;
     ax += k.grav[0]; ay += k.grav[1]; az += k.grav[2];
     if (k.sdf_mode) {
-      // boundary pressure force of the homogenised wall layers along the
-      // SDF normal, with the mirrored pressure p_w = max(max(p_i,0) +
-      // rho_i g.(r_w - r_i), 0) at the middle layer, then the repulsion
-      float d = sdf_sample_clamped(sdf, k, pi.x, pi.y, pi.z);
+      // pressure force of the homogenised wall layers: the energy-consistent
+      // counterpart of their kernel mass in rho_i (the gradient of
+      // E = sum m e(rho) gives a_i += (p_i / rho_i^2) rho0 s grad(phi) per
+      // wall term, the particle's own pressure only). Box faces per axis
+      // (singles - edges + corner, then each face's repulsion), then the
+      // obstacle along its SDF normal.
+      float rest = air ? kAirRho0 : kWaterRho0;
+      float pic = fmaxf(pr[i], 0.0f);
+      float pic_over = pic / (rho_i * rho_i);
+      float cw = rest * k.wall_scale;
+      float base = pic_over * cw;
+      BoxFaces bf = box_faces(k, pi.x, pi.y, pi.z);
+      float wa[3] = {0.0f, 0.0f, 0.0f};
+#pragma unroll
+      for (int a = 0; a < 3; ++a)
+        if (bf.on[a]) wa[a] += base * wall_lookup(wall_tab, k.wall_inv_step, bf.d[a]).y * bf.s[a];
+#pragma unroll
+      for (int a = 0; a < 3; ++a)
+#pragma unroll
+        for (int c = a + 1; c < 3; ++c)
+          if (bf.on[a] && bf.on[c]) {
+            wa[a] -= base * wall_lookup2(wall_tab, k.wall_inv2, bf.d[a], bf.d[c]).y * bf.s[a];
+            wa[c] -= base * wall_lookup2(wall_tab, k.wall_inv2, bf.d[c], bf.d[a]).y * bf.s[c];
+          }
+      if (bf.on[0] && bf.on[1] && bf.on[2]) {
+        wa[0] += base * wall_lookup3(wall_tab, k.wall_inv3, bf.d[0], bf.d[1], bf.d[2]).y * bf.s[0];
+        wa[1] += base * wall_lookup3(wall_tab, k.wall_inv3, bf.d[1], bf.d[0], bf.d[2]).y * bf.s[1];
+        wa[2] += base * wall_lookup3(wall_tab, k.wall_inv3, bf.d[2], bf.d[0], bf.d[1]).y * bf.s[2];
+      }
+      if (k.flags & kFlagRepulsion) {
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+          if (bf.d[a] < k.r0) {
+            float s = 1.0f - fmaxf(bf.d[a], 0.0f) / k.r0;
+            float fm = k.sdf_coef * s * s / k.r0;
+            wa[a] += fm * bf.s[a];
+          }
+      }
+      ax += wa[0];
+      ay += wa[1];
+      az += wa[2];
+      float d = k.has_geo ? sdf_sample_clamped(sdf, k, pi.x, pi.y, pi.z) : k.support;
       if (d < k.support) {
         float nx, ny, nz;
         sdf_gradient_clamped(sdf, k, pi.x, pi.y, pi.z, nx, ny, nz);
-        float rest = air ? kAirRho0 : kWaterRho0;
-        float pic = fmaxf(pr[i], 0.0f);
-        float depth = -(d + k.wall_mid);
-        float g_dot_dr = k.grav[0] * (depth * nx) + k.grav[1] * (depth * ny) + k.grav[2] * (depth * nz);
-        float pw = fmaxf(pic + rho_i * g_dot_dr, 0.0f);
-        float coef = (pic / (rho_i * rho_i) + pw / (rest * rest)) * (rest * k.wall_scale) *
-                     wall_lookup(wall_tab, k.wall_inv_step, d).y;
+        float coef = base * wall_lookup(wall_tab, k.wall_inv_step, d).y;
         ax += coef * nx;
         ay += coef * ny;
         az += coef * nz;

@@ -288,6 +288,12 @@ class Scenario:
         return (self.particles, self.boundary, self.h, self.gravity, self.speed_of_sound,
                 self.cfl_number, self.viscosity, self.domain_min, self.domain_max)
 
+    @property
+    def obstacle_sdf(self) -> GridSDF | None:
+        """The obstacle's own SDF (the SDF wall mode's ``sdf``: the domain
+        box faces are walls of their own), or None without one."""
+        return self.extras.get("sphere_sdf")
+
 
 def dam_break_c0(height: float = 0.2, g: float = 9.81) -> float:
     """``c0 = 10 sqrt(2 g H)`` (19.81 m/s at H = 0.2 m), no auto-tune."""

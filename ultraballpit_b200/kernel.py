@@ -269,7 +269,11 @@ def _boundary_view(boundary: BoundaryParticles | None, keep: list):
 
 
 class CudaKernel(SimulationKernel):
-    """The ``cuda`` backend: one simulation on one B200 through libsph_cuda.so."""
+    """The ``cuda`` backend: one simulation on one B200 through libsph_cuda.so.
+
+    ``boundary_mode`` BOUNDARY_SDF replaces the boundary particles by
+    homogenised walls on the six faces of the domain box plus the obstacle
+    whose SDF ``sdf`` gives (None: no obstacle)."""
 
     def __init__(self, particles: ParticleArrays, boundary: BoundaryParticles | None, h: float,
                  gravity, speed_of_sound: float, cfl_number: float, viscosity: float,
@@ -541,8 +545,8 @@ class CudaBatch(CudaKernel):
                                   cell_order=cell_order, device=device, boundary_mode=boundary_mode)
             views[q] = _particles_view(sc.particles, self._keep)
             bviews[q] = _boundary_view(sc.boundary, self._keep)
-            if boundary_mode == BOUNDARY_SDF:
-                sviews[q] = self._sdf_view(sc.sdf, self._keep)
+            if boundary_mode == BOUNDARY_SDF and sc.obstacle_sdf is not None:
+                sviews[q] = self._sdf_view(sc.obstacle_sdf, self._keep)
         handle = C.c_void_p()
         if boundary_mode == BOUNDARY_SDF:
             st = L.sph_batch_create_sdf(nq, prms, views, sviews, C.byref(handle))
