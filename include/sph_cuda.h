@@ -215,6 +215,15 @@ size_t sph_particle_count(const SphHandle *h);
 int sph_save_checkpoint(SphHandle *h);
 int sph_restore_checkpoint(SphHandle *h);
 
+/* The viewer's Frame message (server ws.rs:233-290) packed on the device:
+ * tag 0x02, frame_number (u64), count (u32), sim_time (f64), then per
+ * particle o = k * stride (stride = max(n / subsample_count, 1), k < count,
+ * count = min(n / stride, subsample_count)): x, y, z, temperature (f32),
+ * fluid type (u8), density ratio (u16), 0 (u8); little endian, no padding.
+ * *bytes gets the message size (21 + 20 count); out NULL only queries it.
+ * Reads back 20 bytes per sampled particle instead of the whole state. */
+int sph_pack_frame(SphHandle *h, uint32_t subsample_count, uint64_t frame_number, double sim_time,
+                   uint8_t *out, size_t cap, size_t *bytes);
 /* Multiply every particle's velocity by `factor` (no reference
  * counterpart). 0 between steps is kinetic damping: relaxing an initial
  * lattice into its equilibrium before a run. */

@@ -78,6 +78,11 @@ struct SphHandle {
   uint32_t *nbr = nullptr, *ncount = nullptr;
   // XSPH gather records: (x, y, z, m), (v + a dt/2, rho) per particle
   float4* xrec = nullptr;
+  // viewer frames (sph_pack_frame): temperature on the device (uploaded on
+  // the first call) and the packed particle records
+  float* temp_dev = nullptr;
+  uint32_t* frame_dev = nullptr;
+  size_t frame_cap = 0;
   // boundary
   float4* bpos = nullptr;
   float* bpress = nullptr;
@@ -1191,6 +1196,47 @@ int sph_scale_velocities(SphHandle* h, float factor) {
     SPH_TRY(h, cudaGetLastError());
   }
   return SPH_OK;
+}
+
+int sph_pack_frame(SphHandle* h, uint32_t subsample_count, uint64_t frame_number, double sim_time,
+                   uint8_t* out, size_t cap, size_t* bytes) {
+  if (!h || !bytes) return SPH_ERR_INVALID_ARG;
+  size_t n = (size_t)h->n;
+  size_t stride = subsample_count > 0 ? std::max<size_t>(n / subsample_count, 1) : 1;
+  size_t count = std::min<size_t>(n / stride, subsample_count);
+  size_t need = 21 + 20 * count;
+  *bytes = need;
+  if (!out) return SPH_OK;
+  if (cap < need) return set_err(h, SPH_ERR_INVALID_ARG, "frame buffer too small");
+  SPH_TRY(h, cudaSetDevice(h->dev));
+  out[0] = 0x02;
+  for (int b = 0; b < 8; ++b) out[1 + b] = (uint8_t)(frame_number >> (8 * b));
+  uint32_t c32 = (uint32_t)count;
+  for (int b = 0; b < 4; ++b) out[9 + b] = (uint8_t)(c32 >> (8 * b));
+  uint64_t tb;
+  std::memcpy(&tb, &sim_time, 8);
+  for (int b = 0; b < 8; ++b) out[13 + b] = (uint8_t)(tb >> (8 * b));
+  if (count == 0) return SPH_OK;
+  if (!h->temp_dev) {
+    float* t = nullptr;
+    cudaError_t e = dalloc(h, &t, n);
+    if (e != cudaSuccess) return cuda_status(h, e, "frame temperature");
+    SPH_TRY(h, cudaMemcpyAsync(t, h->temperature.data(), n * sizeof(float), cudaMemcpyHostToDevice, h->st));
+    h->temp_dev = t;
+  }
+  if (h->frame_cap < count) {
+    uint32_t* f = nullptr;
+    cudaError_t e = dalloc(h, &f, 5 * count);
+    if (e != cudaSuccess) return cuda_status(h, e, "frame buffer");
+    h->frame_dev = f;
+    h->frame_cap = count;
+  }
+  sph::k_pack_frame<<<grid_for(h->n, 256), 256, 0, h->st>>>(h->n, h->pos, h->velout, h->id, h->temp_dev,
+                                                           (uint32_t)stride, (uint32_t)count, h->frame_dev);
+  h->launches += 1;
+  SPH_TRY(h, cudaMemcpyAsync(out + 21, h->frame_dev, 20 * count, cudaMemcpyDeviceToHost, h->st));
+  SPH_TRY(h, cudaStreamSynchronize(h->st));
+  return check_device_flags(h);
 }
 
 int sph_synchronize(SphHandle* h) {

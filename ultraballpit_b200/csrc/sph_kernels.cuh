@@ -1343,6 +1343,34 @@ __global__ void k_metrics_final(int nparts, const double* __restrict__ part_m,
   out_me[0] = m; out_me[1] = e; *out_var = v;
 }
 
+// Particle records of the viewer's Frame message (server ws.rs:233-290):
+// particle o = k * stride (original order, k < count) becomes 20 bytes at
+// out + 20 k: x, y, z, temperature (f32), fluid type (u8), density ratio
+// (u16, (rho / rho0) * 1000 clamped to [0, 65535] and truncated; NaN gives
+// 0 like Rust's saturating cast), a zero byte; little endian, written as
+// five aligned words.
+__global__ void k_pack_frame(int n, const float4* __restrict__ pos, const float4* __restrict__ velout,
+                             const uint32_t* __restrict__ id, const float* __restrict__ temp,
+                             uint32_t stride, uint32_t count, uint32_t* __restrict__ out) {
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n) return;
+  uint32_t raw = id[s];
+  uint32_t o = raw & kIdMask;
+  if (o % stride != 0u) return;
+  uint32_t q = o / stride;
+  if (q >= count) return;
+  float4 p = pos[s];
+  bool air = (raw & kAirBit) != 0;
+  float r = (velout[s].w / (air ? kAirRho0 : kWaterRho0)) * 1000.0f;
+  uint32_t ratio = (uint32_t)fminf(fmaxf(r, 0.0f), 65535.0f);
+  uint32_t* w = out + (size_t)q * 5;
+  w[0] = __float_as_uint(p.x);
+  w[1] = __float_as_uint(p.y);
+  w[2] = __float_as_uint(p.z);
+  w[3] = __float_as_uint(temp[o]);
+  w[4] = (air ? 1u : 0u) | (ratio << 8);
+}
+
 // velocity *= factor (the end-of-step velocity the next step starts from)
 __global__ void k_scale_velocities(int n, float4* __restrict__ velout, float factor) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;

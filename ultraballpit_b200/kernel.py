@@ -44,7 +44,7 @@ EXPORTS = (
     "sph_get_launch", "sph_autotune", "sph_mlp_create", "sph_mlp_destroy", "sph_mlp_set_params",
     "sph_mlp_get_params", "sph_mlp_forward", "sph_mlp_loss_grad", "sph_mlp_train",
     "sph_set_feature_sdf", "sph_batch_set_feature_sdfs", "sph_set_closure", "sph_closure_samples",
-    "sph_interpolate", "sph_batch_create_sdf", "sph_batch_step",
+    "sph_interpolate", "sph_batch_create_sdf", "sph_batch_step", "sph_pack_frame",
 )
 
 
@@ -150,6 +150,9 @@ def load_library(path: str | None = None):
     L.sph_particle_count.restype = C.c_size_t
     L.sph_save_checkpoint.argtypes = [H]
     L.sph_restore_checkpoint.argtypes = [H]
+    L.sph_pack_frame.argtypes = [H, C.c_uint32, C.c_uint64, C.c_double, C.POINTER(C.c_uint8), C.c_size_t,
+                                 C.POINTER(C.c_size_t)]
+    L.sph_pack_frame.restype = C.c_int
     L.sph_batch_step.argtypes = [H, _FP]
     L.sph_batch_step.restype = C.c_int
     L.sph_scale_velocities.argtypes = [H, C.c_float]
@@ -393,6 +396,17 @@ class CudaKernel(SimulationKernel):
         self._check(self._lib.sph_step_profiled(self._h, float(dt), C.byref(prof)), "sph_step_profiled")
         self._cache = None
         return prof.as_dict()
+
+    def pack_frame(self, subsample_count: int, frame_number: int, sim_time: float) -> bytes:
+        """The viewer's Frame message (server ws.rs:233-290) of the current
+        state, packed on the device."""
+        size = C.c_size_t()
+        self._check(self._lib.sph_pack_frame(self._h, int(subsample_count), int(frame_number), float(sim_time),
+                                             None, 0, C.byref(size)), "sph_pack_frame")
+        buf = (C.c_uint8 * size.value)()
+        self._check(self._lib.sph_pack_frame(self._h, int(subsample_count), int(frame_number), float(sim_time),
+                                             buf, size.value, C.byref(size)), "sph_pack_frame")
+        return bytes(buf)
 
     def scale_velocities(self, factor: float) -> None:
         """velocity *= factor for every particle; 0 between steps is kinetic
