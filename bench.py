@@ -101,6 +101,8 @@ class ClockSampler:
         self.index = index
         self.rows = []
         self.proc = None
+        self.first = threading.Event()
+        self.t0 = self.t1 = None
 
     def __enter__(self):
         try:
@@ -109,17 +111,21 @@ class ClockSampler:
                  "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            self.first.wait(timeout=5.0)   # sampling is live before the timed region starts
         except Exception:
             self.proc = None
+        self.t0 = time.monotonic()
         return self
 
     def _read(self):
         for line in self.proc.stdout:
             parts = [s.strip() for s in line.split(",")]
             if len(parts) >= 9:
-                self.rows.append(parts)
+                self.rows.append([time.monotonic()] + parts)
+                self.first.set()
 
     def __exit__(self, *a):
+        self.t1 = time.monotonic()
         if self.proc:
             self.proc.terminate()
             try:
@@ -130,12 +136,16 @@ class ClockSampler:
     def summary(self):
         if not self.rows:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        inside = [r[1:] for r in self.rows if self.t0 <= r[0] <= self.t1]
+        # a region shorter than the sampling period: the samples next to it
+        rows = inside or [r[1:] for r in sorted(self.rows, key=lambda r: min(abs(r[0] - self.t0),
+                                                                           abs(r[0] - self.t1)))[:2]]
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[k] for r in self.rows for k in range(4) if r[5 + k].lower() == "active"})
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower() == "active"})
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(self.rows)}
+                "reasons": reasons, "samples": len(inside), "period_ms": 200}
 
 
 def dist_env():

@@ -224,6 +224,25 @@ int sph_restore_checkpoint(SphHandle *h);
  * Reads back 20 bytes per sampled particle instead of the whole state. */
 int sph_pack_frame(SphHandle *h, uint32_t subsample_count, uint64_t frame_number, double sim_time,
                    uint8_t *out, size_t cap, size_t *bytes);
+/* The reference runner's optimistic time stepping (orchestrator
+ * runner.rs:189-240) on the device: per step dt_safe = compute_timestep;
+ * outside a cooldown a checkpoint, a step of dt_safe * alpha, and if the
+ * maximum density variation then exceeds density_limit a restore, a step of
+ * dt_safe and `cooldown_steps` steps without optimism. Each step is one
+ * graph launch (a conditional node takes the retry branch), so the host
+ * does not wait between steps. The reference's constants are alpha 1.5,
+ * limit 0.03, cooldown 10; alpha must be positive and finite, the limit
+ * non-negative (infinity accepts every step). Counters accumulate over calls; `stats` (may be
+ * NULL) gets them after the last step. One simulation per handle; the
+ * handle's checkpoint is the runner's, left at the start of its last step. */
+typedef struct SphRunStats {
+  double sim_time;
+  uint64_t steps, accepted, rejected;
+  float last_dt;
+  uint32_t cooldown;
+} SphRunStats;
+int sph_run_optimistic(SphHandle *h, int nsteps, float alpha, float density_limit, uint32_t cooldown_steps,
+                       SphRunStats *stats);
 /* Multiply every particle's velocity by `factor` (no reference
  * counterpart). 0 between steps is kinetic damping: relaxing an initial
  * lattice into its equilibrium before a run. */

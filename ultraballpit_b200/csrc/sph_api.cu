@@ -83,6 +83,15 @@ struct SphHandle {
   float* temp_dev = nullptr;
   uint32_t* frame_dev = nullptr;
   size_t frame_cap = 0;
+  // optimistic runner (sph_run_optimistic): state on the device, one graph
+  // per parameter set, kernels per launch of its main part and retry branch
+  sph::RunState* run = nullptr;
+  float* dt_safe_dev = nullptr;
+  cudaGraphExec_t g_opt = nullptr;
+  float opt_alpha = 0.0f, opt_limit = 0.0f;
+  uint32_t opt_cool = 0;
+  int opt_kernels = 0, retry_kernels = 0;
+  unsigned long long opt_rejected_counted = 0;
   // boundary
   float4* bpos = nullptr;
   float* bpress = nullptr;
@@ -566,8 +575,10 @@ int capture(SphHandle* h, bool with_finalize, cudaGraphExec_t* out) {
 void drop_graphs(SphHandle* h) {
   if (h->g_step) cudaGraphExecDestroy(h->g_step);
   if (h->g_auto) cudaGraphExecDestroy(h->g_auto);
+  if (h->g_opt) cudaGraphExecDestroy(h->g_opt);
   h->g_step = nullptr;
   h->g_auto = nullptr;
+  h->g_opt = nullptr;
 }
 
 int check_device_flags(SphHandle* h) {
@@ -1123,16 +1134,51 @@ int sph_read_boundary_pressure(SphHandle* h, float* out, size_t nb) {
   return check_device_flags(h);
 }
 
+namespace {
+// FP64 mass / energy sums and the maximum density variation into h->me, h->var
+void enqueue_metrics(SphHandle* h) {
+  sph::k_metrics_partial<<<h->nparts, sph::kMetricThreads, 0, h->st>>>(h->k, h->n, h->pos, h->velout, h->id,
+                                                                     h->part_m, h->part_e, h->part_var);
+  sph::k_metrics_final<<<1, 32, 0, h->st>>>(h->nparts, h->part_m, h->part_e, h->part_var, h->me, h->var);
+  h->launches += 2;
+}
+
+cudaError_t ensure_ck(SphHandle* h) {
+  if (h->ck_pos) return cudaSuccess;
+  size_t n = (size_t)h->n;
+  cudaError_t e = cudaSuccess;
+  if (e == cudaSuccess) e = dalloc(h, &h->ck_pos, n);
+  if (e == cudaSuccess) e = dalloc(h, &h->ck_velout, n);
+  if (e == cudaSuccess) e = dalloc(h, &h->ck_acc, n);
+  if (e == cudaSuccess) e = dalloc(h, &h->ck_pr, n);
+  if (e == cudaSuccess) e = dalloc(h, &h->ck_slot, n);
+  return e;
+}
+
+void enqueue_save_ck(SphHandle* h) {
+  size_t n = (size_t)h->n;
+  cudaMemcpyAsync(h->ck_pos, h->pos, n * sizeof(float4), cudaMemcpyDeviceToDevice, h->st);
+  cudaMemcpyAsync(h->ck_velout, h->velout, n * sizeof(float4), cudaMemcpyDeviceToDevice, h->st);
+  cudaMemcpyAsync(h->ck_acc, h->acc, n * sizeof(float4), cudaMemcpyDeviceToDevice, h->st);
+  cudaMemcpyAsync(h->ck_pr, h->pr, n * sizeof(float), cudaMemcpyDeviceToDevice, h->st);
+  sph::k_index_ids<<<grid_for(h->n, 256), 256, 0, h->st>>>(h->n, h->id, h->ck_slot);
+  h->launches += 1;
+}
+
+void enqueue_restore_ck(SphHandle* h) {
+  sph::k_restore<<<grid_for(h->n, 256), 256, 0, h->st>>>(h->n, h->id, h->ck_slot, h->ck_pos, h->ck_velout,
+                                                        h->ck_acc, h->ck_pr, h->pos, h->velout, h->acc, h->pr);
+  h->launches += 1;
+}
+}  // namespace
+
 int sph_error_metrics(SphHandle* h, SphErrorMetrics* out) {
   if (!h || !out) return SPH_ERR_INVALID_ARG;
   SPH_TRY(h, cudaSetDevice(h->dev));
   double me[2] = {0.0, 0.0};
   float var = 0.0f;
   if (h->n > 0) {
-    sph::k_metrics_partial<<<h->nparts, sph::kMetricThreads, 0, h->st>>>(h->k, h->n, h->pos, h->velout, h->id,
-                                                                       h->part_m, h->part_e, h->part_var);
-    sph::k_metrics_final<<<1, 32, 0, h->st>>>(h->nparts, h->part_m, h->part_e, h->part_var, h->me, h->var);
-    h->launches += 2;
+    enqueue_metrics(h);
     SPH_TRY(h, cudaMemcpyAsync(me, h->me, 2 * sizeof(double), cudaMemcpyDeviceToHost, h->st));
     SPH_TRY(h, cudaMemcpyAsync(&var, h->var, sizeof(float), cudaMemcpyDeviceToHost, h->st));
     SPH_TRY(h, cudaStreamSynchronize(h->st));
@@ -1149,24 +1195,11 @@ size_t sph_particle_count(const SphHandle* h) { return h ? (size_t)h->n : 0; }
 int sph_save_checkpoint(SphHandle* h) {
   if (!h) return SPH_ERR_INVALID_ARG;
   SPH_TRY(h, cudaSetDevice(h->dev));
-  size_t n = (size_t)h->n;
-  if (!h->ck_pos) {
-    cudaError_t e = cudaSuccess;
-    if (e == cudaSuccess) e = dalloc(h, &h->ck_pos, n);
-    if (e == cudaSuccess) e = dalloc(h, &h->ck_velout, n);
-    if (e == cudaSuccess) e = dalloc(h, &h->ck_acc, n);
-    if (e == cudaSuccess) e = dalloc(h, &h->ck_pr, n);
-    if (e == cudaSuccess) e = dalloc(h, &h->ck_slot, n);
+  {
+    cudaError_t e = ensure_ck(h);
     if (e != cudaSuccess) return cuda_status(h, e, "checkpoint allocation");
   }
-  if (n) {
-    SPH_TRY(h, cudaMemcpyAsync(h->ck_pos, h->pos, n * sizeof(float4), cudaMemcpyDeviceToDevice, h->st));
-    SPH_TRY(h, cudaMemcpyAsync(h->ck_velout, h->velout, n * sizeof(float4), cudaMemcpyDeviceToDevice, h->st));
-    SPH_TRY(h, cudaMemcpyAsync(h->ck_acc, h->acc, n * sizeof(float4), cudaMemcpyDeviceToDevice, h->st));
-    SPH_TRY(h, cudaMemcpyAsync(h->ck_pr, h->pr, n * sizeof(float), cudaMemcpyDeviceToDevice, h->st));
-    sph::k_index_ids<<<grid_for(h->n, 256), 256, 0, h->st>>>(h->n, h->id, h->ck_slot);
-    h->launches += 1;
-  }
+  if (h->n) enqueue_save_ck(h);
   h->has_ck = true;
   return cuda_status(h, cudaGetLastError(), "sph_save_checkpoint");
 }
@@ -1175,16 +1208,189 @@ int sph_restore_checkpoint(SphHandle* h) {
   if (!h) return SPH_ERR_INVALID_ARG;
   if (!h->has_ck) return set_err(h, SPH_ERR_NO_CHECKPOINT, "no checkpoint saved");
   SPH_TRY(h, cudaSetDevice(h->dev));
-  if (h->n) {
-    sph::k_restore<<<grid_for(h->n, 256), 256, 0, h->st>>>(h->n, h->id, h->ck_slot, h->ck_pos, h->ck_velout,
-                                                          h->ck_acc, h->ck_pr, h->pos, h->velout, h->acc, h->pr);
-    h->launches += 1;
-  }
+  if (h->n) enqueue_restore_ck(h);
   h->has_ck = false;
   h->red_valid = false;
   h->list_valid = false;
   ensure_red(h);
   return cuda_status(h, cudaGetLastError(), "sph_restore_checkpoint");
+}
+
+namespace {
+// The optimistic step as one graph: the main part runs every time, the
+// retry branch (restore + the step with dt_safe) only when k_opt_decide
+// sets the conditional handle.
+int capture_opt(SphHandle* h, float alpha, float limit, uint32_t cool) {
+  using namespace sph;
+  cudaGraph_t g = nullptr;
+  SPH_TRY(h, cudaGraphCreate(&g, 0));
+  cudaGraphConditionalHandle retry;
+  cudaError_t e = cudaGraphConditionalHandleCreate(&retry, g, 0, cudaGraphCondAssignDefault);
+  if (e != cudaSuccess) {
+    cudaGraphDestroy(g);
+    return cuda_status(h, e, "cudaGraphConditionalHandleCreate");
+  }
+  uint64_t before = h->launches;
+  e = cudaStreamBeginCaptureToGraph(h->st, g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+  if (e != cudaSuccess) {
+    cudaGraphDestroy(g);
+    return cuda_status(h, e, "cudaStreamBeginCaptureToGraph");
+  }
+  enqueue_dt_finalize(h, h->dt_safe_dev);
+  k_opt_begin<<<1, 1, 0, h->st>>>(h->run, h->dt_safe_dev, h->dt, alpha);
+  h->launches += 1;
+  enqueue_save_ck(h);
+  enqueue_body(h, true);
+  enqueue_metrics(h);
+  k_opt_decide<<<1, 1, 0, h->st>>>(h->run, h->var, limit, cool, retry);
+  h->launches += 1;
+  e = cudaStreamEndCapture(h->st, &g);
+  h->opt_kernels = (int)(h->launches - before);
+  if (e != cudaSuccess) {
+    if (g) cudaGraphDestroy(g);
+    h->launches = before;
+    return cuda_status(h, e, "cudaStreamEndCapture");
+  }
+  // the retry branch depends on every leaf of the main part
+  size_t nn = 0;
+  cudaGraphGetNodes(g, nullptr, &nn);
+  std::vector<cudaGraphNode_t> nodes(nn), leaves;
+  cudaGraphGetNodes(g, nodes.data(), &nn);
+  for (cudaGraphNode_t nd : nodes) {
+    size_t nd_out = 0;
+    cudaGraphNodeGetDependentNodes(nd, nullptr, &nd_out);
+    if (nd_out == 0) leaves.push_back(nd);
+  }
+  cudaGraphNodeParams cp = {};
+  cp.type = cudaGraphNodeTypeConditional;
+  cp.conditional.handle = retry;
+  cp.conditional.type = cudaGraphCondTypeIf;
+  cp.conditional.size = 1;
+  cudaGraphNode_t cn;
+  e = cudaGraphAddNode(&cn, g, leaves.data(), leaves.size(), &cp);
+  if (e != cudaSuccess) {
+    cudaGraphDestroy(g);
+    h->launches = before;
+    return cuda_status(h, e, "conditional node");
+  }
+  cudaGraph_t body = cp.conditional.phGraph_out[0];
+  uint64_t mid = h->launches;
+  e = cudaStreamBeginCaptureToGraph(h->st, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+  if (e == cudaSuccess) {
+    enqueue_restore_ck(h);
+    k_opt_retry<<<1, 1, 0, h->st>>>(h->run, h->dt);
+    h->launches += 1;
+    enqueue_body(h, false);
+    k_opt_commit<<<1, 1, 0, h->st>>>(h->run);
+    h->launches += 1;
+    e = cudaStreamEndCapture(h->st, &body);
+  }
+  h->retry_kernels = (int)(h->launches - mid);
+  h->launches = before;
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&h->g_opt, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) h->g_opt = nullptr;
+  return cuda_status(h, e, "optimistic step graph");
+}
+
+// The same step through the public entry points (runner.rs:189-240 as
+// written): the first step of a handle (whose force bootstrap the reference
+// ties to its first step() call) and a step after a caller's restore.
+int opt_step_host(SphHandle* h, float alpha, float limit, uint32_t cool) {
+  sph::RunState r;
+  SPH_TRY(h, cudaMemcpyAsync(&r, h->run, sizeof(r), cudaMemcpyDeviceToHost, h->st));
+  SPH_TRY(h, cudaStreamSynchronize(h->st));
+  float dt_safe = 0.0f, used = 0.0f;
+  int st = sph_compute_timestep(h, &dt_safe);
+  if (st != SPH_OK) return st;
+  if (r.cooldown > 0u) {
+    r.cooldown -= 1u;
+    if ((st = sph_step(h, dt_safe)) != SPH_OK) return st;
+    used = dt_safe;
+  } else {
+    if ((st = sph_save_checkpoint(h)) != SPH_OK) return st;
+    float dt_try = dt_safe * alpha;
+    if ((st = sph_step(h, dt_try)) != SPH_OK) return st;
+    SphErrorMetrics m;
+    if ((st = sph_error_metrics(h, &m)) != SPH_OK) return st;
+    if (m.max_density_variation > limit) {
+      if ((st = sph_restore_checkpoint(h)) != SPH_OK) return st;
+      if ((st = sph_step(h, dt_safe)) != SPH_OK) return st;
+      used = dt_safe;
+      r.rejected += 1ull;
+      r.cooldown = cool;
+    } else {
+      used = dt_try;
+      r.accepted += 1ull;
+    }
+  }
+  r.sim_time += (double)used;
+  r.steps += 1ull;
+  r.dt_safe = dt_safe;
+  r.dt_used = used;
+  SPH_TRY(h, cudaMemcpyAsync(h->run, &r, sizeof(r), cudaMemcpyHostToDevice, h->st));
+  SPH_TRY(h, cudaStreamSynchronize(h->st));
+  h->opt_rejected_counted = r.rejected;
+  return SPH_OK;
+}
+}  // namespace
+
+int sph_run_optimistic(SphHandle* h, int nsteps, float alpha, float density_limit, uint32_t cooldown_steps,
+                       SphRunStats* stats) {
+  if (!h || nsteps < 0 || !(alpha > 0.0f) || !std::isfinite(alpha) || !(density_limit >= 0.0f))
+    return SPH_ERR_INVALID_ARG;
+  if (h->ninst != 1) return set_err(h, SPH_ERR_INVALID_ARG, "the optimistic runner steps one simulation");
+  SPH_TRY(h, cudaSetDevice(h->dev));
+  if (!h->run) {
+    cudaError_t e = dalloc(h, &h->run, 1);
+    if (e == cudaSuccess) e = dalloc(h, &h->dt_safe_dev, 1);
+    if (e == cudaSuccess) e = cudaMemsetAsync(h->run, 0, sizeof(sph::RunState), h->st);
+    if (e != cudaSuccess) return cuda_status(h, e, "runner state");
+  }
+  {
+    cudaError_t e = ensure_ck(h);
+    if (e != cudaSuccess) return cuda_status(h, e, "checkpoint allocation");
+  }
+  for (int s = 0; s < nsteps && h->n > 0; ++s) {
+    ensure_red(h);
+    if (h->needs_init || !h->list_valid) {
+      int st = opt_step_host(h, alpha, density_limit, cooldown_steps);
+      if (st != SPH_OK) return st;
+      continue;
+    }
+    if (h->g_opt && (h->opt_alpha != alpha || h->opt_limit != density_limit || h->opt_cool != cooldown_steps)) {
+      cudaGraphExecDestroy(h->g_opt);
+      h->g_opt = nullptr;
+    }
+    if (!h->g_opt) {
+      int st = capture_opt(h, alpha, density_limit, cooldown_steps);
+      if (st != SPH_OK) return st;
+      h->opt_alpha = alpha;
+      h->opt_limit = density_limit;
+      h->opt_cool = cooldown_steps;
+    }
+    SPH_TRY(h, cudaGraphLaunch(h->g_opt, h->st));
+    h->launches += h->opt_kernels;
+    h->list_valid = true;
+    h->red_valid = true;
+    h->has_ck = true;
+  }
+  sph::RunState r;
+  SPH_TRY(h, cudaMemcpyAsync(&r, h->run, sizeof(r), cudaMemcpyDeviceToHost, h->st));
+  SPH_TRY(h, cudaStreamSynchronize(h->st));
+  if (r.rejected > h->opt_rejected_counted) {  // retry branches the graphs ran
+    h->launches += (r.rejected - h->opt_rejected_counted) * (uint64_t)h->retry_kernels;
+    h->opt_rejected_counted = r.rejected;
+  }
+  if (stats) {
+    stats->sim_time = r.sim_time;
+    stats->steps = r.steps;
+    stats->accepted = r.accepted;
+    stats->rejected = r.rejected;
+    stats->last_dt = r.dt_used;
+    stats->cooldown = r.cooldown;
+  }
+  return check_device_flags(h);
 }
 
 int sph_scale_velocities(SphHandle* h, float factor) {

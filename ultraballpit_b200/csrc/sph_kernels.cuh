@@ -1371,6 +1371,53 @@ __global__ void k_pack_frame(int n, const float4* __restrict__ pos, const float4
   w[4] = (air ? 1u : 0u) | (ratio << 8);
 }
 
+// ---- optimistic time stepping (orchestrator runner.rs:189-240) ------------
+// Per step: dt_safe from the CFL maxima; outside a cooldown try
+// dt_safe * alpha with a checkpoint, and if the step left a maximum density
+// variation above the limit, restore and redo it with dt_safe, then skip
+// the optimism for `cooldown` steps. One graph per step: these kernels keep
+// the runner's state on the device and k_opt_decide selects the retry branch
+// (a conditional graph node) without a host round trip.
+struct RunState {
+  double sim_time;
+  unsigned long long steps, accepted, rejected;
+  float dt_safe, dt_used;
+  uint32_t cooldown, reject;
+};
+
+__global__ void k_opt_begin(RunState* run, const float* __restrict__ dt_safe, float* __restrict__ dt, float alpha) {
+  float ds = *dt_safe;
+  float try_dt = run->cooldown > 0u ? ds : ds * alpha;
+  run->dt_safe = ds;
+  run->dt_used = try_dt;
+  *dt = try_dt;
+}
+
+__global__ void k_opt_decide(RunState* run, const float* __restrict__ var, float limit, uint32_t cooldown,
+                             cudaGraphConditionalHandle retry) {
+  uint32_t reject = 0u;
+  if (run->cooldown > 0u) {
+    run->cooldown -= 1u;
+  } else if (*var > limit) {
+    reject = 1u;
+    run->cooldown = cooldown;
+    run->rejected += 1ull;
+  } else {
+    run->accepted += 1ull;
+  }
+  if (!reject) run->sim_time += (double)run->dt_used;
+  run->steps += 1ull;
+  run->reject = reject;
+  cudaGraphSetConditional(retry, reject);
+}
+
+__global__ void k_opt_retry(RunState* run, float* __restrict__ dt) {
+  run->dt_used = run->dt_safe;
+  *dt = run->dt_safe;
+}
+
+__global__ void k_opt_commit(RunState* run) { run->sim_time += (double)run->dt_used; }
+
 // velocity *= factor (the end-of-step velocity the next step starts from)
 __global__ void k_scale_velocities(int n, float4* __restrict__ velout, float factor) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;

@@ -44,7 +44,7 @@ EXPORTS = (
     "sph_get_launch", "sph_autotune", "sph_mlp_create", "sph_mlp_destroy", "sph_mlp_set_params",
     "sph_mlp_get_params", "sph_mlp_forward", "sph_mlp_loss_grad", "sph_mlp_train",
     "sph_set_feature_sdf", "sph_batch_set_feature_sdfs", "sph_set_closure", "sph_closure_samples",
-    "sph_interpolate", "sph_batch_create_sdf", "sph_batch_step", "sph_pack_frame",
+    "sph_interpolate", "sph_batch_create_sdf", "sph_batch_step", "sph_pack_frame", "sph_run_optimistic",
 )
 
 
@@ -83,6 +83,14 @@ class SphBoundaryView(C.Structure):
 class SphSdfView(C.Structure):
     _fields_ = [("origin", C.c_float * 3), ("cell_size", C.c_float), ("dims", C.c_uint32 * 3),
                 ("distances", _FP)]
+
+
+class SphRunStats(C.Structure):
+    _fields_ = [("sim_time", C.c_double), ("steps", C.c_uint64), ("accepted", C.c_uint64),
+                ("rejected", C.c_uint64), ("last_dt", C.c_float), ("cooldown", C.c_uint32)]
+
+    def as_dict(self) -> dict:
+        return {k: (float if k in ("sim_time", "last_dt") else int)(getattr(self, k)) for k, _ in self._fields_}
 
 
 class SphErrorMetrics(C.Structure):
@@ -155,6 +163,8 @@ def load_library(path: str | None = None):
     L.sph_pack_frame.restype = C.c_int
     L.sph_batch_step.argtypes = [H, _FP]
     L.sph_batch_step.restype = C.c_int
+    L.sph_run_optimistic.argtypes = [H, C.c_int, C.c_float, C.c_float, C.c_uint32, C.POINTER(SphRunStats)]
+    L.sph_run_optimistic.restype = C.c_int
     L.sph_scale_velocities.argtypes = [H, C.c_float]
     L.sph_scale_velocities.restype = C.c_int
     L.sph_synchronize.argtypes = [H]
@@ -407,6 +417,18 @@ class CudaKernel(SimulationKernel):
         self._check(self._lib.sph_pack_frame(self._h, int(subsample_count), int(frame_number), float(sim_time),
                                              buf, size.value, C.byref(size)), "sph_pack_frame")
         return bytes(buf)
+
+    def run_optimistic(self, nsteps: int, alpha: float = 1.5, density_limit: float = 0.03,
+                       cooldown_steps: int = 10) -> dict:
+        """``nsteps`` steps of the orchestrator's optimistic time stepping
+        (orchestrator runner.rs:189-240) on the device, one graph launch a
+        step. Returns the run's counters (sim_time, steps, accepted,
+        rejected, last_dt, cooldown), which accumulate over calls."""
+        stats = SphRunStats()
+        self._check(self._lib.sph_run_optimistic(self._h, int(nsteps), float(alpha), float(density_limit),
+                                                 int(cooldown_steps), C.byref(stats)), "sph_run_optimistic")
+        self._cache = None
+        return stats.as_dict()
 
     def scale_velocities(self, factor: float) -> None:
         """velocity *= factor for every particle; 0 between steps is kinetic
