@@ -439,6 +439,21 @@ def run_cuda_arm(args):
            "includes": "handle creation from host arrays, per step compute_timestep + step + "
                        "error_metrics, final particles() readback"}
 
+    # ---- setup_domain (domain.rs:36-402) of this box and obstacle --------
+    setup = None
+    if sc.obstacle_sdf is not None:
+        from ultraballpit_b200.kernel import setup_domain
+        from ultraballpit_b200.particles import DomainSpec
+        spec = DomainSpec(float(np.float32(WORKLOADS[args.workload]["dx"])), sc.domain_min, sc.domain_max)
+        setup_domain(spec, sc.obstacle_sdf, device=local)          # warm-up
+        t0 = time.perf_counter()
+        sp, sb = setup_domain(spec, sc.obstacle_sdf, device=local)
+        setup_s = time.perf_counter() - t0
+        setup = {"fluid": len(sp), "boundary": len(sb), "device_call_ms": setup_s * 1e3,
+                 "includes": "SDF upload, count + scan + emit kernels, both particle sets read back into "
+                             "pageable host arrays (two calls: count, then fill)"}
+        del sp, sb
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
@@ -446,6 +461,12 @@ def run_cuda_arm(args):
         cpu = {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
                "sample": f"{done} full steps of {args.workload} ({n} particles) on {threads} host threads, "
                          f"oracle tier G ({el:.1f} s)"}
+        if setup is not None:
+            from oracle import oracle as orc
+            t0 = time.perf_counter()
+            orc.setup_domain(spec, sc.obstacle_sdf)
+            setup["oracle_ms"] = (time.perf_counter() - t0) * 1e3
+            setup["oracle"] = "literal restatement of domain.rs:36-402, one host thread"
 
     rep.barrier()
     rep.close()
@@ -460,7 +481,7 @@ def run_cuda_arm(args):
                        "l2": f"inputs larger than L2 (state {state_bytes / 1e6:.0f} MB per GPU)",
                        "alpha": sc.alpha, "cell_order": "morton"},
             "clocks": clk.summary(), "gpu_launches": launches, "e2e": e2e,
-            "roofline": roofline, "cpu_baseline": cpu,
+            "roofline": roofline, "cpu_baseline": cpu, "domain_setup": setup,
         }
         print(json.dumps(line), flush=True)
 

@@ -243,6 +243,36 @@ typedef struct SphRunStats {
 } SphRunStats;
 int sph_run_optimistic(SphHandle *h, int nsteps, float alpha, float density_limit, uint32_t cooldown_steps,
                        SphRunStats *stats);
+/* ---- domain setup (orchestrator domain.rs:36-402) on the device ---- */
+#define SPH_FLUID_WATER 0
+#define SPH_FLUID_AIR 1
+#define SPH_FLUID_MIXED 2 /* y below the box's middle is water, above it air */
+/* The SimulationConfig fields setup_domain reads (config.rs:9-64). */
+typedef struct SphDomainSpec {
+  float particle_spacing;
+  float domain_min[3], domain_max[3];
+  int fluid_type; /* SPH_FLUID_* (config.rs:66-73) */
+  float initial_temperature;
+  /* bit f set: face f is Simple(Wall); f = 0..5 is x_min, x_max, y_min,
+   * y_max, z_min, z_max (BoundaryConditions::default() = 0x3f) */
+  uint32_t wall_faces;
+} SphDomainSpec;
+typedef struct SphBoundaryMut {
+  size_t n;
+  float *x, *y, *z, *mass, *nx, *ny, *nz;
+} SphBoundaryMut;
+/* setup_domain(config, sdf) (domain.rs:36-83) on `device`: the fluid
+ * particles of the lattice (domain.rs:88-160) and the boundary particles,
+ * wall layers face by face (domain.rs:162-348) then geometry layers
+ * (domain.rs:351-402), in the reference's order and bit for bit. The SDF's
+ * distances are read from host or device memory. *n_fluid / *n_boundary get
+ * the counts; with fluid and boundary both NULL nothing else happens.
+ * Otherwise each non-NULL output (host or device arrays, capacity in its n
+ * field) receives its particles; a capacity below the count returns
+ * SPH_ERR_CAPACITY. The lattice may hold at most 2^31 - 1 points. */
+int sph_setup_domain(int device, const SphDomainSpec *spec, const SphSdfView *sdf, SphParticlesMut *fluid,
+                     SphBoundaryMut *boundary, size_t *n_fluid, size_t *n_boundary);
+
 /* Multiply every particle's velocity by `factor` (no reference
  * counterpart). 0 between steps is kinetic damping: relaxing an initial
  * lattice into its equilibrium before a run. */

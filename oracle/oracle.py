@@ -91,6 +91,8 @@ def lib():
         L.orc_wall_table.argtypes = [C.c_float, fp, fp, fp]
         L.orc_wall_tables_box.restype = C.c_int
         L.orc_wall_tables_box.argtypes = [C.c_float, fp, fp, fp, fp, fp, fp]
+        L.orc_setup_domain.argtypes = [C.c_float, fp, fp, C.c_int, C.c_uint32, fp, u32p, fp, C.c_float,
+                                       C.POINTER(C.c_uint64)] + [fp] * 5 + [C.POINTER(C.c_uint8)] + [fp] * 7
         L.orc_sdf_sample_clamped.restype = C.c_float
         L.orc_sdf_sample_clamped.argtypes = [fp, u32p, fp, C.c_float, fp]
         L.orc_sdf_gradient_clamped.argtypes = [fp, u32p, fp, C.c_float, fp, fp]
@@ -312,3 +314,24 @@ class OracleKernel:
 
     def boundary_list_size(self) -> int:
         return int(lib().orc_boundary_list_size(self._h))
+
+
+def setup_domain(spec, sdf):
+    """``setup_domain(config, sdf)`` (orchestrator domain.rs:36-402) by the
+    literal restatement: (ParticleArrays, BoundaryParticles)."""
+    L = lib()
+    dims = np.asarray(sdf.dimensions, np.uint32)
+    dist = np.ascontiguousarray(sdf.distances, np.float32)
+    args = (C.c_float(spec.particle_spacing), _f3(spec.domain_min), _f3(spec.domain_max), int(spec.fluid_type),
+            int(spec.wall_faces), _fp(dist), _u32p(dims), _f3(sdf.origin), C.c_float(sdf.cell_size))
+    counts = (C.c_uint64 * 2)()
+    nul = C.POINTER(C.c_float)()
+    L.orc_setup_domain(*args, counts, nul, nul, nul, nul, nul, C.POINTER(C.c_uint8)(), *([nul] * 7))
+    n, nb = int(counts[0]), int(counts[1])
+    p = ParticleArrays.empty(n)
+    b = BoundaryParticles.from_arrays(*[np.zeros(nb, np.float32) for _ in range(7)])
+    L.orc_setup_domain(*args, counts, _fp(p.x), _fp(p.y), _fp(p.z), _fp(p.mass), _fp(p.density),
+                       p.fluid_type.ctypes.data_as(C.POINTER(C.c_uint8)),
+                       *[_fp(getattr(b, f)) for f in BOUNDARY_FIELDS])
+    p.temperature[:] = np.float32(spec.initial_temperature)
+    return p, b

@@ -1336,6 +1336,116 @@ void orc_sdf_gradient_clamped(const float* d, const uint32_t* dims, const float*
   sdf_gradient_clamped(d, dims, origin, cell, pt[0], pt[1], pt[2], out3);
 }
 
+// ---- setup_domain (orchestrator domain.rs:36-402), literally ------------
+// Loops, tests and f32 expressions as the reference writes them; results
+// appended in its order. `counts` gets (fluid, boundary); the arrays (NULL to
+// count only) must hold that many. fluid_type: 0 water, 1 air, 2 mixed;
+// wall_faces bit f = face f (x_min, x_max, y_min, y_max, z_min, z_max) is a
+// Wall. Fluid fields written: x, y, z, mass, density, type (the others are
+// push_particle's zeros and the temperature); boundary: x, y, z, mass, n.
+void orc_setup_domain(float spacing, const float* dmin, const float* dmax, int fluid_type, uint32_t wall_faces,
+                      const float* d, const uint32_t* dims, const float* origin, float cell, uint64_t* counts,
+                      float* fx, float* fy, float* fz, float* fmass, float* fdens, uint8_t* ftype, float* bx,
+                      float* by, float* bz, float* bmass_out, float* bnx, float* bny, float* bnz) {
+  const float volume = spacing * (spacing * spacing);  // powi(3) (domain.rs:43)
+  const float water_mass = 1000.0f * volume, air_mass = 1.2f * volume;
+  std::vector<float> F[5];
+  std::vector<uint8_t> T;
+  std::vector<float> B[7];
+  auto axis = [&](int a) {
+    float v = std::ceil((dmax[a] - dmin[a]) / spacing);
+    return v > 0.0f ? (size_t)v : (size_t)0;
+  };
+  size_t nx = axis(0), ny = axis(1), nz = axis(2);
+  // domain.rs:88-160
+  float center_y = (dmin[1] + dmax[1]) * 0.5f;
+  for (size_t i = 0; i < nx; ++i)
+    for (size_t j = 0; j < ny; ++j)
+      for (size_t k = 0; k < nz; ++k) {
+        float x = dmin[0] + ((float)i + 0.5f) * spacing;
+        float y = dmin[1] + ((float)j + 0.5f) * spacing;
+        float z = dmin[2] + ((float)k + 0.5f) * spacing;
+        if (x < dmin[0] || x > dmax[0] || y < dmin[1] || y > dmax[1] || z < dmin[2] || z > dmax[2]) continue;
+        float pt[3] = {x, y, z};
+        if (sdf_sample(d, dims, origin, cell, pt) < 0.0f) continue;
+        bool water = fluid_type == 0 || (fluid_type == 2 && y < center_y);
+        F[0].push_back(x);
+        F[1].push_back(y);
+        F[2].push_back(z);
+        F[3].push_back(water ? water_mass : air_mass);
+        F[4].push_back(water ? 1000.0f : 1.2f);
+        T.push_back(water ? 0 : 1);
+      }
+  float mass = fluid_type == 1 ? air_mass : water_mass;  // domain.rs:60-66
+  auto push = [&](float x, float y, float z, float a, float b, float c) {
+    B[0].push_back(x); B[1].push_back(y); B[2].push_back(z); B[3].push_back(mass);
+    B[4].push_back(a); B[5].push_back(b); B[6].push_back(c);
+  };
+  // domain.rs:189-347, face by face
+  if (wall_faces & 1u)
+    for (size_t l = 0; l < 3; ++l)
+      for (size_t j = 0; j < ny; ++j)
+        for (size_t k = 0; k < nz; ++k)
+          push(dmin[0] - ((float)l + 0.5f) * spacing, dmin[1] + ((float)j + 0.5f) * spacing,
+               dmin[2] + ((float)k + 0.5f) * spacing, 1.0f, 0.0f, 0.0f);
+  if (wall_faces & 2u)
+    for (size_t l = 0; l < 3; ++l)
+      for (size_t j = 0; j < ny; ++j)
+        for (size_t k = 0; k < nz; ++k)
+          push(dmax[0] + ((float)l + 0.5f) * spacing, dmin[1] + ((float)j + 0.5f) * spacing,
+               dmin[2] + ((float)k + 0.5f) * spacing, -1.0f, 0.0f, 0.0f);
+  if (wall_faces & 4u)
+    for (size_t l = 0; l < 3; ++l)
+      for (size_t i = 0; i < nx; ++i)
+        for (size_t k = 0; k < nz; ++k)
+          push(dmin[0] + ((float)i + 0.5f) * spacing, dmin[1] - ((float)l + 0.5f) * spacing,
+               dmin[2] + ((float)k + 0.5f) * spacing, 0.0f, 1.0f, 0.0f);
+  if (wall_faces & 8u)
+    for (size_t l = 0; l < 3; ++l)
+      for (size_t i = 0; i < nx; ++i)
+        for (size_t k = 0; k < nz; ++k)
+          push(dmin[0] + ((float)i + 0.5f) * spacing, dmax[1] + ((float)l + 0.5f) * spacing,
+               dmin[2] + ((float)k + 0.5f) * spacing, 0.0f, -1.0f, 0.0f);
+  if (wall_faces & 16u)
+    for (size_t l = 0; l < 3; ++l)
+      for (size_t i = 0; i < nx; ++i)
+        for (size_t j = 0; j < ny; ++j)
+          push(dmin[0] + ((float)i + 0.5f) * spacing, dmin[1] + ((float)j + 0.5f) * spacing,
+               dmin[2] - ((float)l + 0.5f) * spacing, 0.0f, 0.0f, 1.0f);
+  if (wall_faces & 32u)
+    for (size_t l = 0; l < 3; ++l)
+      for (size_t i = 0; i < nx; ++i)
+        for (size_t j = 0; j < ny; ++j)
+          push(dmin[0] + ((float)i + 0.5f) * spacing, dmin[1] + ((float)j + 0.5f) * spacing,
+               dmax[2] + ((float)l + 0.5f) * spacing, 0.0f, 0.0f, -1.0f);
+  // domain.rs:351-402
+  float thr = spacing * 0.5f;
+  for (size_t i = 0; i < nx; ++i)
+    for (size_t j = 0; j < ny; ++j)
+      for (size_t k = 0; k < nz; ++k) {
+        float pt[3] = {dmin[0] + ((float)i + 0.5f) * spacing, dmin[1] + ((float)j + 0.5f) * spacing,
+                       dmin[2] + ((float)k + 0.5f) * spacing};
+        float dist = sdf_sample(d, dims, origin, cell, pt);
+        if (dist > 0.0f && dist < thr) {
+          float n[3];
+          sdf_gradient(d, dims, origin, cell, pt, n);
+          for (size_t l = 0; l < 3; ++l) {
+            float off = ((float)l + 0.5f) * spacing;
+            push(pt[0] - n[0] * off, pt[1] - n[1] * off, pt[2] - n[2] * off, n[0], n[1], n[2]);
+          }
+        }
+      }
+  counts[0] = T.size();
+  counts[1] = B[0].size();
+  float* fo[5] = {fx, fy, fz, fmass, fdens};
+  for (int c = 0; c < 5; ++c)
+    if (fo[c] && !F[c].empty()) std::memcpy(fo[c], F[c].data(), F[c].size() * 4);
+  if (ftype && !T.empty()) std::memcpy(ftype, T.data(), T.size());
+  float* bo[7] = {bx, by, bz, bmass_out, bnx, bny, bnz};
+  for (int c = 0; c < 7; ++c)
+    if (bo[c] && !B[c].empty()) std::memcpy(bo[c], B[c].data(), B[c].size() * 4);
+}
+
 // ---- GridSDF ------------------------------------------------------------
 float orc_sdf_sample(const float* d, const uint32_t* dims, const float* origin, float cell,
                      const float* pt) {

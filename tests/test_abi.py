@@ -46,7 +46,9 @@ def test_struct_layouts_match_header(tmp_path):
     structs = {"SphParams": K.SphParams, "SphParticlesView": K.SphParticlesView,
                "SphParticlesMut": K.SphParticlesMut, "SphBoundaryView": K.SphBoundaryView,
                "SphSdfView": K.SphSdfView, "SphErrorMetrics": K.SphErrorMetrics,
-               "SphStepProfile": K.SphStepProfile, "SphGridInfo": K.SphGridInfo}
+               "SphStepProfile": K.SphStepProfile, "SphGridInfo": K.SphGridInfo,
+               "SphSurfaceForce": K.SphSurfaceForce, "SphBodyForce": K.SphBodyForce, "SphLaunch": K.SphLaunch,
+               "SphRunStats": K.SphRunStats, "SphDomainSpec": K.SphDomainSpec, "SphBoundaryMut": K.SphBoundaryMut}
     lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "sph_cuda.h"', "int main(void){"]
     for name, cls in structs.items():
         lines.append(f'printf("{name} %zu\\n", sizeof({name}));')

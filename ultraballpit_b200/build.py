@@ -19,8 +19,9 @@ CSRC = os.path.join(PKG, "csrc")
 LIB_DIR = os.path.join(PKG, "lib")
 LIB_PATH = os.path.join(LIB_DIR, "libsph_cuda.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-SOURCES = ["sph_api.cu", "sph_noalloc.cu", "sph_mlp.cu"]
-DEPS = ["sph_api.cu", "sph_kernels.cuh", "sph_noalloc.cu", "sph_mlp.cu", "sph_mlp.cuh"]
+SOURCES = ["sph_api.cu", "sph_noalloc.cu", "sph_mlp.cu", "sph_domain.cu"]
+DEPS = ["sph_api.cu", "sph_kernels.cuh", "sph_noalloc.cu", "sph_mlp.cu", "sph_mlp.cuh", "sph_sdf.cuh",
+        "sph_domain.cu"]
 
 
 def nvcc() -> str:

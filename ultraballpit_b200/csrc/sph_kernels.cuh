@@ -22,6 +22,7 @@
 
 #include "sph_cuda.h"
 #include "sph_mlp.cuh"
+#include "sph_sdf.cuh"
 
 namespace sph {
 
@@ -1502,26 +1503,6 @@ __global__ void k_list_neighbors(SimConst k, const float4* __restrict__ pos,
 namespace sph {
 
 // ---- force extraction (orchestrator force.rs:39-129) and body reaction ----
-
-// GridSDF::sample (geometry.rs:99-150) exactly, f32::MAX off the grid.
-__device__ __forceinline__ float sdf_sample_exact(const float* __restrict__ d, const float origin[3],
-                                                  float cell, const int dims[3], float px, float py,
-                                                  float pz) {
-  float gx = (px - origin[0]) / cell, gy = (py - origin[1]) / cell, gz = (pz - origin[2]) / cell;
-  int i0 = (int)floorf(gx), j0 = (int)floorf(gy), k0 = (int)floorf(gz);
-  if (i0 < 0 || j0 < 0 || k0 < 0) return 3.40282347e38f;
-  if (i0 + 1 >= dims[0] || j0 + 1 >= dims[1] || k0 + 1 >= dims[2]) return 3.40282347e38f;
-  float fx = gx - (float)i0, fy = gy - (float)j0, fz = gz - (float)k0;
-  size_t ny = dims[1], nz = dims[2];
-  size_t b = (size_t)i0 * ny * nz + (size_t)j0 * nz + (size_t)k0, si = ny * nz, sj = nz;
-  float c00 = d[b] * (1.0f - fz) + d[b + 1] * fz;
-  float c01 = d[b + sj] * (1.0f - fz) + d[b + sj + 1] * fz;
-  float c10 = d[b + si] * (1.0f - fz) + d[b + si + 1] * fz;
-  float c11 = d[b + si + sj] * (1.0f - fz) + d[b + si + sj + 1] * fz;
-  float c0 = c00 * (1.0f - fy) + c01 * fy;
-  float c1 = c10 * (1.0f - fy) + c11 * fy;
-  return c0 * (1.0f - fx) + c1 * fx;
-}
 
 // One warp per surface node: Shepard-averaged fluid pressure (terms sorted by
 // particle index, force.rs:88-100), then -p n dA and r x F in f32 as the

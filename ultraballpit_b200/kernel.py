@@ -44,7 +44,7 @@ EXPORTS = (
     "sph_get_launch", "sph_autotune", "sph_mlp_create", "sph_mlp_destroy", "sph_mlp_set_params",
     "sph_mlp_get_params", "sph_mlp_forward", "sph_mlp_loss_grad", "sph_mlp_train",
     "sph_set_feature_sdf", "sph_batch_set_feature_sdfs", "sph_set_closure", "sph_closure_samples",
-    "sph_interpolate", "sph_batch_create_sdf", "sph_batch_step", "sph_pack_frame", "sph_run_optimistic",
+    "sph_interpolate", "sph_batch_create_sdf", "sph_batch_step", "sph_pack_frame", "sph_run_optimistic", "sph_setup_domain",
 )
 
 
@@ -83,6 +83,15 @@ class SphBoundaryView(C.Structure):
 class SphSdfView(C.Structure):
     _fields_ = [("origin", C.c_float * 3), ("cell_size", C.c_float), ("dims", C.c_uint32 * 3),
                 ("distances", _FP)]
+
+
+class SphDomainSpec(C.Structure):
+    _fields_ = [("particle_spacing", C.c_float), ("domain_min", C.c_float * 3), ("domain_max", C.c_float * 3),
+                ("fluid_type", C.c_int), ("initial_temperature", C.c_float), ("wall_faces", C.c_uint32)]
+
+
+class SphBoundaryMut(C.Structure):
+    _fields_ = [("n", C.c_size_t)] + [(f, _FP) for f in BOUNDARY_FIELDS]
 
 
 class SphRunStats(C.Structure):
@@ -163,6 +172,10 @@ def load_library(path: str | None = None):
     L.sph_pack_frame.restype = C.c_int
     L.sph_batch_step.argtypes = [H, _FP]
     L.sph_batch_step.restype = C.c_int
+    L.sph_setup_domain.argtypes = [C.c_int, C.POINTER(SphDomainSpec), C.POINTER(SphSdfView),
+                                   C.POINTER(SphParticlesMut), C.POINTER(SphBoundaryMut), C.POINTER(C.c_size_t),
+                                   C.POINTER(C.c_size_t)]
+    L.sph_setup_domain.restype = C.c_int
     L.sph_run_optimistic.argtypes = [H, C.c_int, C.c_float, C.c_float, C.c_uint32, C.POINTER(SphRunStats)]
     L.sph_run_optimistic.restype = C.c_int
     L.sph_scale_velocities.argtypes = [H, C.c_float]
@@ -628,3 +641,30 @@ class CudaBatch(CudaKernel):
         out = ParticleArrays(**{f: getattr(p, f)[a:b].copy() for f in PARTICLE_FIELDS})
         out.fluid_type = p.fluid_type[a:b].copy()
         return out
+
+
+def setup_domain(spec, sdf: GridSDF, device: int = 0) -> tuple[ParticleArrays, BoundaryParticles]:
+    """``setup_domain(config, sdf)`` (orchestrator domain.rs:36-402) on the
+    device: the fluid lattice, the wall layers and the geometry layers, in
+    the reference's order and bit for bit. ``spec`` is a
+    ``particles.DomainSpec``."""
+    L = load_library()
+    s = SphDomainSpec(float(spec.particle_spacing), (C.c_float * 3)(*map(float, spec.domain_min)),
+                      (C.c_float * 3)(*map(float, spec.domain_max)), int(spec.fluid_type),
+                      float(spec.initial_temperature), int(spec.wall_faces))
+    keep = []
+    sv = CudaKernel._sdf_view(sdf, keep)
+    nf, nb = C.c_size_t(), C.c_size_t()
+
+    def check(st):
+        if st != SPH_OK:
+            raise SphError(st, "sph_setup_domain")
+    check(L.sph_setup_domain(int(device), C.byref(s), C.byref(sv), None, None, C.byref(nf), C.byref(nb)))
+    p = ParticleArrays.empty(nf.value)
+    b = BoundaryParticles.from_arrays(*[np.zeros(nb.value, np.float32) for _ in range(7)])
+    pm = SphParticlesMut(nf.value, *[_fp(getattr(p, f)) for f in PARTICLE_FIELDS],
+                         p.fluid_type.ctypes.data_as(C.POINTER(C.c_uint8)))
+    bm = SphBoundaryMut(nb.value, *[_fp(getattr(b, f)) for f in BOUNDARY_FIELDS])
+    check(L.sph_setup_domain(int(device), C.byref(s), C.byref(sv), C.byref(pm), C.byref(bm), C.byref(nf),
+                             C.byref(nb)))
+    return p, b

@@ -158,3 +158,29 @@ class GridSDF:
         nx, ny, nz = self.dimensions
         if self.distances.shape != (nx * ny * nz,):
             raise ValueError("distances must have nx*ny*nz entries")
+
+
+FLUID_WATER, FLUID_AIR, FLUID_MIXED = 0, 1, 2
+FACES = ("x_min", "x_max", "y_min", "y_max", "z_min", "z_max")
+
+
+@dataclass
+class DomainSpec:
+    """The ``SimulationConfig`` fields ``setup_domain`` reads
+    (``orchestrator/src/config.rs:9-64``): the particle spacing, the domain
+    box, the fluid type (``config.rs:66-73``: water, air, or mixed = water
+    below the box's middle in y, air above), the initial temperature, and
+    which faces are ``Simple(Wall)`` (bit f of ``wall_faces`` for face
+    ``FACES[f]``; the default has all six)."""
+
+    particle_spacing: float
+    domain_min: tuple
+    domain_max: tuple
+    fluid_type: int = FLUID_WATER
+    initial_temperature: float = 293.15
+    wall_faces: int = 0x3F
+
+    @staticmethod
+    def faces_mask(walls) -> int:
+        """Mask of the faces named in ``walls`` (names from ``FACES``)."""
+        return sum(1 << FACES.index(f) for f in walls)
