@@ -74,7 +74,7 @@ struct SphHandle {
   uint32_t *rank_of_lin = nullptr, *lin_of_rank = nullptr;
   uint2* ctab = nullptr;
   int nbsum = 0;
-  // neighbour lists recorded by k_density: nbr[c * n + i], count per particle
+  // neighbour lists recorded by k_density (chunked, sph::nbr_index), count per particle
   uint32_t *nbr = nullptr, *ncount = nullptr;
   // XSPH gather records: (x, y, z, m), (v + a dt/2, rho) per particle
   float4* xrec = nullptr;
@@ -457,11 +457,11 @@ void enqueue_density_only(SphHandle* h) {
   dispatch(h, false, [&](auto kp) {
     using KPT = decltype(kp);
     if (h->cl_mode)
-      k_density<KPT, 1><<<grid_for(h->n, bs), bs, 0, h->st>>>(kp, h->n, h->dt, h->pos, h->rv, h->id, h->ctab,
+      k_density<KPT, 1><<<grid_for(h->n, bs), bs, bs * kNbrChunk * sizeof(uint32_t), h->st>>>(kp, h->n, h->dt, h->pos, h->rv, h->id, h->ctab,
                                                             h->bc_start, h->bc_list, h->bpos, h->rf, h->pr,
                                                             h->err, h->nbr, h->ncount, h->sdf, h->wall_tab, cb);
     else
-      k_density<KPT, 0><<<grid_for(h->n, bs), bs, 0, h->st>>>(kp, h->n, h->dt, h->pos, h->rv, h->id, h->ctab,
+      k_density<KPT, 0><<<grid_for(h->n, bs), bs, bs * kNbrChunk * sizeof(uint32_t), h->st>>>(kp, h->n, h->dt, h->pos, h->rv, h->id, h->ctab,
                                                             h->bc_start, h->bc_list, h->bpos, h->rf, h->pr,
                                                             h->err, h->nbr, h->ncount, h->sdf, h->wall_tab, cb);
   });

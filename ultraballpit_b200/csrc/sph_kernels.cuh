@@ -33,10 +33,11 @@ constexpr float kAirRho0 = 1.204f;     // eos.rs:10
 constexpr int kAdamiCap = 256;         // fluid terms per boundary particle
 constexpr int kCellCap = 4096;         // particles per cell for the id ranking
 constexpr uint32_t kNbrCap = 128;      // listed neighbours per particle
+constexpr uint32_t kNbrChunk = 8;      // list entries per 32-byte chunk
 // The neighbour kernels are latency-bound on gathered loads, so occupancy
-// pays more than registers: k_xsph_drift is capped at 40 registers,
-// k_density and k_forces at 48 (__maxnreg__ below; at 2M particles the
-// step is 10 % faster than with the compiler's 58-64, same results).
+// pays more than registers: k_density, k_forces and k_xsph_drift are capped
+// at 48 registers (__maxnreg__ below; measured at 2M particles against the
+// compiler's 58-64 and against caps of 40 and 56, same results).
 
 enum : uint32_t { kFlagDelta = 1, kFlagXsph = 2, kFlagRepulsion = 4, kFlagClamp = 8 };
 enum : uint32_t { kErrCellCap = 1, kErrAdamiCap = 2 };
@@ -415,8 +416,121 @@ __device__ __forceinline__ void for_each_neighbor(float px, float py, float pz, 
   }
 }
 
+// Packed f32x2 arithmetic (sm_100): two IEEE f32 operations per instruction,
+// each rounded exactly as its scalar form (explicit .rn, never contracted).
+__device__ __forceinline__ unsigned long long f2_pack(float a, float b) {
+  unsigned long long r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));
+  return r;
+}
+__device__ __forceinline__ void f2_unpack(unsigned long long v, float& a, float& b) {
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(v));
+}
+__device__ __forceinline__ unsigned long long f2_sub(unsigned long long a, unsigned long long b) {
+  unsigned long long r;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
+__device__ __forceinline__ unsigned long long f2_mul(unsigned long long a, unsigned long long b) {
+  unsigned long long r;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
+__device__ __forceinline__ unsigned long long f2_add(unsigned long long a, unsigned long long b) {
+  unsigned long long r;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
+// ((px - x)^2 + (py - y)^2) + (pz - z)^2 of two candidates at once, rounded
+// as the reference's scalar expression.
+__device__ __forceinline__ void dist2_pair(unsigned long long X, unsigned long long Y, unsigned long long Z,
+                                           const float4& a, const float4& b, float& da, float& db) {
+  unsigned long long dx = f2_sub(X, f2_pack(a.x, b.x));
+  unsigned long long dy = f2_sub(Y, f2_pack(a.y, b.y));
+  unsigned long long dz = f2_sub(Z, f2_pack(a.z, b.z));
+  f2_unpack(f2_add(f2_add(f2_mul(dx, dx), f2_mul(dy, dy)), f2_mul(dz, dz)), da, db);
+}
+
+// The visit of for_each_neighbor reduced to the support test, for recording:
+// rec(slot, ok) for every candidate in the same order, ok = in support and
+// not `self`. Calling rec for every candidate (not only the kept ones) lets
+// the caller record without a divergent branch per candidate.
+template <class R>
+__device__ __forceinline__ void scan_support(float px, float py, float pz, int self,
+                                             const float4* __restrict__ pos, const uint2* __restrict__ ctab,
+                                             const SimConst& k, R&& rec) {
+  int cx = axis_cell(px, k.gmin[0], k.cell, k.dims[0]);
+  int cy = axis_cell(py, k.gmin[1], k.cell, k.dims[1]);
+  int cz = axis_cell(pz, k.gmin[2], k.cell, k.dims[2]);
+  const float margin = 1.0e-5f * k.cell + 1.0e-6f;  // as for_each_neighbor
+  float lo2[3], hi2[3];
+  {
+    float p3[3] = {px, py, pz};
+    int c3[3] = {cx, cy, cz};
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      float face = k.gmin[a] + (float)c3[a] * k.cell;
+      float dl = fmaxf(p3[a] - face - margin, 0.0f);
+      float dh = fmaxf(face + k.cell - p3[a] - margin, 0.0f);
+      lo2[a] = dl * dl;
+      hi2[a] = dh * dh;
+    }
+  }
+  const unsigned long long X = f2_pack(px, px), Y = f2_pack(py, py), Z = f2_pack(pz, pz);
+  const float r2 = k.radius_sq;
+  for (int dz = -1; dz <= 1; ++dz) {
+    int nz = cz + dz;
+    if (nz < 0 || nz >= k.dims[2]) continue;
+    float ez = dz < 0 ? lo2[2] : (dz > 0 ? hi2[2] : 0.0f);
+    for (int dy = -1; dy <= 1; ++dy) {
+      int ny = cy + dy;
+      if (ny < 0 || ny >= k.dims[1]) continue;
+      float ey = ez + (dy < 0 ? lo2[1] : (dy > 0 ? hi2[1] : 0.0f));
+      if (ey > r2) continue;
+      int row = (ny + nz * k.dims[1]) * k.dims[0];
+      for (int dx = -1; dx <= 1; ++dx) {
+        int nx = cx + dx;
+        if (nx < 0 || nx >= k.dims[0]) continue;
+        if (ey + (dx < 0 ? lo2[0] : (dx > 0 ? hi2[0] : 0.0f)) > r2) continue;
+        uint2 se = __ldg(&ctab[k.coff + row + nx]);
+        int end = (int)(se.x + se.y);
+        int s = (int)se.x;
+        for (; s + 3 < end; s += 4) {
+          float4 q0 = __ldg(&pos[s]), q1 = __ldg(&pos[s + 1]), q2 = __ldg(&pos[s + 2]), q3 = __ldg(&pos[s + 3]);
+          float d0, d1, d2, d3;
+          dist2_pair(X, Y, Z, q0, q1, d0, d1);
+          dist2_pair(X, Y, Z, q2, q3, d2, d3);
+          rec(s, d0 <= r2 && s != self);
+          rec(s + 1, d1 <= r2 && s + 1 != self);
+          rec(s + 2, d2 <= r2 && s + 2 != self);
+          rec(s + 3, d3 <= r2 && s + 3 != self);
+        }
+        for (; s < end; ++s) {
+          float4 q = __ldg(&pos[s]);
+          float ax = px - q.x, ay = py - q.y, az = pz - q.z;
+          rec(s, ax * ax + ay * ay + az * az <= r2 && s != self);
+        }
+      }
+    }
+  }
+}
+
+// Neighbour lists: entry c of slot i lies in chunk c / 8 of the slot, and the
+// chunks of consecutive slots lie side by side: nbr[((c / 8) n + i) 8 + c % 8].
+// k_density writes each chunk as one whole 32-byte sector (its entries are
+// staged in shared memory); entry-by-entry stores across a warp scatter into
+// partial sectors and cost more than the 27-cell scan itself. The replays read
+// two entries at a time.
+__device__ __forceinline__ size_t nbr_index(uint32_t c, int n, int i) {
+  return ((size_t)(c / kNbrChunk) * (size_t)n + (size_t)i) * kNbrChunk + (c % kNbrChunk);
+}
+// entries c and c + 1 of slot i, c even (one 8-byte load)
+__device__ __forceinline__ uint2 nbr_pair(const uint32_t* __restrict__ nbr, uint32_t c, int n, int i) {
+  return __ldg(reinterpret_cast<const uint2*>(nbr + nbr_index(c, n, i)));
+}
+
 // Same visit as for_each_neighbor, replayed from the neighbour list that
-// k_density recorded on this grid (slots in visit order, nbr[c * n + i]).
+// k_density recorded on this grid (slots in visit order, see nbr_index).
 // Particles whose list overflowed kNbrCap, and calls without a list, scan.
 template <class F>
 __device__ __forceinline__ void visit_neighbors(int i, int n, float px, float py, float pz,
@@ -430,16 +544,24 @@ __device__ __forceinline__ void visit_neighbors(int i, int n, float px, float py
     // two neighbours per iteration: both list entries and both positions are
     // loaded before either is used (same order of f calls)
     uint32_t c = 0;
-    for (; c + 1 < cnt; c += 2) {
-      int s0 = (int)__ldg(&nbr[(size_t)c * n + i]), s1 = (int)__ldg(&nbr[(size_t)(c + 1) * n + i]);
+    auto pair = [&](int s0, int s1) {
       float4 p0 = __ldg(&pos[s0]), p1 = __ldg(&pos[s1]);
       float ax = px - p0.x, ay = py - p0.y, az = pz - p0.z;
       f(s0, p0, ax, ay, az, ax * ax + ay * ay + az * az);
       float bx = px - p1.x, by = py - p1.y, bz = pz - p1.z;
       f(s1, p1, bx, by, bz, bx * bx + by * by + bz * bz);
+    };
+    for (; c + 3 < cnt; c += 4) {
+      uint4 e = __ldg(reinterpret_cast<const uint4*>(nbr + nbr_index(c, n, i)));
+      pair((int)e.x, (int)e.y);
+      pair((int)e.z, (int)e.w);
+    }
+    for (; c + 1 < cnt; c += 2) {
+      uint2 e = nbr_pair(nbr, c, n, i);
+      pair((int)e.x, (int)e.y);
     }
     if (c < cnt) {
-      int s = (int)__ldg(&nbr[(size_t)c * n + i]);
+      int s = (int)__ldg(&nbr[nbr_index(c, n, i)]);
       float4 pj = __ldg(&pos[s]);
       float ddx = px - pj.x, ddy = py - pj.y, ddz = pz - pj.z;
       f(s, pj, ddx, ddy, ddz, ddx * ddx + ddy * ddy + ddz * ddz);
@@ -481,7 +603,7 @@ k_xsph_prep(KP kp, int n, const float* __restrict__ dtp, const float4* __restric
 // (neighbor.rs:89-101) into a rank-indexed histogram. Reads the sorted state,
 // writes the unsorted "U" arrays in the same slot order.
 template <class KP>
-__global__ void __maxnreg__(40)
+__global__ void __maxnreg__(48)
 k_xsph_drift(KP kp, int n, const float* __restrict__ dtp, const float4* __restrict__ pos,
              const float4* __restrict__ velout, const float4* __restrict__ acc, const float4* __restrict__ rec,
              const uint32_t* __restrict__ id, const uint2* __restrict__ ctab,
@@ -517,17 +639,25 @@ k_xsph_drift(KP kp, int n, const float* __restrict__ dtp, const float4* __restri
     if (cnt <= kNbrCap) {
       // one 32-byte record per neighbour, two neighbours in flight
       uint32_t c = 0;
-      for (; c + 1 < cnt; c += 2) {
-        int s0 = (int)__ldg(&nbr[(size_t)c * n + i]), s1 = (int)__ldg(&nbr[(size_t)(c + 1) * n + i]);
+      auto pair = [&](int s0, int s1) {
         float4 p0 = __ldg(&rec[2 * s0]), h0 = __ldg(&rec[2 * s0 + 1]);
         float4 p1 = __ldg(&rec[2 * s1]), h1 = __ldg(&rec[2 * s1 + 1]);
         float ax = pi.x - p0.x, ay = pi.y - p0.y, az = pi.z - p0.z;
         term(p0, h0, ax, ay, az, ax * ax + ay * ay + az * az);
         float bx = pi.x - p1.x, by = pi.y - p1.y, bz = pi.z - p1.z;
         term(p1, h1, bx, by, bz, bx * bx + by * by + bz * bz);
+      };
+      for (; c + 3 < cnt; c += 4) {
+        uint4 e = __ldg(reinterpret_cast<const uint4*>(nbr + nbr_index(c, n, i)));
+        pair((int)e.x, (int)e.y);
+        pair((int)e.z, (int)e.w);
+      }
+      for (; c + 1 < cnt; c += 2) {
+        uint2 e = nbr_pair(nbr, c, n, i);
+        pair((int)e.x, (int)e.y);
       }
       if (c < cnt) {
-        int s = (int)__ldg(&nbr[(size_t)c * n + i]);
+        int s = (int)__ldg(&nbr[nbr_index(c, n, i)]);
         float4 pj = __ldg(&rec[2 * s]), vh = __ldg(&rec[2 * s + 1]);
         float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
         term(pj, vh, dx, dy, dz, dx * dx + dy * dy + dz * dz);
@@ -751,13 +881,27 @@ k_density(KP kp, int n, const float* __restrict__ dtp, const float4* __restrict_
   float rho = pi.w * k.norm_h3;
   float diff_sum = 0.0f;
   bool delta = (k.flags & kFlagDelta) != 0;
-  // Phase 1: the 27-cell scan only records in-support slots, in visit order.
+  // Phase 1: the 27-cell scan only records in-support slots, in visit order;
+  // entry j of the open chunk is staged at stage[j * blockDim.x] (this
+  // thread's column of the block's dynamic shared memory) and each full chunk
+  // goes out as one 32-byte store.
   uint32_t listed = 0;
-  for_each_neighbor(pi.x, pi.y, pi.z, i, pos, ctab, k,
-                    [&](int s, const float4&, float, float, float, float) {
-                      if (listed < kNbrCap) nbr[(size_t)listed * n + i] = (uint32_t)s;
-                      ++listed;
-                    });
+  extern __shared__ uint32_t s_stage[];
+  uint32_t* stage = s_stage + threadIdx.x;
+  const unsigned bsz = blockDim.x;
+  auto flush = [&](uint32_t chunk) {
+    uint4* dst = reinterpret_cast<uint4*>(nbr + ((size_t)chunk * (size_t)n + (size_t)i) * kNbrChunk);
+    dst[0] = make_uint4(stage[0], stage[bsz], stage[2 * bsz], stage[3 * bsz]);
+    dst[1] = make_uint4(stage[4 * bsz], stage[5 * bsz], stage[6 * bsz], stage[7 * bsz]);
+  };
+  scan_support(pi.x, pi.y, pi.z, i, pos, ctab, k, [&](int s, bool ok) {
+    stage[(listed % kNbrChunk) * bsz] = (uint32_t)s;  // kept only if ok advances `listed`
+    if (ok) {
+      if (listed % kNbrChunk == kNbrChunk - 1 && listed < kNbrCap) flush(listed / kNbrChunk);
+      ++listed;
+    }
+  });
+  if (listed < kNbrCap && listed % kNbrChunk != 0) flush(listed / kNbrChunk);  // the open chunk
   ncount[i] = listed;
   // Phase 2: density and delta-SPH terms over the list, same order.
   auto term = [&](int s, const float4& pj, float dx, float dy, float dz, float d2) {
@@ -777,7 +921,8 @@ k_density(KP kp, int n, const float* __restrict__ dtp, const float4* __restrict_
   if (listed <= kNbrCap) {
     uint32_t c = 0;
     for (; c + 1 < listed; c += 2) {
-      int s0 = (int)nbr[(size_t)c * n + i], s1 = (int)nbr[(size_t)(c + 1) * n + i];
+      uint2 e = *reinterpret_cast<const uint2*>(nbr + nbr_index(c, n, i));  // written above by this thread
+      int s0 = (int)e.x, s1 = (int)e.y;
       float4 p0 = __ldg(&pos[s0]), p1 = __ldg(&pos[s1]);
       float ax = pi.x - p0.x, ay = pi.y - p0.y, az = pi.z - p0.z;
       term(s0, p0, ax, ay, az, ax * ax + ay * ay + az * az);
@@ -785,7 +930,7 @@ k_density(KP kp, int n, const float* __restrict__ dtp, const float4* __restrict_
       term(s1, p1, bx, by, bz, bx * bx + by * by + bz * bz);
     }
     if (c < listed) {
-      int s = (int)nbr[(size_t)c * n + i];
+      int s = (int)nbr[nbr_index(c, n, i)];
       float4 pj = __ldg(&pos[s]);
       float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
       term(s, pj, dx, dy, dz, dx * dx + dy * dy + dz * dz);
