@@ -479,7 +479,7 @@ def run_cuda_arm(args):
             "config": {"workload": args.workload, "particles_per_gpu": n, "boundary_particles": len(sc.boundary),
                        "parallelism": f"replicas{world}", "dt": "device CFL each step",
                        "l2": f"inputs larger than L2 (state {state_bytes / 1e6:.0f} MB per GPU)",
-                       "alpha": sc.alpha, "cell_order": "morton"},
+                       "alpha": sc.alpha, "cell_order": "rows"},
             "clocks": clk.summary(), "gpu_launches": launches, "e2e": e2e,
             "roofline": roofline, "cpu_baseline": cpu, "domain_setup": setup,
         }

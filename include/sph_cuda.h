@@ -57,7 +57,9 @@ typedef enum SphBoundaryMode {
 
 typedef enum SphCellOrder {
   SPH_CELL_ORDER_MORTON = 0, /* particles stored by (30-bit Morton cell rank, id) */
-  SPH_CELL_ORDER_LINEAR = 1  /* particles stored by (linear cell hash, id): the reference sorted_indices */
+  SPH_CELL_ORDER_LINEAR = 1, /* particles stored by (linear cell hash, id): the reference sorted_indices */
+  SPH_CELL_ORDER_ROWS = 2    /* the cells of each x-row stored consecutively, the rows in Morton order
+                                over (y, z): a neighbourhood's three cells of a row are one range */
 } SphCellOrder;
 
 /* Stage switches; SPH_FLAGS_REFERENCE keeps every reference stage on

@@ -37,7 +37,7 @@ def test_library_exports_every_header_symbol(lib):
 def test_params_default(lib):
     p = K.default_params()
     assert p.alpha == 1.0 and p.beta == 2.0
-    assert p.flags == K.FLAGS_REFERENCE and p.cell_order == K.CELL_ORDER_MORTON
+    assert p.flags == K.FLAGS_REFERENCE and p.cell_order == K.CELL_ORDER_ROWS
     assert p.boundary_mode == K.BOUNDARY_PARTICLES
 
 

@@ -11,7 +11,7 @@ import pytest
 
 from oracle import oracle as orc
 from ultraballpit_b200 import domain
-from ultraballpit_b200.kernel import CELL_ORDER_LINEAR, CELL_ORDER_MORTON, CudaKernel, SphError
+from ultraballpit_b200.kernel import CELL_ORDER_LINEAR, CELL_ORDER_MORTON, CELL_ORDER_ROWS, CudaKernel, SphError
 from ultraballpit_b200.particles import BoundaryParticles, ParticleArrays
 
 pytestmark = pytest.mark.gpu
@@ -55,13 +55,28 @@ def _grid_vs_oracle(sc, order):
     if order == CELL_ORDER_LINEAR:
         np.testing.assert_array_equal(g["cell_start"], o["offsets"])
         np.testing.assert_array_equal(g["slot_id"], o["sorted"])
+    elif order == CELL_ORDER_ROWS:
+        # cells ranked by (Morton code of (cy, cz)) * nx + cx; slots by (rank, id)
+        nx, ny, nz = o["dims"]
+        lin = np.arange(nx * ny * nz, dtype=np.int64)
+        cx, cy, cz = lin % nx, (lin // nx) % ny, lin // (nx * ny)
+        spread = lambda v: sum(((v >> b) & 1) << (2 * b) for b in range(21))
+        key = (spread(cy) | (spread(cz) << 1)) * nx + cx
+        rank_of_lin = np.empty_like(lin)
+        rank_of_lin[np.argsort(key, kind="stable")] = lin.copy()  # rank of each linear cell (lin is 0..N-1)
+        counts_by_rank = np.zeros(len(lin), np.int64)
+        counts_by_rank[rank_of_lin] = o["counts"]
+        start_by_rank = np.cumsum(counts_by_rank) - counts_by_rank
+        np.testing.assert_array_equal(g["cell_start"], start_by_rank[rank_of_lin].astype(np.uint32))
+        prank = rank_of_lin[o["cell_idx"].astype(np.int64)]
+        np.testing.assert_array_equal(g["slot_id"], np.lexsort((np.arange(len(prank)), prank)).astype(np.uint32))
     else:
         np.testing.assert_array_equal(g["cell_start"], o["morton_offsets"])
         np.testing.assert_array_equal(g["slot_id"], o["morton_perm"])
     return gpu, o
 
 
-@pytest.mark.parametrize("order", [CELL_ORDER_MORTON, CELL_ORDER_LINEAR])
+@pytest.mark.parametrize("order", [CELL_ORDER_MORTON, CELL_ORDER_LINEAR, CELL_ORDER_ROWS])
 def test_grid_bit_exact_dam_break(order):
     _grid_vs_oracle(domain.dam_break(0.004, seed=11, with_sdf=False), order)
 
@@ -71,7 +86,7 @@ def _custom(x, y, z, dmin=(0, 0, 0), dmax=(1, 1, 1), h=0.05):
     return domain.Scenario("custom", p, BoundaryParticles(), h, (0, 0, -9.81), 20.0, 0.25, 0.0, dmin, dmax)
 
 
-@pytest.mark.parametrize("order", [CELL_ORDER_MORTON, CELL_ORDER_LINEAR])
+@pytest.mark.parametrize("order", [CELL_ORDER_MORTON, CELL_ORDER_LINEAR, CELL_ORDER_ROWS])
 def test_grid_adversarial(order):
     rng = np.random.default_rng(5)
     cell = np.float32(0.1)
@@ -177,15 +192,23 @@ def test_checkpoint_restore_matches_oracle():
     assert_same(gpu.particles(), cpu.particles())
 
 
-def test_linear_and_morton_layouts_give_identical_physics():
+def test_cell_orders_give_identical_physics():
+    """Morton, linear and row orders (the latter two scan a row's cells as one
+    range) give the same steps bit for bit, also against the oracle."""
     sc = small_dam_break(seed=6)
-    a = CudaKernel(*sc.kernel_args(), alpha=sc.alpha, cell_order=CELL_ORDER_MORTON)
-    b = CudaKernel(*sc.kernel_args(), alpha=sc.alpha, cell_order=CELL_ORDER_LINEAR)
+    ks = [CudaKernel(*sc.kernel_args(), alpha=sc.alpha, cell_order=o)
+          for o in (CELL_ORDER_MORTON, CELL_ORDER_LINEAR, CELL_ORDER_ROWS)]
+    cpu = orc.OracleKernel(*sc.kernel_args(), alpha=sc.alpha, beta=sc.beta, tier=1, threads=8, pow_mode=1)
     for _ in range(10):
-        dt = a.compute_timestep()
-        a.step(dt)
-        b.step(dt)
-    assert_same(a.particles(), b.particles())
+        dt = ks[0].compute_timestep()
+        for k in ks:
+            k.step(dt)
+        cpu.step(dt)
+    for k in ks[1:]:
+        assert_same(ks[0].particles(), k.particles())
+    assert_same(ks[2].particles(), cpu.particles())
+    with pytest.raises(SphError):
+        CudaKernel(*sc.kernel_args(), alpha=sc.alpha, cell_order=3)
 
 
 def test_profiled_step_equals_graph_step():

@@ -172,6 +172,11 @@ uint64_t spread21(uint64_t v) {
   for (int b = 0; b < 21; ++b) r |= ((v >> b) & 1ull) << (3 * b);
   return r;
 }
+uint64_t spread2(uint64_t v) {  // 21 bits to every second bit
+  uint64_t r = 0;
+  for (int b = 0; b < 21; ++b) r |= ((v >> b) & 1ull) << (2 * b);
+  return r;
+}
 
 // Largest float t with sqrtf(t) < s (sqrtf is correctly rounded on host and
 // device, and monotone), so that sqrtf(d2) < s  <=>  d2 <= t.
@@ -617,6 +622,9 @@ int check_views(const SphParams& P, const SphParticlesView* pv, const SphBoundar
   for (int a = 0; a < 3; ++a)
     if (!(P.domain_max[a] > P.domain_min[a])) return SPH_ERR_INVALID_ARG;
   if (pv->n > 0x7fffffffull) return SPH_ERR_INVALID_ARG;
+  if (P.cell_order != SPH_CELL_ORDER_MORTON && P.cell_order != SPH_CELL_ORDER_LINEAR &&
+      P.cell_order != SPH_CELL_ORDER_ROWS)
+    return SPH_ERR_INVALID_ARG;
   if (pv->n > 0 && (!pv->x || !pv->y || !pv->z || !pv->vx || !pv->vy || !pv->vz || !pv->ax || !pv->ay ||
                     !pv->az || !pv->density || !pv->pressure || !pv->mass || !pv->temperature ||
                     !pv->fluid_type))
@@ -722,6 +730,7 @@ int create_impl(int ninst, const SphParams* PP, const SphParticlesView* pvs,
     }
     if (C + Cq > (1ull << 30)) return fail(SPH_ERR_INVALID_ARG);
     SimConst k = make_const(P, dims);
+    k.rows = P.cell_order == SPH_CELL_ORDER_LINEAR || P.cell_order == SPH_CELL_ORDER_ROWS;
     k.inst = q;
     k.coff = (int)C;
     k.cfl = P.cfl_number;
@@ -747,8 +756,9 @@ int create_impl(int ninst, const SphParams* PP, const SphParticlesView* pvs,
       for (uint32_t cy = 0; cy < dims[1]; ++cy)
         for (uint32_t cx = 0; cx < dims[0]; ++cx) {
           uint32_t lin = cx + cy * dims[0] + cz * dims[0] * dims[1];
-          uint64_t key = P.cell_order == SPH_CELL_ORDER_LINEAR
-                             ? lin
+          uint64_t key = P.cell_order == SPH_CELL_ORDER_LINEAR ? lin
+                         : P.cell_order == SPH_CELL_ORDER_ROWS
+                             ? (spread2(cy) | (spread2(cz) << 1)) * dims[0] + cx
                              : (spread21(cx) | (spread21(cy) << 1) | (spread21(cz) << 2));
           cells[lin] = {key, lin};
         }
@@ -919,7 +929,7 @@ void sph_params_default(SphParams* p) {
   p->alpha = 1.0f;
   p->beta = 2.0f;
   p->boundary_mode = SPH_BOUNDARY_PARTICLES;
-  p->cell_order = SPH_CELL_ORDER_MORTON;
+  p->cell_order = SPH_CELL_ORDER_ROWS;
   p->flags = SPH_FLAGS_REFERENCE;
   p->device = 0;
   p->cfl_number = 0.25f;

@@ -79,6 +79,7 @@ struct SimConst {
   // its cells in the global cell tables (0 for a single simulation)
   int inst;
   int coff;
+  int rows;  // the cells of an x-row are consecutive in the particle order
   float cfl;
   // geometry SDF for the closure features (boundary-particle mode) or the
   // SDF walls, at sdf_off in the device SDF array
@@ -487,14 +488,8 @@ __device__ __forceinline__ void scan_support(float px, float py, float pz, int s
       if (ny < 0 || ny >= k.dims[1]) continue;
       float ey = ez + (dy < 0 ? lo2[1] : (dy > 0 ? hi2[1] : 0.0f));
       if (ey > r2) continue;
-      int row = (ny + nz * k.dims[1]) * k.dims[0];
-      for (int dx = -1; dx <= 1; ++dx) {
-        int nx = cx + dx;
-        if (nx < 0 || nx >= k.dims[0]) continue;
-        if (ey + (dx < 0 ? lo2[0] : (dx > 0 ? hi2[0] : 0.0f)) > r2) continue;
-        uint2 se = __ldg(&ctab[k.coff + row + nx]);
-        int end = (int)(se.x + se.y);
-        int s = (int)se.x;
+      int row = k.coff + (ny + nz * k.dims[1]) * k.dims[0];
+      auto range = [&](int s, int end) {
         for (; s + 3 < end; s += 4) {
           float4 q0 = __ldg(&pos[s]), q1 = __ldg(&pos[s + 1]), q2 = __ldg(&pos[s + 2]), q3 = __ldg(&pos[s + 3]);
           float d0, d1, d2, d3;
@@ -509,6 +504,23 @@ __device__ __forceinline__ void scan_support(float px, float py, float pz, int s
           float4 q = __ldg(&pos[s]);
           float ax = px - q.x, ay = py - q.y, az = pz - q.z;
           rec(s, ax * ax + ay * ay + az * az <= r2 && s != self);
+        }
+      };
+      if (k.rows) {
+        // the row's surviving cells are consecutive (the home column always
+        // survives once the row does), and so are their particles: one range
+        // in the same order as three cell visits
+        int xa = (cx > 0 && ey + lo2[0] <= r2) ? cx - 1 : cx;
+        int xb = (cx + 1 < k.dims[0] && ey + hi2[0] <= r2) ? cx + 1 : cx;
+        uint2 sa = __ldg(&ctab[row + xa]), sb = __ldg(&ctab[row + xb]);
+        range((int)sa.x, (int)(sb.x + sb.y));
+      } else {
+        for (int dx = -1; dx <= 1; ++dx) {
+          int nx = cx + dx;
+          if (nx < 0 || nx >= k.dims[0]) continue;
+          if (ey + (dx < 0 ? lo2[0] : (dx > 0 ? hi2[0] : 0.0f)) > r2) continue;
+          uint2 se = __ldg(&ctab[row + nx]);
+          range((int)se.x, (int)(se.x + se.y));
         }
       }
     }

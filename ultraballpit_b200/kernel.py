@@ -28,7 +28,7 @@ STATUS_NAMES = {0: "SPH_OK", 1: "SPH_ERR_INVALID_ARG", 2: "SPH_ERR_OOM", 3: "SPH
                 4: "SPH_ERR_NONFINITE", 5: "SPH_ERR_TIMEOUT", 6: "SPH_ERR_CAPACITY",
                 7: "SPH_ERR_NO_DEVICE", 8: "SPH_ERR_NO_CHECKPOINT"}
 BOUNDARY_PARTICLES, BOUNDARY_SDF = 0, 1
-CELL_ORDER_MORTON, CELL_ORDER_LINEAR = 0, 1
+CELL_ORDER_MORTON, CELL_ORDER_LINEAR, CELL_ORDER_ROWS = 0, 1, 2
 FLAG_DELTA_SPH, FLAG_XSPH, FLAG_REPULSION, FLAG_DOMAIN_CLAMP = 1, 2, 4, 8
 FLAGS_REFERENCE = 0xF
 
@@ -263,7 +263,7 @@ class SimulationKernel(ABC):
 
 
 def make_params(h, gravity, speed_of_sound, cfl_number, viscosity, domain_min, domain_max, *,
-                alpha=1.0, beta=2.0, boundary_mode=BOUNDARY_PARTICLES, cell_order=CELL_ORDER_MORTON,
+                alpha=1.0, beta=2.0, boundary_mode=BOUNDARY_PARTICLES, cell_order=CELL_ORDER_ROWS,
                 flags=FLAGS_REFERENCE, device=0, sdf_wall_coef=0.981) -> SphParams:
     prm = default_params()
     prm.h = h
@@ -305,7 +305,7 @@ class CudaKernel(SimulationKernel):
                  gravity, speed_of_sound: float, cfl_number: float, viscosity: float,
                  domain_min, domain_max, *, alpha: float = 1.0, beta: float = 2.0,
                  boundary_mode: int = BOUNDARY_PARTICLES, sdf: GridSDF | None = None,
-                 cell_order: int = CELL_ORDER_MORTON, flags: int = FLAGS_REFERENCE,
+                 cell_order: int = CELL_ORDER_ROWS, flags: int = FLAGS_REFERENCE,
                  device: int = 0, sdf_wall_coef: float = 0.981):
         L = load_library()
         particles.validate()
@@ -577,7 +577,7 @@ class CudaBatch(CudaKernel):
     per instance (``domain.Scenario``); ``particles()`` returns the instances
     one after another, ``instance(q)`` slices one out."""
 
-    def __init__(self, scenarios, device: int = 0, cell_order: int = CELL_ORDER_MORTON,
+    def __init__(self, scenarios, device: int = 0, cell_order: int = CELL_ORDER_ROWS,
                  boundary_mode: int = BOUNDARY_PARTICLES):
         L = load_library()
         self._lib = L
