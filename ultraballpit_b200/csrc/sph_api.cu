@@ -8,9 +8,11 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <memory>
 #include <mutex>
 #include <new>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include <cuda_bf16.h>
@@ -387,6 +389,41 @@ void host_sdf_gradient(const SphSdfView& g, float px, float py, float pz, float 
 // boundary particle is listed for every cell whose box (widened by a margin
 // above the rounding of pos_to_cell, unbounded outward on edge cells) comes
 // within 2h (plus margin): a superset of the particles in support.
+// f(t, begin, end) on up to `max_threads` host threads over [0, n) in
+// contiguous chunks, chunk t on thread t; small ranges run inline.
+template <class F>
+void parallel_chunks(size_t n, unsigned max_threads, F&& f) {
+  unsigned T = std::max(1u, std::min(max_threads, std::thread::hardware_concurrency()));
+  if (n < 65536 || T == 1) {
+    f(0u, (size_t)0, n);
+    return;
+  }
+  size_t chunk = (n + T - 1) / T;
+  std::vector<std::thread> ts;
+  for (unsigned t = 0; t < T; ++t) {
+    size_t a = (size_t)t * chunk, e = std::min(n, a + chunk);
+    if (a >= e) break;
+    ts.emplace_back([&f, t, a, e] { f(t, a, e); });
+  }
+  for (std::thread& th : ts) th.join();
+}
+constexpr unsigned kHostThreads = 32;
+// f(t) for t < T, one host thread each (inline when T == 1)
+template <class F>
+void run_threads(unsigned T, F&& f) {
+  if (T <= 1) {
+    if (T == 1) f(0u);
+    return;
+  }
+  std::vector<std::thread> ts;
+  for (unsigned t = 0; t < T; ++t) ts.emplace_back([&f, t] { f(t); });
+  for (std::thread& th : ts) th.join();
+}
+
+// Per linear cell, the boundary particles whose support can reach a particle
+// in that cell, in ascending boundary index (CSR: start[C + 1], list). Host
+// threads take contiguous ranges of boundary particles; each cell's entries
+// are laid out thread by thread, so the order is ascending as with one thread.
 void build_boundary_lists(const SimConst& k, const SphBoundaryView* b, int C,
                           std::vector<uint32_t>& start, std::vector<uint32_t>& list) {
   start.assign((size_t)C + 1, 0);
@@ -394,42 +431,70 @@ void build_boundary_lists(const SimConst& k, const SphBoundaryView* b, int C,
   if (!b || b->n == 0) return;
   double cs = k.cell, margin = 1e-4 * cs;
   double reach = 2.0 * (double)k.h * (1.0 + 1e-4) + margin;
-  std::vector<uint64_t> pairs;  // (cell << 32) | b
-  pairs.reserve(b->n * 12);
-  for (size_t bi = 0; bi < b->n; ++bi) {
-    double pos[3] = {b->x[bi], b->y[bi], b->z[bi]};
-    int lo[3], hi[3];
-    bool empty = false;
-    for (int a = 0; a < 3; ++a) {
-      double u0 = std::floor((pos[a] - reach - k.gmin[a]) / cs);
-      double u1 = std::floor((pos[a] + reach - k.gmin[a]) / cs);
-      lo[a] = (int)std::max(0.0, std::min((double)k.dims[a] - 1, u0));
-      hi[a] = (int)std::max(0.0, std::min((double)k.dims[a] - 1, u1));
-      if (!(pos[a] == pos[a])) empty = true;
+  // per-thread cell counts cost C words per thread: bound their memory
+  unsigned T = (unsigned)std::max<size_t>(1, std::min<size_t>(kHostThreads, ((size_t)64 << 20) / ((size_t)C + 1)));
+  std::vector<std::vector<uint64_t>> pairs(T);  // (cell << 32) | b, per thread
+  unsigned used = 0;
+  std::mutex mu;
+  parallel_chunks(b->n, T, [&](unsigned t, size_t first, size_t last) {
+    std::vector<uint64_t>& out = pairs[t];
+    out.reserve((last - first) * 12);
+    for (size_t bi = first; bi < last; ++bi) {
+      double pos[3] = {b->x[bi], b->y[bi], b->z[bi]};
+      int lo[3], hi[3];
+      bool empty = false;
+      for (int a = 0; a < 3; ++a) {
+        double u0 = std::floor((pos[a] - reach - k.gmin[a]) / cs);
+        double u1 = std::floor((pos[a] + reach - k.gmin[a]) / cs);
+        lo[a] = (int)std::max(0.0, std::min((double)k.dims[a] - 1, u0));
+        hi[a] = (int)std::max(0.0, std::min((double)k.dims[a] - 1, u1));
+        if (!(pos[a] == pos[a])) empty = true;
+      }
+      if (empty) continue;
+      for (int cz = lo[2]; cz <= hi[2]; ++cz)
+        for (int cy = lo[1]; cy <= hi[1]; ++cy)
+          for (int cx = lo[0]; cx <= hi[0]; ++cx) {
+            int c3[3] = {cx, cy, cz};
+            double d2 = 0.0;
+            for (int a = 0; a < 3; ++a) {
+              double blo = c3[a] == 0 ? -1e300 : k.gmin[a] + c3[a] * cs - margin;
+              double bhi = c3[a] == k.dims[a] - 1 ? 1e300 : k.gmin[a] + (c3[a] + 1) * cs + margin;
+              double d = pos[a] < blo ? blo - pos[a] : (pos[a] > bhi ? pos[a] - bhi : 0.0);
+              d2 += d * d;
+            }
+            if (d2 < reach * reach) {
+              uint64_t lin = (uint64_t)cx + (uint64_t)cy * k.dims[0] + (uint64_t)cz * k.dims[0] * k.dims[1];
+              out.push_back((lin << 32) | (uint64_t)bi);
+            }
+          }
     }
-    if (empty) continue;
-    for (int cz = lo[2]; cz <= hi[2]; ++cz)
-      for (int cy = lo[1]; cy <= hi[1]; ++cy)
-        for (int cx = lo[0]; cx <= hi[0]; ++cx) {
-          int c3[3] = {cx, cy, cz};
-          double d2 = 0.0;
-          for (int a = 0; a < 3; ++a) {
-            double blo = c3[a] == 0 ? -1e300 : k.gmin[a] + c3[a] * cs - margin;
-            double bhi = c3[a] == k.dims[a] - 1 ? 1e300 : k.gmin[a] + (c3[a] + 1) * cs + margin;
-            double d = pos[a] < blo ? blo - pos[a] : (pos[a] > bhi ? pos[a] - bhi : 0.0);
-            d2 += d * d;
-          }
-          if (d2 < reach * reach) {
-            uint64_t lin = (uint64_t)cx + (uint64_t)cy * k.dims[0] + (uint64_t)cz * k.dims[0] * k.dims[1];
-            pairs.push_back((lin << 32) | (uint64_t)bi);
-          }
-        }
+    std::lock_guard<std::mutex> lock(mu);
+    used = std::max(used, t + 1);
+  });
+  // per-thread counts, then per-thread write offsets within each cell
+  std::vector<std::vector<uint32_t>> at(used, std::vector<uint32_t>((size_t)C, 0u));
+  run_threads(used, [&](unsigned t) {
+    for (uint64_t pr : pairs[t]) at[t][pr >> 32]++;
+  });
+  for (int c = 0; c < C; ++c) {
+    uint32_t run = 0;
+    for (unsigned t = 0; t < used; ++t) run += at[t][c];
+    start[(size_t)c + 1] = start[c] + run;
   }
-  for (uint64_t pr : pairs) start[(pr >> 32) + 1]++;
-  for (int c = 0; c < C; ++c) start[c + 1] += start[c];
-  list.resize(pairs.size());
-  std::vector<uint32_t> head(start.begin(), start.end() - 1);
-  for (uint64_t pr : pairs) list[head[pr >> 32]++] = (uint32_t)(pr & 0xffffffffu);
+  list.resize(start[C]);
+  parallel_chunks((size_t)C, kHostThreads, [&](unsigned, size_t c0, size_t c1) {
+    for (size_t c = c0; c < c1; ++c) {
+      uint32_t off = start[c];
+      for (unsigned t = 0; t < used; ++t) {
+        uint32_t n = at[t][c];
+        at[t][c] = off;
+        off += n;
+      }
+    }
+  });
+  run_threads(used, [&](unsigned t) {
+    for (uint64_t pr : pairs[t]) list[at[t][pr >> 32]++] = (uint32_t)(pr & 0xffffffffu);
+  });
 }
 
 // Calls f with the constants provider of the handle: the by-value constants
@@ -751,36 +816,55 @@ int create_impl(int ninst, const SphParams* PP, const SphParticlesView* pvs,
     }
     h->ktab_h[q] = k;
     hcc[q] = make_float4(P.h, P.speed_of_sound, P.cfl_number, 0.0f);
-    std::vector<std::pair<uint64_t, uint32_t>> cells(Cq);
-    for (uint32_t cz = 0; cz < dims[2]; ++cz)
-      for (uint32_t cy = 0; cy < dims[1]; ++cy)
-        for (uint32_t cx = 0; cx < dims[0]; ++cx) {
-          uint32_t lin = cx + cy * dims[0] + cz * dims[0] * dims[1];
-          uint64_t key = P.cell_order == SPH_CELL_ORDER_LINEAR ? lin
-                         : P.cell_order == SPH_CELL_ORDER_ROWS
-                             ? (spread2(cy) | (spread2(cz) << 1)) * dims[0] + cx
-                             : (spread21(cx) | (spread21(cy) << 1) | (spread21(cz) << 2));
-          cells[lin] = {key, lin};
-        }
-    std::sort(cells.begin(), cells.end());
     lin_of_rank.resize(C + Cq);
     rank_of_lin.resize(C + Cq);
-    for (uint64_t r = 0; r < Cq; ++r) {
-      lin_of_rank[C + r] = (uint32_t)(C + cells[r].second);
-      rank_of_lin[C + cells[r].second] = (uint32_t)(C + r);
+    auto set_rank = [&](uint64_t r, uint32_t lin) {
+      lin_of_rank[C + r] = (uint32_t)(C + lin);
+      rank_of_lin[C + lin] = (uint32_t)(C + r);
+    };
+    if (P.cell_order == SPH_CELL_ORDER_MORTON) {
+      std::vector<std::pair<uint64_t, uint32_t>> cells(Cq);
+      for (uint32_t cz = 0; cz < dims[2]; ++cz)
+        for (uint32_t cy = 0; cy < dims[1]; ++cy)
+          for (uint32_t cx = 0; cx < dims[0]; ++cx) {
+            uint32_t lin = cx + cy * dims[0] + cz * dims[0] * dims[1];
+            cells[lin] = {spread21(cx) | (spread21(cy) << 1) | (spread21(cz) << 2), lin};
+          }
+      std::sort(cells.begin(), cells.end());
+      for (uint64_t r = 0; r < Cq; ++r) set_rank(r, cells[r].second);
+    } else {
+      // linear: rank = linear index; rows: the x-rows ranked by the Morton
+      // code of (cy, cz), x fastest inside a row (only the rows are sorted)
+      std::vector<std::pair<uint64_t, uint32_t>> rows((size_t)dims[1] * dims[2]);
+      for (uint32_t cz = 0; cz < dims[2]; ++cz)
+        for (uint32_t cy = 0; cy < dims[1]; ++cy) {
+          uint32_t row = cy + cz * dims[1];
+          rows[row] = {P.cell_order == SPH_CELL_ORDER_ROWS ? (spread2(cy) | (spread2(cz) << 1)) : row, row};
+        }
+      std::sort(rows.begin(), rows.end());
+      for (size_t rr = 0; rr < rows.size(); ++rr)
+        for (uint32_t cx = 0; cx < dims[0]; ++cx)
+          set_rank((uint64_t)rr * dims[0] + cx, rows[rr].second * dims[0] + cx);
     }
     std::vector<uint32_t> s1, l1;
     build_boundary_lists(k, bv, (int)Cq, s1, l1);
     uint32_t base = (uint32_t)blist.size(), bbase = (uint32_t)h->boff[q];
-    for (uint64_t c = 1; c <= Cq; ++c) bstart.push_back(base + s1[c]);
-    for (uint32_t b : l1) blist.push_back(bbase + b);
+    if (base == 0 && bbase == 0 && bstart.size() == 1) {  // the first instance: take the lists as they are
+      bstart = std::move(s1);
+      blist = std::move(l1);
+    } else {
+      bstart.reserve(bstart.size() + Cq);
+      for (uint64_t c = 1; c <= Cq; ++c) bstart.push_back(base + s1[c]);
+      blist.reserve(blist.size() + l1.size());
+      for (uint32_t b : l1) blist.push_back(bbase + b);
+    }
     h->poff[q + 1] = h->poff[q] + pv->n;
     h->boff[q + 1] = h->boff[q] + (bv ? bv->n : 0);
     // initial conservation totals, in the reference's order (lib.rs:152-156)
     double m = 0.0, e = 0.0;
-    for (size_t i = 0; i < pv->n; ++i) m += (double)pv->mass[i];
-    for (size_t i = 0; i < pv->n; ++i) {
+    for (size_t i = 0; i < pv->n; ++i) {  // two sums, each in index order
       double mi = (double)pv->mass[i];
+      m += mi;
       double vx = pv->vx[i], vy = pv->vy[i], vz = pv->vz[i];
       e += 0.5 * mi * (vx * vx + vy * vy + vz * vz);
       double x = pv->x[i], y = pv->y[i], z = pv->z[i];
@@ -837,23 +921,27 @@ int create_impl(int ninst, const SphParams* PP, const SphParticlesView* pvs,
   if (e != cudaSuccess) return fail(e == cudaErrorMemoryAllocation ? SPH_ERR_OOM : SPH_ERR_CUDA);
 
   // upload (particles of instance q at [poff[q], poff[q+1]), ids global)
-  std::vector<float4> hpos(n), hvel(n), hacc(n), hb(nb);
-  std::vector<uint32_t> hid(n);
-  std::vector<float> hpr(n);
+  // staging arrays left uninitialised: every entry is written below, by the
+  // host threads that also take the first-touch page faults
+  std::unique_ptr<float4[]> hpos(new float4[n]), hvel(new float4[n]), hacc(new float4[n]), hb(new float4[nb]);
+  std::unique_ptr<uint32_t[]> hid(new uint32_t[n]);
+  std::unique_ptr<float[]> hpr(new float[n]);
   std::vector<uint16_t> hip(ninst > 1 ? n : 0), hib(ninst > 1 ? nb : 0);
   h->temperature.resize(n);
   for (int q = 0; q < ninst; ++q) {
     const SphParticlesView* pv = &pvs[q];
     size_t o = h->poff[q];
-    for (size_t i = 0; i < pv->n; ++i) {
-      hpos[o + i] = make_float4(pv->x[i], pv->y[i], pv->z[i], pv->mass[i]);
-      hvel[o + i] = make_float4(pv->vx[i], pv->vy[i], pv->vz[i], pv->density[i]);
-      hacc[o + i] = make_float4(pv->ax[i], pv->ay[i], pv->az[i], 0.0f);
-      hid[o + i] = (uint32_t)(o + i) | (pv->fluid_type[i] ? sph::kAirBit : 0u);
-      hpr[o + i] = pv->pressure[i];
-      h->temperature[o + i] = pv->temperature[i];
-      if (ninst > 1) hip[o + i] = (uint16_t)q;
-    }
+    parallel_chunks(pv->n, kHostThreads, [&](unsigned, size_t i0, size_t i1) {
+      for (size_t i = i0; i < i1; ++i) {
+        hpos[o + i] = make_float4(pv->x[i], pv->y[i], pv->z[i], pv->mass[i]);
+        hvel[o + i] = make_float4(pv->vx[i], pv->vy[i], pv->vz[i], pv->density[i]);
+        hacc[o + i] = make_float4(pv->ax[i], pv->ay[i], pv->az[i], 0.0f);
+        hid[o + i] = (uint32_t)(o + i) | (pv->fluid_type[i] ? sph::kAirBit : 0u);
+        hpr[o + i] = pv->pressure[i];
+        h->temperature[o + i] = pv->temperature[i];
+        if (ninst > 1) hip[o + i] = (uint16_t)q;
+      }
+    });
     const SphBoundaryView* bv = (sdf_mode || !bvs) ? nullptr : bvs[q];
     size_t bo = h->boff[q];
     for (size_t i = 0; bv && i < bv->n; ++i) {
@@ -868,12 +956,12 @@ int create_impl(int ninst, const SphParams* PP, const SphParticlesView* pvs,
   };
   if (e == cudaSuccess) e = cudaMalloc(&accU, std::max<size_t>(1, n) * sizeof(float4));
   if (e == cudaSuccess) e = cudaMalloc(&prU, std::max<size_t>(1, n) * sizeof(float));
-  up(h->posU, hpos.data(), n * sizeof(float4));
-  up(h->velU, hvel.data(), n * sizeof(float4));
-  up(accU, hacc.data(), n * sizeof(float4));
-  up(prU, hpr.data(), n * sizeof(float));
-  up(h->idU, hid.data(), n * sizeof(uint32_t));
-  up(h->bpos, hb.data(), nb * sizeof(float4));
+  up(h->posU, hpos.get(), n * sizeof(float4));
+  up(h->velU, hvel.get(), n * sizeof(float4));
+  up(accU, hacc.get(), n * sizeof(float4));
+  up(prU, hpr.get(), n * sizeof(float));
+  up(h->idU, hid.get(), n * sizeof(uint32_t));
+  up(h->bpos, hb.get(), nb * sizeof(float4));
   up(h->rank_of_lin, rank_of_lin.data(), C * sizeof(uint32_t));
   up(h->lin_of_rank, lin_of_rank.data(), C * sizeof(uint32_t));
   up(h->bc_start, bstart.data(), (C + 1) * sizeof(uint32_t));

@@ -1491,14 +1491,26 @@ k_metrics_partial(SimConst k, int n, const float4* __restrict__ pos, const float
 __global__ void k_metrics_final(int nparts, const double* __restrict__ part_m,
                                 const double* __restrict__ part_e, const float* __restrict__ part_var,
                                 double* __restrict__ out_me, float* __restrict__ out_var) {
-  if (threadIdx.x != 0) return;
+  // one warp: lane l sums partials l, l + 32, ... in order, then a fixed
+  // butterfly combines the lanes, so the result does not vary between runs
+  int lane = threadIdx.x & 31;
   double m = 0.0, e = 0.0;
   float v = 0.0f;
-  for (int b = 0; b < nparts; ++b) {
-    m += part_m[b]; e += part_e[b];
-    if (part_var[b] > v) v = part_var[b];
+  for (int b = lane; b < nparts; b += 32) {
+    m += part_m[b];
+    e += part_e[b];
+    v = fmaxf(v, part_var[b]);
   }
-  out_me[0] = m; out_me[1] = e; *out_var = v;
+  for (int off = 16; off > 0; off >>= 1) {
+    m += __shfl_xor_sync(0xffffffffu, m, off);
+    e += __shfl_xor_sync(0xffffffffu, e, off);
+    v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, off));
+  }
+  if (lane == 0) {
+    out_me[0] = m;
+    out_me[1] = e;
+    *out_var = v;
+  }
 }
 
 // Particle records of the viewer's Frame message (server ws.rs:233-290):
