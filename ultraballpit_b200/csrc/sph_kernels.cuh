@@ -453,9 +453,10 @@ __device__ __forceinline__ void dist2_pair(unsigned long long X, unsigned long l
 }
 
 // The visit of for_each_neighbor reduced to the support test, for recording:
-// rec(slot, ok) for every candidate in the same order, ok = in support and
-// not `self`. Calling rec for every candidate (not only the kept ones) lets
-// the caller record without a divergent branch per candidate.
+// rec(slot, ok) for every candidate in the same order, ok = in support;
+// `self` is never offered (the home cell's range is split around it).
+// Calling rec for every candidate (not only the kept ones) lets the caller
+// record without a divergent branch per candidate.
 template <class R>
 __device__ __forceinline__ void scan_support(float px, float py, float pz, int self,
                                              const float4* __restrict__ pos, const uint2* __restrict__ ctab,
@@ -495,15 +496,15 @@ __device__ __forceinline__ void scan_support(float px, float py, float pz, int s
           float d0, d1, d2, d3;
           dist2_pair(X, Y, Z, q0, q1, d0, d1);
           dist2_pair(X, Y, Z, q2, q3, d2, d3);
-          rec(s, d0 <= r2 && s != self);
-          rec(s + 1, d1 <= r2 && s + 1 != self);
-          rec(s + 2, d2 <= r2 && s + 2 != self);
-          rec(s + 3, d3 <= r2 && s + 3 != self);
+          rec(s, d0 <= r2);
+          rec(s + 1, d1 <= r2);
+          rec(s + 2, d2 <= r2);
+          rec(s + 3, d3 <= r2);
         }
         for (; s < end; ++s) {
           float4 q = __ldg(&pos[s]);
           float ax = px - q.x, ay = py - q.y, az = pz - q.z;
-          rec(s, ax * ax + ay * ay + az * az <= r2 && s != self);
+          rec(s, ax * ax + ay * ay + az * az <= r2);
         }
       };
       if (k.rows) {
@@ -513,14 +514,24 @@ __device__ __forceinline__ void scan_support(float px, float py, float pz, int s
         int xa = (cx > 0 && ey + lo2[0] <= r2) ? cx - 1 : cx;
         int xb = (cx + 1 < k.dims[0] && ey + hi2[0] <= r2) ? cx + 1 : cx;
         uint2 sa = __ldg(&ctab[row + xa]), sb = __ldg(&ctab[row + xb]);
-        range((int)sa.x, (int)(sb.x + sb.y));
+        if (ny == cy && nz == cz) {  // the home row holds `self`: skip it by splitting the range
+          range((int)sa.x, self);
+          range(self + 1, (int)(sb.x + sb.y));
+        } else {
+          range((int)sa.x, (int)(sb.x + sb.y));
+        }
       } else {
         for (int dx = -1; dx <= 1; ++dx) {
           int nx = cx + dx;
           if (nx < 0 || nx >= k.dims[0]) continue;
           if (ey + (dx < 0 ? lo2[0] : (dx > 0 ? hi2[0] : 0.0f)) > r2) continue;
           uint2 se = __ldg(&ctab[row + nx]);
-          range((int)se.x, (int)(se.x + se.y));
+          if (dx == 0 && ny == cy && nz == cz) {
+            range((int)se.x, self);
+            range(self + 1, (int)(se.x + se.y));
+          } else {
+            range((int)se.x, (int)(se.x + se.y));
+          }
         }
       }
     }
@@ -906,11 +917,17 @@ k_density(KP kp, int n, const float* __restrict__ dtp, const float4* __restrict_
     dst[0] = make_uint4(stage[0], stage[bsz], stage[2 * bsz], stage[3 * bsz]);
     dst[1] = make_uint4(stage[4 * bsz], stage[5 * bsz], stage[6 * bsz], stage[7 * bsz]);
   };
+  uint32_t* sp = stage;  // the open chunk's next entry
+  uint32_t* const chunk_end = stage + kNbrChunk * bsz;
   scan_support(pi.x, pi.y, pi.z, i, pos, ctab, k, [&](int s, bool ok) {
-    stage[(listed % kNbrChunk) * bsz] = (uint32_t)s;  // kept only if ok advances `listed`
+    *sp = (uint32_t)s;  // kept only if ok advances the entry
     if (ok) {
-      if (listed % kNbrChunk == kNbrChunk - 1 && listed < kNbrCap) flush(listed / kNbrChunk);
+      sp += bsz;
       ++listed;
+      if (sp == chunk_end) {
+        if (listed <= kNbrCap) flush((listed - 1) / kNbrChunk);
+        sp = stage;
+      }
     }
   });
   if (listed < kNbrCap && listed % kNbrChunk != 0) flush(listed / kNbrChunk);  // the open chunk
