@@ -97,6 +97,7 @@ struct SphHandle {
   // boundary
   float4* bpos = nullptr;
   float* bpress = nullptr;
+  uint8_t* bact = nullptr;  // per boundary particle: an occupied cell lists it (k_adami_mark)
   uint32_t *bc_start = nullptr, *bc_list = nullptr;
   // SDF node grid and wall table (boundary_mode SPH_BOUNDARY_SDF), or the
   // geometry SDF(s) of the closure features
@@ -545,16 +546,24 @@ void enqueue_density_only(SphHandle* h) {
   }
 }
 
-void enqueue_density_adami(SphHandle* h) {
+// boundary.rs:87-123: the Adami boundary pressure, for the boundary particles
+// that an occupied cell lists (the others get the empty sum's 0)
+void enqueue_adami(SphHandle* h) {
   using namespace sph;
-  enqueue_density_only(h);
   if (h->nb > 0) {
+    cudaMemsetAsync(h->bact, 0, (size_t)h->nb, h->st);
+    k_adami_mark<<<grid_for(h->C, 256), 256, 0, h->st>>>(h->C, h->ctab, h->bc_start, h->bc_list, h->bact);
     dispatch(h, true, [&](auto kp) {
       k_adami<<<grid_for(h->nb, kAdamiWarps), kAdamiWarps * 32, 0, h->st>>>(
-          kp, h->nb, h->bpos, h->bpress, h->pos, h->rf, h->pr, h->id, h->ctab, h->err);
+          kp, h->nb, h->bpos, h->bpress, h->pos, h->rf, h->pr, h->id, h->ctab, h->err, h->bact);
     });
-    h->launches += 1;
+    h->launches += 2;
   }
+}
+
+void enqueue_density_adami(SphHandle* h) {
+  enqueue_density_only(h);
+  enqueue_adami(h);
 }
 
 void enqueue_forces(SphHandle* h, float hdt_scale) {
@@ -906,7 +915,7 @@ int create_impl(int ninst, const SphParams* PP, const SphParticlesView* pvs,
   ALLOC(posU, n); ALLOC(velU, n); ALLOC(idU, n); ALLOC(keyU, n); ALLOC(tmp, n); ALLOC(tmpid, n);
   ALLOC(hist, C); ALLOC(cstart, C); ALLOC(ccount, C); ALLOC(cursor, C); ALLOC(bsum, h->nbsum);
   ALLOC(rank_of_lin, C); ALLOC(lin_of_rank, C); ALLOC(ctab, C);
-  ALLOC(bpos, nb); ALLOC(bpress, nb); ALLOC(bc_start, C + 1); ALLOC(bc_list, blist.size());
+  ALLOC(bpos, nb); ALLOC(bpress, nb); ALLOC(bact, nb); ALLOC(bc_start, C + 1); ALLOC(bc_list, blist.size());
   ALLOC(dt, ninst); ALLOC(dt_query, ninst); ALLOC(red, 2 * ninst); ALLOC(err, 1); ALLOC(hcc, ninst);
   ALLOC(part_m, h->nparts); ALLOC(part_e, h->nparts); ALLOC(part_var, h->nparts); ALLOC(me, 2);
   ALLOC(var, 1); ALLOC(bad, 1);
@@ -1176,14 +1185,7 @@ int sph_step_profiled(SphHandle* h, float dt, SphStepProfile* prof) {
   cudaEventRecord(ev[2], h->st);
   enqueue_density_only(h);
   cudaEventRecord(ev[3], h->st);
-  if (h->nb > 0) {
-    using namespace sph;
-    dispatch(h, true, [&](auto kp) {
-      k_adami<<<grid_for(h->nb, kAdamiWarps), kAdamiWarps * 32, 0, h->st>>>(
-          kp, h->nb, h->bpos, h->bpress, h->pos, h->rf, h->pr, h->id, h->ctab, h->err);
-    });
-    h->launches += 1;
-  }
+  enqueue_adami(h);
   cudaEventRecord(ev[4], h->st);
   enqueue_forces(h, 1.0f);
   cudaEventRecord(ev[5], h->st);

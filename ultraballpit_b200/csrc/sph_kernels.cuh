@@ -1116,17 +1116,35 @@ k_closure_apply(KP kp, const __nv_bfloat16* __restrict__ wb, const float* __rest
 // range, a warp bitonic sort orders them by fluid index, and lane 0 sums
 // them in that order.
 constexpr int kAdamiWarps = 4;
+// Marks the boundary particles that an occupied fluid cell lists as
+// candidates (bc_start/bc_list: every boundary particle whose support can
+// reach a particle of the cell). A boundary particle with a fluid particle in
+// support is marked; an unmarked one has no terms, and its Adami pressure is
+// the empty sum's 0.
+__global__ void k_adami_mark(int C, const uint2* __restrict__ ctab, const uint32_t* __restrict__ bc_start,
+                             const uint32_t* __restrict__ bc_list, uint8_t* __restrict__ act) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= C || __ldg(&ctab[c]).y == 0u) return;
+  uint32_t q1 = __ldg(&bc_start[c + 1]);
+  for (uint32_t q = __ldg(&bc_start[c]); q < q1; ++q) act[__ldg(&bc_list[q])] = 1;
+}
+
 template <class KP>
 __global__ void __launch_bounds__(kAdamiWarps * 32)
 k_adami(KP kp, int nb, const float4* __restrict__ bpos, float* __restrict__ bpress,
         const float4* __restrict__ pos, const float2* __restrict__ rf, const float* __restrict__ pr,
-        const uint32_t* __restrict__ id, const uint2* __restrict__ ctab, uint32_t* __restrict__ err) {
+        const uint32_t* __restrict__ id, const uint2* __restrict__ ctab, uint32_t* __restrict__ err,
+        const uint8_t* __restrict__ act) {
   __shared__ uint32_t s_id[kAdamiWarps][kAdamiCap];
   __shared__ float s_w[kAdamiWarps][kAdamiCap];
   __shared__ float s_wp[kAdamiWarps][kAdamiCap];
   int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   int b = blockIdx.x * kAdamiWarps + warp;
   if (b >= nb || *err) return;
+  if (!act[b]) {  // no fluid particle can be in support (k_adami_mark)
+    if (lane == 0) bpress[b] = 0.0f;
+    return;
+  }
   const SimConst& k = kp.at(b);
   float4 bp = bpos[b];
   int lo[3], hi[3];
@@ -1139,16 +1157,29 @@ k_adami(KP kp, int nb, const float4* __restrict__ bpos, float* __restrict__ bpre
   int count = 0;
   bool overflow = false;
   // Lanes look up the (at most 4x4x4) cells of the range in parallel; only
-  // occupied cells are then scanned. The terms are sorted by fluid index
-  // below, so the cell order does not matter.
+  // occupied cells whose box comes within 2h are then scanned (the box is
+  // widened by a margin far above the rounding of the binning, edge cells
+  // unbounded outward, as particles outside the domain are binned there).
+  // The terms are sorted by fluid index below, so the cell order does not
+  // matter.
   int nx = hi[0] - lo[0] + 1, ny = hi[1] - lo[1] + 1, nz = hi[2] - lo[2] + 1;
   int ncell = nx * ny * nz;
+  const float margin = 1.0e-5f * k.cell + 1.0e-6f;
   for (int cbase = 0; cbase < ncell; cbase += 32) {
     int q = cbase + lane;
     uint2 mine = make_uint2(0u, 0u);
     if (q < ncell) {
-      int qx = q % nx, qy = (q / nx) % ny, qz = q / (nx * ny);
-      mine = __ldg(&ctab[k.coff + cell_hash(lo[0] + qx, lo[1] + qy, lo[2] + qz, k)]);
+      int c3[3] = {lo[0] + q % nx, lo[1] + (q / nx) % ny, lo[2] + q / (nx * ny)};
+      float gap2 = 0.0f;
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        float face = k.gmin[a] + (float)c3[a] * k.cell;
+        float below = c3[a] > 0 ? face - margin - bc[a] : 0.0f;
+        float above = c3[a] < k.dims[a] - 1 ? bc[a] - (face + k.cell + margin) : 0.0f;
+        float g = fmaxf(fmaxf(below, above), 0.0f);
+        gap2 += g * g;
+      }
+      if (gap2 <= k.radius_sq) mine = __ldg(&ctab[k.coff + cell_hash(c3[0], c3[1], c3[2], k)]);
     }
     unsigned occupied = __ballot_sync(0xffffffffu, mine.y > 0u);
     while (occupied) {
