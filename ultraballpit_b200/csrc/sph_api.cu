@@ -552,7 +552,7 @@ void enqueue_adami(SphHandle* h) {
   using namespace sph;
   if (h->nb > 0) {
     cudaMemsetAsync(h->bact, 0, (size_t)h->nb, h->st);
-    k_adami_mark<<<grid_for(h->C, 256), 256, 0, h->st>>>(h->C, h->ctab, h->bc_start, h->bc_list, h->bact);
+    k_adami_mark<<<grid_for(h->C, 8), 256, 0, h->st>>>(h->C, h->ctab, h->bc_start, h->bc_list, h->bact);
     dispatch(h, true, [&](auto kp) {
       k_adami<<<grid_for(h->nb, kAdamiWarps), kAdamiWarps * 32, 0, h->st>>>(
           kp, h->nb, h->bpos, h->bpress, h->pos, h->rf, h->pr, h->id, h->ctab, h->err, h->bact);

@@ -1121,12 +1121,13 @@ constexpr int kAdamiWarps = 4;
 // reach a particle of the cell). A boundary particle with a fluid particle in
 // support is marked; an unmarked one has no terms, and its Adami pressure is
 // the empty sum's 0.
+// One warp per cell, the lanes taking the cell's list entries in turn.
 __global__ void k_adami_mark(int C, const uint2* __restrict__ ctab, const uint32_t* __restrict__ bc_start,
                              const uint32_t* __restrict__ bc_list, uint8_t* __restrict__ act) {
-  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  int c = (int)((blockIdx.x * (unsigned)blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
   if (c >= C || __ldg(&ctab[c]).y == 0u) return;
   uint32_t q1 = __ldg(&bc_start[c + 1]);
-  for (uint32_t q = __ldg(&bc_start[c]); q < q1; ++q) act[__ldg(&bc_list[q])] = 1;
+  for (uint32_t q = __ldg(&bc_start[c]) + lane; q < q1; q += 32) act[__ldg(&bc_list[q])] = 1;
 }
 
 template <class KP>
@@ -1222,6 +1223,34 @@ k_adami(KP kp, int nb, const float4* __restrict__ bpos, float* __restrict__ bpre
   }
   if (__any_sync(0xffffffffu, overflow) || count > kAdamiCap) {
     if (lane == 0) atomicOr(err, kErrAdamiCap);
+    return;
+  }
+  if (count <= 32) {
+    // up to 32 terms: one per lane, bitonic-sorted by fluid index across the
+    // lanes, then summed in that order (the same additions as below)
+    __syncwarp();
+    uint32_t key = lane < count ? s_id[warp][lane] : 0xffffffffu;
+    float w = lane < count ? s_w[warp][lane] : 0.0f;
+    float wp = lane < count ? s_wp[warp][lane] : 0.0f;
+    for (int kk = 2; kk <= 32; kk <<= 1) {
+      for (int j = kk >> 1; j > 0; j >>= 1) {
+        uint32_t ok = __shfl_xor_sync(0xffffffffu, key, j);
+        float ow = __shfl_xor_sync(0xffffffffu, w, j);
+        float owp = __shfl_xor_sync(0xffffffffu, wp, j);
+        bool up = (lane & kk) == 0, lower = (lane & j) == 0;
+        if (lower == up ? ok < key : ok > key) {
+          key = ok;
+          w = ow;
+          wp = owp;
+        }
+      }
+    }
+    float weighted_pressure = 0.0f, weight_sum = 0.0f;
+    for (int q = 0; q < count; ++q) {
+      weighted_pressure += __shfl_sync(0xffffffffu, wp, q);
+      weight_sum += __shfl_sync(0xffffffffu, w, q);
+    }
+    if (lane == 0) bpress[b] = weight_sum > 1.0e-12f ? fmaxf(weighted_pressure / weight_sum, 0.0f) : 0.0f;
     return;
   }
   int m2 = 1;
