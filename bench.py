@@ -398,16 +398,24 @@ def run_cuda_arm(args):
                 "forces_us": rb["SPH_BYTES_FORCES"] * n}
     peak, peak_kind = measured_peaks()
     achieved = bytes_of[dom] / (avg[dom] * 1e-6) / 1e9
-    traffic = None
+    traffic, l2_pct = None, None
     tfile = os.path.join(ROOT, "profiles", "ncu_traffic.json")
     if os.path.exists(tfile):
         t = json.load(open(tfile)).get(dom.replace("_us", ""))
         if t and "bytes_per_particle" in t:
             traffic = t["bytes_per_particle"] * n
+            l2_pct = t.get("l2_pct_of_peak")
     roofline = {"bound": "hbm", "kernel": dom.replace("_us", ""), "achieved": achieved, "peak": peak,
                 "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
                 "peak_source": peak_kind, "stage_us": {s.replace("_us", ""): round(avg[s], 2) for s in stage_keys},
                 "algorithmic_bytes_per_launch": bytes_of[dom]}
+    if traffic is not None:
+        # the neighbour kernels are bound by L1 and instruction issue, not HBM:
+        # the DRAM rate of the ncu-measured traffic at this run's launch time,
+        # and the L2 throughput share from the same capture
+        roofline["dram_gbs_of_measured_traffic"] = traffic / (avg[dom] * 1e-6) / 1e9
+        roofline["dram_frac_of_measured_traffic"] = roofline["dram_gbs_of_measured_traffic"] / peak
+        roofline["l2_pct_of_peak_ncu"] = l2_pct
     ps = pair_stats(sc)
     roofline["pairs"] = dict(ps, **{
         "density_candidate_tests_per_s": n * ps["candidates_per_particle"] / (avg["density_us"] * 1e-6),
