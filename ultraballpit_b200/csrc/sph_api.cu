@@ -903,11 +903,42 @@ int create_impl(int ninst, const SphParams* PP, const SphParticlesView* pvs,
   }
   h->k = h->ktab_h[0];
 
-  if (cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking) != cudaSuccess) return fail(SPH_ERR_CUDA);
+  // upload staging (particles of instance q at [poff[q], poff[q+1]), ids
+  // global), left uninitialised: every entry is written by the packing
+  // thread (and its helpers, which also take the first-touch page faults)
+  // while this thread allocates the device arrays
   size_t n = (size_t)h->n, nb = (size_t)h->nb;
+  std::unique_ptr<float4[]> hpos(new float4[n]), hvel(new float4[n]), hacc(new float4[n]), hb(new float4[nb]);
+  std::unique_ptr<uint32_t[]> hid(new uint32_t[n]);
+  std::unique_ptr<float[]> hpr(new float[n]);
+  std::vector<uint16_t> hip(ninst > 1 ? n : 0), hib(ninst > 1 ? nb : 0);
+  h->temperature.resize(n);
+  std::thread packer([&] {
+    for (int q = 0; q < ninst; ++q) {
+      const SphParticlesView* pv = &pvs[q];
+      size_t o = h->poff[q];
+      parallel_chunks(pv->n, kHostThreads, [&](unsigned, size_t i0, size_t i1) {
+        for (size_t i = i0; i < i1; ++i) {
+          hpos[o + i] = make_float4(pv->x[i], pv->y[i], pv->z[i], pv->mass[i]);
+          hvel[o + i] = make_float4(pv->vx[i], pv->vy[i], pv->vz[i], pv->density[i]);
+          hacc[o + i] = make_float4(pv->ax[i], pv->ay[i], pv->az[i], 0.0f);
+          hid[o + i] = (uint32_t)(o + i) | (pv->fluid_type[i] ? sph::kAirBit : 0u);
+          hpr[o + i] = pv->pressure[i];
+          h->temperature[o + i] = pv->temperature[i];
+          if (ninst > 1) hip[o + i] = (uint16_t)q;
+        }
+      });
+      const SphBoundaryView* bv = (sdf_mode || !bvs) ? nullptr : bvs[q];
+      size_t bo = h->boff[q];
+      for (size_t i = 0; bv && i < bv->n; ++i) {
+        hb[bo + i] = make_float4(bv->x[i], bv->y[i], bv->z[i], bv->mass[i]);
+        if (ninst > 1) hib[bo + i] = (uint16_t)q;
+      }
+    }
+  });
+  cudaError_t e = cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking);
   h->nbsum = grid_for(h->C, sph::kScanTile);
   h->nparts = std::max(1, std::min(grid_for((long long)n, sph::kMetricThreads), 1184));
-  cudaError_t e = cudaSuccess;
 #define ALLOC(ptr, cnt) \
   if (e == cudaSuccess) e = dalloc(h, &h->ptr, (cnt))
   ALLOC(pos, n); ALLOC(vel, n); ALLOC(velout, n); ALLOC(acc, n);
@@ -927,37 +958,9 @@ int create_impl(int ninst, const SphParams* PP, const SphParticlesView* pvs,
   if (sdf_mode) ALLOC(sdf, std::max<uint64_t>(sdf_nodes, 1));
   if (sdf_mode) ALLOC(wall_tab, wall_host.size());
 #undef ALLOC
+  packer.join();
   if (e != cudaSuccess) return fail(e == cudaErrorMemoryAllocation ? SPH_ERR_OOM : SPH_ERR_CUDA);
 
-  // upload (particles of instance q at [poff[q], poff[q+1]), ids global)
-  // staging arrays left uninitialised: every entry is written below, by the
-  // host threads that also take the first-touch page faults
-  std::unique_ptr<float4[]> hpos(new float4[n]), hvel(new float4[n]), hacc(new float4[n]), hb(new float4[nb]);
-  std::unique_ptr<uint32_t[]> hid(new uint32_t[n]);
-  std::unique_ptr<float[]> hpr(new float[n]);
-  std::vector<uint16_t> hip(ninst > 1 ? n : 0), hib(ninst > 1 ? nb : 0);
-  h->temperature.resize(n);
-  for (int q = 0; q < ninst; ++q) {
-    const SphParticlesView* pv = &pvs[q];
-    size_t o = h->poff[q];
-    parallel_chunks(pv->n, kHostThreads, [&](unsigned, size_t i0, size_t i1) {
-      for (size_t i = i0; i < i1; ++i) {
-        hpos[o + i] = make_float4(pv->x[i], pv->y[i], pv->z[i], pv->mass[i]);
-        hvel[o + i] = make_float4(pv->vx[i], pv->vy[i], pv->vz[i], pv->density[i]);
-        hacc[o + i] = make_float4(pv->ax[i], pv->ay[i], pv->az[i], 0.0f);
-        hid[o + i] = (uint32_t)(o + i) | (pv->fluid_type[i] ? sph::kAirBit : 0u);
-        hpr[o + i] = pv->pressure[i];
-        h->temperature[o + i] = pv->temperature[i];
-        if (ninst > 1) hip[o + i] = (uint16_t)q;
-      }
-    });
-    const SphBoundaryView* bv = (sdf_mode || !bvs) ? nullptr : bvs[q];
-    size_t bo = h->boff[q];
-    for (size_t i = 0; bv && i < bv->n; ++i) {
-      hb[bo + i] = make_float4(bv->x[i], bv->y[i], bv->z[i], bv->mass[i]);
-      if (ninst > 1) hib[bo + i] = (uint16_t)q;
-    }
-  }
   float4* accU = nullptr;
   float* prU = nullptr;
   auto up = [&](void* d, const void* src, size_t bytes) {
