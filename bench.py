@@ -191,7 +191,14 @@ def run_batch_arm(args):
     torch.cuda.set_device(local)
     rep = Replicas("nccl")
     w = WORKLOADS[args.workload]
-    scs = domain.batch_boxes(w["batch"], seed=args.seed + rank, draw=w.get("draw", "stated"))
+    if args.shard:
+        # one draw shared by all ranks, instances bin-packed across the GPUs
+        from ultraballpit_b200.replicas import partition_lpt
+        allscs = domain.batch_boxes(w["batch"], seed=args.seed, draw=w.get("draw", "stated"))
+        mine = partition_lpt([len(s.particles) for s in allscs], world)[rank]
+        scs = [allscs[i] for i in mine]
+    else:
+        scs = domain.batch_boxes(w["batch"], seed=args.seed + rank, draw=w.get("draw", "stated"))
     ntot = sum(len(s.particles) for s in scs)
     b = CudaBatch(scs, device=local)
     stream = torch.cuda.ExternalStream(b.stream())
@@ -228,13 +235,17 @@ def run_batch_arm(args):
         k.close()
     value, ms = rep.whole_job_rate(ntot, args.steps, ms)
     seq_value, seq_ms = rep.whole_job_rate(ntot, args.steps, seq_ms)
+    per_rank = rep.gather({"instances": len(scs), "particles": ntot})
     rep.close()
     counts = [len(s.particles) for s in scs]
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+        "scaling": "strong" if args.shard else "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded boxes, host-built)",
         "config": {"workload": args.workload, "instances": len(scs), "particles": ntot,
+                   "sharding": "one draw bin-packed across ranks" if args.shard else "a draw per rank",
+                   "per_rank": per_rank,
                    "boundary_particles": sum(len(s.boundary) for s in scs),
                    "instance_particles_min_max": [min(counts), max(counts)],
                    "size_histogram_log2": domain.size_histogram(scs), "launch": tuned,
@@ -505,6 +516,8 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=25.0)
     ap.add_argument("--ref-budget", type=float, default=120.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--shard", action="store_true",
+                    help="batch workloads: bin-pack one draw of instances across the ranks (strong scaling)")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "cuda":
         args.warmup = 3

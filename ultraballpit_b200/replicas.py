@@ -11,6 +11,24 @@ import os
 from datetime import timedelta
 
 
+def partition_lpt(sizes, parts: int) -> list[list[int]]:
+    """Greedy bin-packing of independent instances onto ``parts`` GPUs
+    (longest processing time first): instances by decreasing size, each to the
+    least-loaded GPU so far (ties: lower index). Deterministic, so every rank
+    computes the same assignment without communicating. Returns, per part, the
+    instance indices in increasing order."""
+    if parts < 1:
+        raise ValueError("parts must be >= 1")
+    order = sorted(range(len(sizes)), key=lambda i: (-sizes[i], i))
+    load = [0] * parts
+    out = [[] for _ in range(parts)]
+    for i in order:
+        p = min(range(parts), key=lambda q: (load[q], q))
+        out[p].append(i)
+        load[p] += sizes[i]
+    return [sorted(o) for o in out]
+
+
 def env() -> tuple[int, int, int]:
     return (int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")),
             int(os.environ.get("LOCAL_RANK", "0")))
@@ -49,6 +67,15 @@ class Replicas:
 
     def sum(self, x: float) -> float:
         return float(x) if self.dist is None else self._reduce(x, self.dist.ReduceOp.SUM)
+
+    def gather(self, obj) -> list:
+        """Every rank's ``obj`` (picklable), in rank order, on every rank (a
+        host gather of per-instance statistics at the end of a run)."""
+        if self.dist is None:
+            return [obj]
+        out = [None] * self.world
+        self.dist.all_gather_object(out, obj)
+        return out
 
     def whole_job_rate(self, local_particles: int, steps: int, local_ms: float) -> tuple[float, float]:
         """(particle-steps/s of all ranks together, max ms over ranks): the
