@@ -602,6 +602,13 @@ __global__ void k_set_dt(float* dt, int ninst, float value) {
   for (int q = threadIdx.x; q < ninst; q += blockDim.x) dt[q] = value;
 }
 
+// One 32-byte gather record (two float4) in a single 256-bit load.
+__device__ __forceinline__ void ld_record(const float4* __restrict__ p, float4& a, float4& b) {
+  asm("ld.global.nc.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+      : "=f"(a.x), "=f"(a.y), "=f"(a.z), "=f"(a.w), "=f"(b.x), "=f"(b.y), "=f"(b.z), "=f"(b.w)
+      : "l"(p));
+}
+
 // Gather records of k_xsph_drift, one 32-byte pair per particle:
 // rec[2i] = (x, y, z, m), rec[2i+1] = (v + a dt/2, rho), the half-kicked
 // velocity computed as the reference's kick 1 does (lib.rs:301-305). The
@@ -663,8 +670,9 @@ k_xsph_drift(KP kp, int n, const float* __restrict__ dtp, const float4* __restri
       // one 32-byte record per neighbour, two neighbours in flight
       uint32_t c = 0;
       auto pair = [&](int s0, int s1) {
-        float4 p0 = __ldg(&rec[2 * s0]), h0 = __ldg(&rec[2 * s0 + 1]);
-        float4 p1 = __ldg(&rec[2 * s1]), h1 = __ldg(&rec[2 * s1 + 1]);
+        float4 p0, h0, p1, h1;
+        ld_record(rec + 2 * s0, p0, h0);
+        ld_record(rec + 2 * s1, p1, h1);
         float ax = pi.x - p0.x, ay = pi.y - p0.y, az = pi.z - p0.z;
         term(p0, h0, ax, ay, az, ax * ax + ay * ay + az * az);
         float bx = pi.x - p1.x, by = pi.y - p1.y, bz = pi.z - p1.z;
@@ -681,7 +689,8 @@ k_xsph_drift(KP kp, int n, const float* __restrict__ dtp, const float4* __restri
       }
       if (c < cnt) {
         int s = (int)__ldg(&nbr[nbr_index(c, n, i)]);
-        float4 pj = __ldg(&rec[2 * s]), vh = __ldg(&rec[2 * s + 1]);
+        float4 pj, vh;
+        ld_record(rec + 2 * s, pj, vh);
         float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
         term(pj, vh, dx, dy, dz, dx * dx + dy * dy + dz * dz);
       }
