@@ -957,15 +957,23 @@ k_density(KP kp, int n, const float* __restrict__ dtp, const float4* __restrict_
     if (CL) ssum += __ldg(&rv[s]).y * w;
   };
   if (listed <= kNbrCap) {
-    uint32_t c = 0;
-    for (; c + 1 < listed; c += 2) {
-      uint2 e = *reinterpret_cast<const uint2*>(nbr + nbr_index(c, n, i));  // written above by this thread
-      int s0 = (int)e.x, s1 = (int)e.y;
+    auto pair = [&](int s0, int s1) {
       float4 p0 = __ldg(&pos[s0]), p1 = __ldg(&pos[s1]);
       float ax = pi.x - p0.x, ay = pi.y - p0.y, az = pi.z - p0.z;
       term(s0, p0, ax, ay, az, ax * ax + ay * ay + az * az);
       float bx = pi.x - p1.x, by = pi.y - p1.y, bz = pi.z - p1.z;
       term(s1, p1, bx, by, bz, bx * bx + by * by + bz * bz);
+    };
+    // the list was written above by this thread: plain (coherent) loads
+    uint32_t c = 0;
+    for (; c + 3 < listed; c += 4) {
+      uint4 e = *reinterpret_cast<const uint4*>(nbr + nbr_index(c, n, i));
+      pair((int)e.x, (int)e.y);
+      pair((int)e.z, (int)e.w);
+    }
+    for (; c + 1 < listed; c += 2) {
+      uint2 e = *reinterpret_cast<const uint2*>(nbr + nbr_index(c, n, i));
+      pair((int)e.x, (int)e.y);
     }
     if (c < listed) {
       int s = (int)nbr[nbr_index(c, n, i)];
