@@ -771,7 +771,10 @@ int create_impl(int ninst, const SphParams* PP, const SphParticlesView* pvs,
   h->ninst = ninst;
   h->n = (int)ntot;
   h->nb = (int)nbtot;
+  std::thread allocator;  // device arrays, allocated while the host builds tables and packs
+  cudaError_t ae = cudaSuccess;
   auto fail = [&](int code) {
+    if (allocator.joinable()) allocator.join();
     free_all(h);
     delete h;
     return code;
@@ -788,6 +791,50 @@ int create_impl(int ninst, const SphParams* PP, const SphParticlesView* pvs,
   h->boff.assign(ninst + 1, 0);
   h->init_e.assign(ninst, 0.0);
   h->init_m.assign(ninst, 0.0);
+  // grid sizes first: they size the device arrays, which another thread
+  // allocates while this one builds the cell ranks and boundary lists
+  uint64_t Ctot = 0;
+  for (int q = 0; q < ninst; ++q) {
+    float cell = 2.0f * PP[q].h;
+    uint64_t Cq = 1;
+    for (int a = 0; a < 3; ++a) {
+      uint32_t d = (uint32_t)fmaxf(ceilf((PP[q].domain_max[a] - PP[q].domain_min[a]) / cell), 1.0f);
+      if (d > (1u << 21)) return fail(SPH_ERR_INVALID_ARG);
+      Cq *= d;
+    }
+    if (Ctot + Cq > (1ull << 30)) return fail(SPH_ERR_INVALID_ARG);
+    Ctot += Cq;
+  }
+  const size_t n = (size_t)h->n, nb = (size_t)h->nb;
+  h->C = (int)Ctot;
+  h->nbsum = grid_for(h->C, sph::kScanTile);
+  h->nparts = std::max(1, std::min(grid_for((long long)n, sph::kMetricThreads), 1184));
+  allocator = std::thread([&, Ctot] {
+    const uint64_t C = Ctot;
+    if (cudaSetDevice(h->dev) != cudaSuccess) {
+      ae = cudaErrorInvalidDevice;
+      return;
+    }
+    ae = cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking);
+#define ALLOC(ptr, cnt) \
+  if (ae == cudaSuccess) ae = dalloc(h, &h->ptr, (cnt))
+    ALLOC(pos, n); ALLOC(vel, n); ALLOC(velout, n); ALLOC(acc, n);
+    ALLOC(rv, n); ALLOC(rf, n); ALLOC(pr, n); ALLOC(id, n);
+    ALLOC(posU, n); ALLOC(velU, n); ALLOC(idU, n); ALLOC(keyU, n); ALLOC(tmp, n); ALLOC(tmpid, n);
+    ALLOC(hist, C); ALLOC(cstart, C); ALLOC(ccount, C); ALLOC(cursor, C); ALLOC(bsum, h->nbsum);
+    ALLOC(rank_of_lin, C); ALLOC(lin_of_rank, C); ALLOC(ctab, C);
+    ALLOC(bpos, nb); ALLOC(bpress, nb); ALLOC(bact, nb); ALLOC(bc_start, C + 1);
+    ALLOC(dt, ninst); ALLOC(dt_query, ninst); ALLOC(red, 2 * ninst); ALLOC(err, 1); ALLOC(hcc, ninst);
+    ALLOC(part_m, h->nparts); ALLOC(part_e, h->nparts); ALLOC(part_var, h->nparts); ALLOC(me, 2);
+    ALLOC(var, 1); ALLOC(bad, 1);
+    ALLOC(stage, 12 * n); ALLOC(stage_ft, n); ALLOC(diag, 2);
+    ALLOC(nbr, (size_t)sph::kNbrCap * n); ALLOC(ncount, n); ALLOC(xrec, 2 * n);
+    if (ninst > 1) {
+      ALLOC(ktab, ninst); ALLOC(inst_p, n); ALLOC(inst_b, nb);
+    }
+    if (sdf_mode) ALLOC(sdf, std::max<uint64_t>(sdf_nodes, 1));
+#undef ALLOC
+  });
   uint64_t C = 0;
   bstart.push_back(0);
   for (int q = 0; q < ninst; ++q) {
@@ -797,12 +844,10 @@ int create_impl(int ninst, const SphParams* PP, const SphParticlesView* pvs,
     uint32_t dims[3];
     float cell = 2.0f * P.h;
     uint64_t Cq = 1;
-    for (int a = 0; a < 3; ++a) {
+    for (int a = 0; a < 3; ++a) {  // as above (checked there)
       dims[a] = (uint32_t)fmaxf(ceilf((P.domain_max[a] - P.domain_min[a]) / cell), 1.0f);
       Cq *= dims[a];
-      if (dims[a] > (1u << 21)) return fail(SPH_ERR_INVALID_ARG);
     }
-    if (C + Cq > (1ull << 30)) return fail(SPH_ERR_INVALID_ARG);
     SimConst k = make_const(P, dims);
     k.rows = P.cell_order == SPH_CELL_ORDER_LINEAR || P.cell_order == SPH_CELL_ORDER_ROWS;
     k.inst = q;
@@ -904,61 +949,39 @@ int create_impl(int ninst, const SphParams* PP, const SphParticlesView* pvs,
   h->k = h->ktab_h[0];
 
   // upload staging (particles of instance q at [poff[q], poff[q+1]), ids
-  // global), left uninitialised: every entry is written by the packing
-  // thread (and its helpers, which also take the first-touch page faults)
-  // while this thread allocates the device arrays
-  size_t n = (size_t)h->n, nb = (size_t)h->nb;
+  // global), left uninitialised: every entry is written below, by host
+  // threads that also take the first-touch page faults, while the device
+  // arrays are being allocated
   std::unique_ptr<float4[]> hpos(new float4[n]), hvel(new float4[n]), hacc(new float4[n]), hb(new float4[nb]);
   std::unique_ptr<uint32_t[]> hid(new uint32_t[n]);
   std::unique_ptr<float[]> hpr(new float[n]);
   std::vector<uint16_t> hip(ninst > 1 ? n : 0), hib(ninst > 1 ? nb : 0);
   h->temperature.resize(n);
-  std::thread packer([&] {
-    for (int q = 0; q < ninst; ++q) {
-      const SphParticlesView* pv = &pvs[q];
-      size_t o = h->poff[q];
-      parallel_chunks(pv->n, kHostThreads, [&](unsigned, size_t i0, size_t i1) {
-        for (size_t i = i0; i < i1; ++i) {
-          hpos[o + i] = make_float4(pv->x[i], pv->y[i], pv->z[i], pv->mass[i]);
-          hvel[o + i] = make_float4(pv->vx[i], pv->vy[i], pv->vz[i], pv->density[i]);
-          hacc[o + i] = make_float4(pv->ax[i], pv->ay[i], pv->az[i], 0.0f);
-          hid[o + i] = (uint32_t)(o + i) | (pv->fluid_type[i] ? sph::kAirBit : 0u);
-          hpr[o + i] = pv->pressure[i];
-          h->temperature[o + i] = pv->temperature[i];
-          if (ninst > 1) hip[o + i] = (uint16_t)q;
-        }
-      });
-      const SphBoundaryView* bv = (sdf_mode || !bvs) ? nullptr : bvs[q];
-      size_t bo = h->boff[q];
-      for (size_t i = 0; bv && i < bv->n; ++i) {
-        hb[bo + i] = make_float4(bv->x[i], bv->y[i], bv->z[i], bv->mass[i]);
-        if (ninst > 1) hib[bo + i] = (uint16_t)q;
+  for (int q = 0; q < ninst; ++q) {
+    const SphParticlesView* pv = &pvs[q];
+    size_t o = h->poff[q];
+    parallel_chunks(pv->n, kHostThreads, [&](unsigned, size_t i0, size_t i1) {
+      for (size_t i = i0; i < i1; ++i) {
+        hpos[o + i] = make_float4(pv->x[i], pv->y[i], pv->z[i], pv->mass[i]);
+        hvel[o + i] = make_float4(pv->vx[i], pv->vy[i], pv->vz[i], pv->density[i]);
+        hacc[o + i] = make_float4(pv->ax[i], pv->ay[i], pv->az[i], 0.0f);
+        hid[o + i] = (uint32_t)(o + i) | (pv->fluid_type[i] ? sph::kAirBit : 0u);
+        hpr[o + i] = pv->pressure[i];
+        h->temperature[o + i] = pv->temperature[i];
+        if (ninst > 1) hip[o + i] = (uint16_t)q;
       }
+    });
+    const SphBoundaryView* bv = (sdf_mode || !bvs) ? nullptr : bvs[q];
+    size_t bo = h->boff[q];
+    for (size_t i = 0; bv && i < bv->n; ++i) {
+      hb[bo + i] = make_float4(bv->x[i], bv->y[i], bv->z[i], bv->mass[i]);
+      if (ninst > 1) hib[bo + i] = (uint16_t)q;
     }
-  });
-  cudaError_t e = cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking);
-  h->nbsum = grid_for(h->C, sph::kScanTile);
-  h->nparts = std::max(1, std::min(grid_for((long long)n, sph::kMetricThreads), 1184));
-#define ALLOC(ptr, cnt) \
-  if (e == cudaSuccess) e = dalloc(h, &h->ptr, (cnt))
-  ALLOC(pos, n); ALLOC(vel, n); ALLOC(velout, n); ALLOC(acc, n);
-  ALLOC(rv, n); ALLOC(rf, n); ALLOC(pr, n); ALLOC(id, n);
-  ALLOC(posU, n); ALLOC(velU, n); ALLOC(idU, n); ALLOC(keyU, n); ALLOC(tmp, n); ALLOC(tmpid, n);
-  ALLOC(hist, C); ALLOC(cstart, C); ALLOC(ccount, C); ALLOC(cursor, C); ALLOC(bsum, h->nbsum);
-  ALLOC(rank_of_lin, C); ALLOC(lin_of_rank, C); ALLOC(ctab, C);
-  ALLOC(bpos, nb); ALLOC(bpress, nb); ALLOC(bact, nb); ALLOC(bc_start, C + 1); ALLOC(bc_list, blist.size());
-  ALLOC(dt, ninst); ALLOC(dt_query, ninst); ALLOC(red, 2 * ninst); ALLOC(err, 1); ALLOC(hcc, ninst);
-  ALLOC(part_m, h->nparts); ALLOC(part_e, h->nparts); ALLOC(part_var, h->nparts); ALLOC(me, 2);
-  ALLOC(var, 1); ALLOC(bad, 1);
-  ALLOC(stage, 12 * n); ALLOC(stage_ft, n); ALLOC(diag, 2);
-  ALLOC(nbr, (size_t)sph::kNbrCap * n); ALLOC(ncount, n); ALLOC(xrec, 2 * n);
-  if (ninst > 1) {
-    ALLOC(ktab, ninst); ALLOC(inst_p, n); ALLOC(inst_b, nb);
   }
-  if (sdf_mode) ALLOC(sdf, std::max<uint64_t>(sdf_nodes, 1));
-  if (sdf_mode) ALLOC(wall_tab, wall_host.size());
-#undef ALLOC
-  packer.join();
+  allocator.join();
+  cudaError_t e = ae;
+  if (e == cudaSuccess) e = dalloc(h, &h->bc_list, blist.size());
+  if (e == cudaSuccess && sdf_mode) e = dalloc(h, &h->wall_tab, wall_host.size());
   if (e != cudaSuccess) return fail(e == cudaErrorMemoryAllocation ? SPH_ERR_OOM : SPH_ERR_CUDA);
 
   float4* accU = nullptr;
