@@ -144,7 +144,7 @@ def test_two_particle_newton3_on_gpu():
 
 
 def test_dam_break_100_steps_bit_exact_and_within_tolerance_of_powf():
-    """BASELINE config 1 inputs (31,250 particles, 52,500 wall particles)."""
+    """The 4 mm dam break: 31,250 particles, 52,500 wall particles."""
     sc = domain.dam_break(0.004, seed=1234, with_sdf=False)
     gpu, cpu = make_pair(sc, pow_mode=1)
     ref = orc.OracleKernel(*sc.kernel_args(), alpha=sc.alpha, tier=1, threads=8, pow_mode=0)
@@ -249,10 +249,10 @@ def test_health_counts_nonfinite():
     assert k.health() == 1
 
 
-# ---- BASELINE config 2 scale -------------------------------------------------------
+# ---- the 1 mm dam break with the sphere: 2,000,000 particles ----------------------
 
 def test_dam_break_sphere_2m_particles_one_step_bit_exact_and_invariants():
-    """BASELINE config 2 inputs: 2,000,000 particles at dx = 1 mm with the sphere."""
+    """The 1 mm dam break with the sphere: 2,000,000 particles."""
     sc = domain.dam_break(0.001, seed=2024, sphere=True)
     assert len(sc.particles) == 2_000_000
     gpu, cpu = make_pair(sc, threads=16)
@@ -294,7 +294,7 @@ def test_sdf_mode_bit_exact_with_sphere():
     assert_same(gpu.particles(), cpu.particles())
 
 
-# ---- force extraction on the sphere (BASELINE config 2 reports these) ------------
+# ---- force extraction on the sphere of the 1 mm dam break ----------------------
 
 def test_surface_and_body_forces_on_sphere():
     sc = domain.tank_with_sphere(0.004, seed=41, velocity=(0.3, 0.0, 0.0))
