@@ -35,9 +35,10 @@ constexpr int kCellCap = 4096;         // particles per cell for the id ranking
 constexpr uint32_t kNbrCap = 128;      // listed neighbours per particle
 constexpr uint32_t kNbrChunk = 8;      // list entries per 32-byte chunk
 // The neighbour kernels are latency-bound on gathered loads, so occupancy
-// pays more than registers: k_density, k_forces and k_xsph_drift are capped
-// at 48 registers (__maxnreg__ below; measured at 2M particles against the
-// compiler's 58-64 and against caps of 40 and 56, same results).
+// pays more than registers: k_density and k_forces are capped at 48
+// registers, k_xsph_drift (whose 256-bit record loads want more in flight)
+// at 56 (__maxnreg__ below; each measured at 2M particles against caps of
+// 40, 48, 56, 64 and 72 and the compiler's choice, same results).
 
 enum : uint32_t { kFlagDelta = 1, kFlagXsph = 2, kFlagRepulsion = 4, kFlagClamp = 8 };
 enum : uint32_t { kErrCellCap = 1, kErrAdamiCap = 2 };
@@ -633,7 +634,7 @@ k_xsph_prep(KP kp, int n, const float* __restrict__ dtp, const float4* __restric
 // (neighbor.rs:89-101) into a rank-indexed histogram. Reads the sorted state,
 // writes the unsorted "U" arrays in the same slot order.
 template <class KP>
-__global__ void __maxnreg__(48)
+__global__ void __maxnreg__(56)
 k_xsph_drift(KP kp, int n, const float* __restrict__ dtp, const float4* __restrict__ pos,
              const float4* __restrict__ velout, const float4* __restrict__ acc, const float4* __restrict__ rec,
              const uint32_t* __restrict__ id, const uint2* __restrict__ ctab,
