@@ -35,10 +35,10 @@ constexpr int kCellCap = 4096;         // particles per cell for the id ranking
 constexpr uint32_t kNbrCap = 128;      // listed neighbours per particle
 constexpr uint32_t kNbrChunk = 8;      // list entries per 32-byte chunk
 // The neighbour kernels are latency-bound on gathered loads, so occupancy
-// pays more than registers: k_density and k_forces are capped at 48
-// registers, k_xsph_drift (whose 256-bit record loads want more in flight)
-// at 56 (__maxnreg__ below; each measured at 2M particles against caps of
-// 40, 48, 56, 64 and 72 and the compiler's choice, same results).
+// pays more than registers: k_density is capped at 48 registers, k_forces
+// and k_xsph_drift (whose replays put two neighbours' gathers in flight
+// before using them) at 56 (__maxnreg__ below; each measured at 2M particles
+// against caps from 40 to 72 and the compiler's choice, same results).
 
 enum : uint32_t { kFlagDelta = 1, kFlagXsph = 2, kFlagRepulsion = 4, kFlagClamp = 8 };
 enum : uint32_t { kErrCellCap = 1, kErrAdamiCap = 2 };
@@ -551,48 +551,6 @@ __device__ __forceinline__ size_t nbr_index(uint32_t c, int n, int i) {
 // entries c and c + 1 of slot i, c even (one 8-byte load)
 __device__ __forceinline__ uint2 nbr_pair(const uint32_t* __restrict__ nbr, uint32_t c, int n, int i) {
   return __ldg(reinterpret_cast<const uint2*>(nbr + nbr_index(c, n, i)));
-}
-
-// Same visit as for_each_neighbor, replayed from the neighbour list that
-// k_density recorded on this grid (slots in visit order, see nbr_index).
-// Particles whose list overflowed kNbrCap, and calls without a list, scan.
-template <class F>
-__device__ __forceinline__ void visit_neighbors(int i, int n, float px, float py, float pz,
-                                                const float4* __restrict__ pos,
-                                                const uint2* __restrict__ ctab,
-                                                const uint32_t* __restrict__ nbr,
-                                                const uint32_t* __restrict__ ncount,
-                                                const SimConst& k, F&& f) {
-  uint32_t cnt = nbr ? __ldg(&ncount[i]) : 0xffffffffu;
-  if (cnt <= kNbrCap) {
-    // two neighbours per iteration: both list entries and both positions are
-    // loaded before either is used (same order of f calls)
-    uint32_t c = 0;
-    auto pair = [&](int s0, int s1) {
-      float4 p0 = __ldg(&pos[s0]), p1 = __ldg(&pos[s1]);
-      float ax = px - p0.x, ay = py - p0.y, az = pz - p0.z;
-      f(s0, p0, ax, ay, az, ax * ax + ay * ay + az * az);
-      float bx = px - p1.x, by = py - p1.y, bz = pz - p1.z;
-      f(s1, p1, bx, by, bz, bx * bx + by * by + bz * bz);
-    };
-    for (; c + 3 < cnt; c += 4) {
-      uint4 e = __ldg(reinterpret_cast<const uint4*>(nbr + nbr_index(c, n, i)));
-      pair((int)e.x, (int)e.y);
-      pair((int)e.z, (int)e.w);
-    }
-    for (; c + 1 < cnt; c += 2) {
-      uint2 e = nbr_pair(nbr, c, n, i);
-      pair((int)e.x, (int)e.y);
-    }
-    if (c < cnt) {
-      int s = (int)__ldg(&nbr[nbr_index(c, n, i)]);
-      float4 pj = __ldg(&pos[s]);
-      float ddx = px - pj.x, ddy = py - pj.y, ddz = pz - pj.z;
-      f(s, pj, ddx, ddy, ddz, ddx * ddx + ddy * ddy + ddz * ddz);
-    }
-  } else {
-    for_each_neighbor(px, py, pz, i, pos, ctab, k, f);
-  }
 }
 
 // ---------------------------------------------------------------------------
@@ -1306,7 +1264,7 @@ k_adami(KP kp, int nb, const float4* __restrict__ bpos, float* __restrict__ bpre
 // repulsion (lib.rs:247-282; sph.rs:322-508; boundary.rs:143-181), then
 // kick 2 (lib.rs:330-334) and the dt reduction inputs (sph.rs:597-616).
 template <class KP, int CL>
-__global__ void __maxnreg__(48)
+__global__ void __maxnreg__(56)
 k_forces(KP kp, int n, const float* __restrict__ dtp, float hdt_scale,
          const float4* __restrict__ pos, const float4* __restrict__ vel,
          const float2* __restrict__ rf, const float* __restrict__ pr,
@@ -1331,30 +1289,63 @@ k_forces(KP kp, int n, const float* __restrict__ dtp, float hdt_scale,
     float fpx = 0.0f, fpy = 0.0f, fpz = 0.0f;
     float fvx = 0.0f, fvy = 0.0f, fvz = 0.0f;
     float neg_mi = -pi.w;
-    visit_neighbors(i, n, pi.x, pi.y, pi.z, pos, ctab, nbr, ncount, k,
-                      [&](int s, const float4& pj, float dx, float dy, float dz, float d2) {
-                        float r = sqrtf(d2);
-                        float gx, gy, gz;
-                        grad_c2(dx, dy, dz, r, k, gx, gy, gz);
-                        float2 rfj = __ldg(&rf[s]);
-                        float factor = neg_mi * pj.w * (rfi.y + rfj.y);
-                        fpx += factor * gx;
-                        fpy += factor * gy;
-                        fpz += factor * gz;
-                        float4 vj = __ldg(&vel[s]);
-                        float dvx = vi.x - vj.x, dvy = vi.y - vj.y, dvz = vi.z - vj.z;
-                        float vr_dot = dvx * dx + dvy * dy + dvz * dz;
-                        if (vr_dot < 0.0f) {
-                          float r_sq = r * r;
-                          float mu = k.h * vr_dot / (r_sq + k.eta_sq);
-                          float rho_avg = 0.5f * (rho_i + rfj.x);
-                          float pi_ij = (k.neg_alpha_c * mu + k.beta * mu * mu) / rho_avg;
-                          float fv = -pj.w * pi_ij;
-                          fvx += fv * gx;
-                          fvy += fv * gy;
-                          fvz += fv * gz;
-                        }
-                      });
+    // one neighbour's terms, its position, velocity and (rho, p / rho^2) given
+    auto term = [&](const float4& pj, const float4& vj, const float2& rfj, float dx, float dy, float dz,
+                    float d2) {
+      float r = sqrtf(d2);
+      float gx, gy, gz;
+      grad_c2(dx, dy, dz, r, k, gx, gy, gz);
+      float factor = neg_mi * pj.w * (rfi.y + rfj.y);
+      fpx += factor * gx;
+      fpy += factor * gy;
+      fpz += factor * gz;
+      float dvx = vi.x - vj.x, dvy = vi.y - vj.y, dvz = vi.z - vj.z;
+      float vr_dot = dvx * dx + dvy * dy + dvz * dz;
+      if (vr_dot < 0.0f) {
+        float r_sq = r * r;
+        float mu = k.h * vr_dot / (r_sq + k.eta_sq);
+        float rho_avg = 0.5f * (rho_i + rfj.x);
+        float pi_ij = (k.neg_alpha_c * mu + k.beta * mu * mu) / rho_avg;
+        float fv = -pj.w * pi_ij;
+        fvx += fv * gx;
+        fvy += fv * gy;
+        fvz += fv * gz;
+      }
+    };
+    uint32_t cnt = nbr ? __ldg(&ncount[i]) : 0xffffffffu;
+    if (cnt <= kNbrCap) {
+      // both neighbours' gathers (position, velocity, density) issued before either term
+      auto pair = [&](int s0, int s1) {
+        float4 p0 = __ldg(&pos[s0]), p1 = __ldg(&pos[s1]);
+        float4 v0 = __ldg(&vel[s0]), v1 = __ldg(&vel[s1]);
+        float2 f0 = __ldg(&rf[s0]), f1 = __ldg(&rf[s1]);
+        float ax = pi.x - p0.x, ay = pi.y - p0.y, az = pi.z - p0.z;
+        term(p0, v0, f0, ax, ay, az, ax * ax + ay * ay + az * az);
+        float bx = pi.x - p1.x, by = pi.y - p1.y, bz = pi.z - p1.z;
+        term(p1, v1, f1, bx, by, bz, bx * bx + by * by + bz * bz);
+      };
+      uint32_t c = 0;
+      for (; c + 3 < cnt; c += 4) {
+        uint4 e = __ldg(reinterpret_cast<const uint4*>(nbr + nbr_index(c, n, i)));
+        pair((int)e.x, (int)e.y);
+        pair((int)e.z, (int)e.w);
+      }
+      for (; c + 1 < cnt; c += 2) {
+        uint2 e = nbr_pair(nbr, c, n, i);
+        pair((int)e.x, (int)e.y);
+      }
+      if (c < cnt) {
+        int s = (int)__ldg(&nbr[nbr_index(c, n, i)]);
+        float4 pj = __ldg(&pos[s]);
+        float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
+        term(pj, __ldg(&vel[s]), __ldg(&rf[s]), dx, dy, dz, dx * dx + dy * dy + dz * dz);
+      }
+    } else {
+      for_each_neighbor(pi.x, pi.y, pi.z, i, pos, ctab, k,
+                        [&](int s, const float4& pj, float dx, float dy, float dz, float d2) {
+                          term(pj, __ldg(&vel[s]), __ldg(&rf[s]), dx, dy, dz, d2);
+                        });
+    }
     int lin = cell_hash(axis_cell(pi.x, k.gmin[0], k.cell, k.dims[0]),
                         axis_cell(pi.y, k.gmin[1], k.cell, k.dims[1]),
                         axis_cell(pi.z, k.gmin[2], k.cell, k.dims[2]), k);
