@@ -901,27 +901,30 @@ k_density(KP kp, int n, const float* __restrict__ dtp, const float4* __restrict_
   if (listed < kNbrCap && listed % kNbrChunk != 0) flush(listed / kNbrChunk);  // the open chunk
   ncount[i] = listed;
   // Phase 2: density and delta-SPH terms over the list, same order.
-  auto term = [&](int s, const float4& pj, float dx, float dy, float dz, float d2) {
+  auto term_rv = [&](const float4& pj, const float2& rvj, float dx, float dy, float dz, float d2) {
     float r = sqrtf(d2);
     if (delta) {
       float gx, gy, gz;
       grad_c2(dx, dy, dz, r, k, gx, gy, gz);
-      float2 rvj = __ldg(&rv[s]);
       float r_dot_grad = dx * gx + dy * gy + dz * gz;
       float density_diff = rho_old_i - rvj.x;
       diff_sum += rvj.y * density_diff * 2.0f * r_dot_grad / (d2 + k.eta_sq);
     }
     float w = w_c2(r, k);
     rho += pj.w * w;
-    if (CL) ssum += __ldg(&rv[s]).y * w;
+    if (CL) ssum += rvj.y * w;
+  };
+  auto term = [&](int s, const float4& pj, float dx, float dy, float dz, float d2) {
+    term_rv(pj, __ldg(&rv[s]), dx, dy, dz, d2);
   };
   if (listed <= kNbrCap) {
-    auto pair = [&](int s0, int s1) {
+    auto pair = [&](int s0, int s1) {  // both neighbours' gathers in flight before either term
       float4 p0 = __ldg(&pos[s0]), p1 = __ldg(&pos[s1]);
+      float2 r0 = __ldg(&rv[s0]), r1 = __ldg(&rv[s1]);
       float ax = pi.x - p0.x, ay = pi.y - p0.y, az = pi.z - p0.z;
-      term(s0, p0, ax, ay, az, ax * ax + ay * ay + az * az);
+      term_rv(p0, r0, ax, ay, az, ax * ax + ay * ay + az * az);
       float bx = pi.x - p1.x, by = pi.y - p1.y, bz = pi.z - p1.z;
-      term(s1, p1, bx, by, bz, bx * bx + by * by + bz * bz);
+      term_rv(p1, r1, bx, by, bz, bx * bx + by * by + bz * bz);
     };
     // the list was written above by this thread: plain (coherent) loads
     uint32_t c = 0;
