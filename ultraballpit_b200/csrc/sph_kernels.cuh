@@ -950,8 +950,7 @@ k_density(KP kp, int n, const float* __restrict__ dtp, const float4* __restrict_
                       axis_cell(pi.y, k.gmin[1], k.cell, k.dims[1]),
                       axis_cell(pi.z, k.gmin[2], k.cell, k.dims[2]), k);
   uint32_t b0 = __ldg(&bc_start[k.coff + lin]), b1 = __ldg(&bc_start[k.coff + lin + 1]);
-  for (uint32_t q = b0; q < b1; ++q) {
-    float4 bp = __ldg(&bpos[__ldg(&bc_list[q])]);
+  auto bterm = [&](const float4& bp) {
     float dx = pi.x - bp.x, dy = pi.y - bp.y, dz = pi.z - bp.z;
     float d2 = dx * dx + dy * dy + dz * dz;
     if (d2 <= k.sup_d2) {
@@ -959,7 +958,15 @@ k_density(KP kp, int n, const float* __restrict__ dtp, const float4* __restrict_
       rho += wb;
       if (CL) { rho_wall += wb; ++nwall; }
     }
+  };
+  uint32_t q = b0;
+  for (; q + 1 < b1; q += 2) {  // two candidates' loads in flight, terms in order
+    uint32_t i0 = __ldg(&bc_list[q]), i1 = __ldg(&bc_list[q + 1]);
+    float4 bp0 = __ldg(&bpos[i0]), bp1 = __ldg(&bpos[i1]);
+    bterm(bp0);
+    bterm(bp1);
   }
+  if (q < b1) bterm(__ldg(&bpos[__ldg(&bc_list[q])]));
   bool air = (id[i] & kAirBit) != 0;
   float wall_m = 0.0f;
   if (k.sdf_mode) {  // kernel mass of the walls: box faces and obstacle
@@ -1359,9 +1366,7 @@ k_forces(KP kp, int n, const float* __restrict__ dtp, float hdt_scale,
       float pic_over = pic / (rho_i * rho_i);
       float brho = air ? kAirRho0 : kWaterRho0;
       float brho2 = brho * brho;
-      for (uint32_t q = b0; q < b1; ++q) {
-        uint32_t bi = __ldg(&bc_list[q]);
-        float4 bp = __ldg(&bpos[bi]);
+      auto bterm = [&](uint32_t bi, const float4& bp) {
         float dx = pi.x - bp.x, dy = pi.y - bp.y, dz = pi.z - bp.z;
         float d2 = dx * dx + dy * dy + dz * dz;
         if (d2 <= k.sup_d2) {
@@ -1374,6 +1379,17 @@ k_forces(KP kp, int n, const float* __restrict__ dtp, float hdt_scale,
           fpy += factor * gy;
           fpz += factor * gz;
         }
+      };
+      uint32_t q = b0;
+      for (; q + 1 < b1; q += 2) {  // two candidates' loads in flight, terms in order
+        uint32_t i0 = __ldg(&bc_list[q]), i1 = __ldg(&bc_list[q + 1]);
+        float4 bp0 = __ldg(&bpos[i0]), bp1 = __ldg(&bpos[i1]);
+        bterm(i0, bp0);
+        bterm(i1, bp1);
+      }
+      if (q < b1) {
+        uint32_t bi = __ldg(&bc_list[q]);
+        bterm(bi, __ldg(&bpos[bi]));
       }
     }
     float ax = 0.0f + fpx / pi.w, ay = 0.0f + fpy / pi.w, az = 0.0f + fpz / pi.w;
@@ -1439,8 +1455,7 @@ k_forces(KP kp, int n, const float* __restrict__ dtp, float hdt_scale,
       }
     }
     if ((k.flags & kFlagRepulsion) && b1 > b0) {
-      for (uint32_t q = b0; q < b1; ++q) {
-        float4 bp = __ldg(&bpos[__ldg(&bc_list[q])]);
+      auto rterm = [&](const float4& bp) {
         float dx = pi.x - bp.x, dy = pi.y - bp.y, dz = pi.z - bp.z;
         float d2 = dx * dx + dy * dy + dz * dz;
         if (d2 <= k.r0_d2 && d2 > k.tiny_d2) {
@@ -1452,7 +1467,15 @@ k_forces(KP kp, int n, const float* __restrict__ dtp, float hdt_scale,
           ay += force_mag * dy * inv_r;
           az += force_mag * dz * inv_r;
         }
+      };
+      uint32_t q = b0;
+      for (; q + 1 < b1; q += 2) {
+        uint32_t i0 = __ldg(&bc_list[q]), i1 = __ldg(&bc_list[q + 1]);
+        float4 bp0 = __ldg(&bpos[i0]), bp1 = __ldg(&bpos[i1]);
+        rterm(bp0);
+        rterm(bp1);
       }
+      if (q < b1) rterm(__ldg(&bpos[__ldg(&bc_list[q])]));
     }
     if (CL) {  // learned near-wall correction (k_closure_apply)
       float4 cr = corr[i];
