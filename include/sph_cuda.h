@@ -178,15 +178,18 @@ typedef struct SphGridInfo {
   uint64_t boundary_candidates; /* entries of the static per-cell boundary lists */
 } SphGridInfo;
 
-/* Fill `p` with the reference defaults: alpha 1, beta 2, Morton order, all
- * reference stages on, boundary particles, device 0. */
+/* Fill `p` with the reference defaults: alpha 1, beta 2, all reference
+ * stages on, boundary particles, device 0; cell order SPH_CELL_ORDER_ROWS
+ * (storage order only: the physics is the same in every order). */
 void sph_params_default(SphParams *p);
 
 /* CpuKernel::new / GpuKernel::new (lib.rs:138-174, gpu/mod.rs:190-200).
  * `boundary` may be NULL (no walls). With SPH_BOUNDARY_SDF the walls are
  * the faces of the domain box (which must span at least 4h on every axis)
  * plus the obstacle whose SDF `sdf` gives (NULL, or NULL distances: no
- * obstacle); otherwise `sdf` is ignored. */
+ * obstacle); otherwise `sdf` is ignored. Creation uses the host's hardware
+ * threads (up to 32) for its tables and allocates the device arrays on a
+ * second thread; it returns once the handle is ready. */
 int sph_create(const SphParams *params, const SphParticlesView *particles,
                const SphBoundaryView *boundary, const SphSdfView *sdf, SphHandle **out);
 void sph_destroy(SphHandle *h);
