@@ -404,7 +404,11 @@ void parallel_chunks(size_t n, unsigned max_threads, F&& f) {
   for (unsigned t = 0; t < T; ++t) {
     size_t a = (size_t)t * chunk, e = std::min(n, a + chunk);
     if (a >= e) break;
-    ts.emplace_back([&f, t, a, e] { f(t, a, e); });
+    try {
+      ts.emplace_back([&f, t, a, e] { f(t, a, e); });
+    } catch (...) {  // no thread to be had: this chunk runs here
+      f(t, a, e);
+    }
   }
   for (std::thread& th : ts) th.join();
 }
@@ -417,7 +421,13 @@ void run_threads(unsigned T, F&& f) {
     return;
   }
   std::vector<std::thread> ts;
-  for (unsigned t = 0; t < T; ++t) ts.emplace_back([&f, t] { f(t); });
+  for (unsigned t = 0; t < T; ++t) {
+    try {
+      ts.emplace_back([&f, t] { f(t); });
+    } catch (...) {  // no thread to be had: this part runs here
+      f(t);
+    }
+  }
   for (std::thread& th : ts) th.join();
 }
 
@@ -809,7 +819,7 @@ int create_impl(int ninst, const SphParams* PP, const SphParticlesView* pvs,
   h->C = (int)Ctot;
   h->nbsum = grid_for(h->C, sph::kScanTile);
   h->nparts = std::max(1, std::min(grid_for((long long)n, sph::kMetricThreads), 1184));
-  allocator = std::thread([&, Ctot] {
+  auto allocate_all = [&, Ctot] {
     const uint64_t C = Ctot;
     if (cudaSetDevice(h->dev) != cudaSuccess) {
       ae = cudaErrorInvalidDevice;
@@ -834,7 +844,12 @@ int create_impl(int ninst, const SphParams* PP, const SphParticlesView* pvs,
     }
     if (sdf_mode) ALLOC(sdf, std::max<uint64_t>(sdf_nodes, 1));
 #undef ALLOC
-  });
+  };
+  try {
+    allocator = std::thread(allocate_all);
+  } catch (...) {  // no thread to be had: allocate here, before the host tables
+    allocate_all();
+  }
   uint64_t C = 0;
   bstart.push_back(0);
   for (int q = 0; q < ninst; ++q) {
