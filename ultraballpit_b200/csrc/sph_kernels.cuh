@@ -1146,9 +1146,9 @@ k_adami(KP kp, int nb, const float4* __restrict__ bpos, float* __restrict__ bpre
   // Lanes look up the (at most 4x4x4) cells of the range in parallel; only
   // occupied cells whose box comes within 2h are then scanned (the box is
   // widened by a margin far above the rounding of the binning, edge cells
-  // unbounded outward, as particles outside the domain are binned there).
-  // The terms are sorted by fluid index below, so the cell order does not
-  // matter.
+  // unbounded outward, as particles outside the domain are binned there),
+  // their candidates taken 32 at a time across cells. The terms are sorted
+  // by fluid index below, so the order of the candidates does not matter.
   int nx = hi[0] - lo[0] + 1, ny = hi[1] - lo[1] + 1, nz = hi[2] - lo[2] + 1;
   int ncell = nx * ny * nz;
   const float margin = 1.0e-5f * k.cell + 1.0e-6f;
@@ -1168,18 +1168,32 @@ k_adami(KP kp, int nb, const float4* __restrict__ bpos, float* __restrict__ bpre
       }
       if (gap2 <= k.radius_sq) mine = __ldg(&ctab[k.coff + cell_hash(c3[0], c3[1], c3[2], k)]);
     }
-    unsigned occupied = __ballot_sync(0xffffffffu, mine.y > 0u);
-    while (occupied) {
-      int src = __ffs(occupied) - 1;
-      occupied &= occupied - 1u;
+    // the candidates of this round's cells as one stream, 32 at a time: lane
+    // l takes candidate t = base + l, which lies in the cell whose prefix range
+    // [excl, incl) holds it (the last lane with excl <= t, by bisection)
+    uint32_t incl = mine.y;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += v;
+    }
+    uint32_t excl = incl - mine.y;
+    uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
+    for (uint32_t base = 0; base < total; base += 32) {
+      uint32_t t = base + lane;
+      int src = 0;
+#pragma unroll
+      for (int step = 16; step > 0; step >>= 1) {
+        uint32_t e = __shfl_sync(0xffffffffu, excl, src + step);
+        if (e <= t) src += step;
+      }
       uint32_t st = __shfl_sync(0xffffffffu, mine.x, src);
-      uint32_t cn = __shfl_sync(0xffffffffu, mine.y, src);
-      for (uint32_t base = st; base < st + cn; base += 32) {
-        uint32_t s = base + lane;
+      uint32_t s = st + (t - __shfl_sync(0xffffffffu, excl, src));
+      {
         bool inr = false;
         float w = 0.0f, wp = 0.0f;
         uint32_t fid = 0;
-        if (s < st + cn) {
+        if (t < total) {
           float4 pf = __ldg(&pos[s]);
           float dx = bp.x - pf.x, dy = bp.y - pf.y, dz = bp.z - pf.z;
           float d2 = dx * dx + dy * dy + dz * dz;
