@@ -100,6 +100,8 @@ struct SphHandle {
   float4* bpos = nullptr;
   float* bpress = nullptr;
   uint8_t* bact = nullptr;  // per boundary particle: an occupied cell lists it (k_adami_mark)
+  uint32_t* bc_cells = nullptr;  // the linear cells whose boundary candidate list is not empty
+  int nbc_cells = 0;
   uint32_t *bc_start = nullptr, *bc_list = nullptr;
   // SDF node grid and wall table (boundary_mode SPH_BOUNDARY_SDF), or the
   // geometry SDF(s) of the closure features
@@ -564,7 +566,9 @@ void enqueue_adami(SphHandle* h) {
   using namespace sph;
   if (h->nb > 0) {
     cudaMemsetAsync(h->bact, 0, (size_t)h->nb, h->st);
-    k_adami_mark<<<grid_for(h->C, 8), 256, 0, h->st>>>(h->C, h->ctab, h->bc_start, h->bc_list, h->bact);
+    if (h->nbc_cells > 0)
+      k_adami_mark<<<grid_for(h->nbc_cells, 8), 256, 0, h->st>>>(h->nbc_cells, h->bc_cells, h->ctab, h->bc_start,
+                                                                  h->bc_list, h->bact);
     dispatch(h, true, [&](auto kp) {
       k_adami<<<grid_for(h->nb, kAdamiWarps), kAdamiWarps * 32, 0, h->st>>>(
           kp, h->nb, h->bpos, h->bpress, h->pos, h->rf, h->pr, h->id, h->ctab, h->err, h->bact);
@@ -948,6 +952,9 @@ int create_impl(int ninst, const SphParams* PP, const SphParticlesView* pvs,
   h->k = h->ktab_h[0];
   h->C = (int)C;
   h->boundary_candidates = blist.size();
+  std::vector<uint32_t> bcells;  // cells with boundary candidates (static: they bound k_adami_mark)
+  for (uint64_t c = 0; c < C; ++c)
+    if (bstart[c + 1] > bstart[c]) bcells.push_back((uint32_t)c);
   for (int q = 0; q < ninst; ++q) {
     h->init_mass += h->init_m[q];
     h->init_energy += h->init_e[q];
@@ -998,6 +1005,8 @@ int create_impl(int ninst, const SphParams* PP, const SphParticlesView* pvs,
   allocator.join();
   cudaError_t e = ae;
   if (e == cudaSuccess) e = dalloc(h, &h->bc_list, blist.size());
+  if (e == cudaSuccess) e = dalloc(h, &h->bc_cells, bcells.size());
+  h->nbc_cells = (int)bcells.size();
   if (e == cudaSuccess && sdf_mode) e = dalloc(h, &h->wall_tab, wall_host.size());
   if (e != cudaSuccess) return fail(e == cudaErrorMemoryAllocation ? SPH_ERR_OOM : SPH_ERR_CUDA);
 
@@ -1018,6 +1027,7 @@ int create_impl(int ninst, const SphParams* PP, const SphParticlesView* pvs,
   up(h->lin_of_rank, lin_of_rank.data(), C * sizeof(uint32_t));
   up(h->bc_start, bstart.data(), (C + 1) * sizeof(uint32_t));
   up(h->bc_list, blist.data(), blist.size() * sizeof(uint32_t));
+  up(h->bc_cells, bcells.data(), bcells.size() * sizeof(uint32_t));
   up(h->hcc, hcc.data(), ninst * sizeof(float4));
   if (ninst > 1) {
     up(h->ktab, h->ktab_h.data(), ninst * sizeof(SimConst));

@@ -1107,11 +1107,15 @@ constexpr int kAdamiWarps = 4;
 // reach a particle of the cell). A boundary particle with a fluid particle in
 // support is marked; an unmarked one has no terms, and its Adami pressure is
 // the empty sum's 0.
-// One warp per cell, the lanes taking the cell's list entries in turn.
-__global__ void k_adami_mark(int C, const uint2* __restrict__ ctab, const uint32_t* __restrict__ bc_start,
-                             const uint32_t* __restrict__ bc_list, uint8_t* __restrict__ act) {
-  int c = (int)((blockIdx.x * (unsigned)blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
-  if (c >= C || __ldg(&ctab[c]).y == 0u) return;
+// One warp per cell with a non-empty list (`cells`, ncl of them), the lanes
+// taking the cell's list entries in turn.
+__global__ void k_adami_mark(int ncl, const uint32_t* __restrict__ cells, const uint2* __restrict__ ctab,
+                             const uint32_t* __restrict__ bc_start, const uint32_t* __restrict__ bc_list,
+                             uint8_t* __restrict__ act) {
+  int w = (int)((blockIdx.x * (unsigned)blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+  if (w >= ncl) return;
+  uint32_t c = __ldg(&cells[w]);
+  if (__ldg(&ctab[c]).y == 0u) return;
   uint32_t q1 = __ldg(&bc_start[c + 1]);
   for (uint32_t q = __ldg(&bc_start[c]) + lane; q < q1; q += 32) act[__ldg(&bc_list[q])] = 1;
 }
