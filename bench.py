@@ -79,7 +79,21 @@ def pair_stats(sc, sample: int = 20000, seed: int = 0) -> dict:
 
 def roofline_bytes():
     src = open(os.path.join(ROOT, "include", "sph_roofline.h")).read()
-    return {k: int(v) for k, v in re.findall(r"#define (SPH_BYTES_\w+) (\d+)", src)}
+    return {k: int(v) for k, v in re.findall(r"#define (SPH_\w+) (\d+)", src)}
+
+
+KERNEL_SOURCES = ["ultraballpit_b200/csrc/sph_kernels.cuh", "ultraballpit_b200/csrc/sph_api.cu",
+                  "ultraballpit_b200/csrc/sph_mlp.cuh"]
+
+
+def kernel_sources_digest() -> str:
+    """sha1 over the step's kernel sources: an ncu figure recorded with the
+    same digest was captured on this build."""
+    import hashlib
+    h = hashlib.sha1()
+    for f in KERNEL_SOURCES:
+        h.update(open(os.path.join(ROOT, f), "rb").read())
+    return h.hexdigest()
 
 
 def measured_peaks():
@@ -214,6 +228,9 @@ def run_batch_arm(args):
         e1.synchronize()
     ms = e0.elapsed_time(e1)
     launches = b.launch_count() - l0
+    b.synchronize()
+    if b.health() != 0:
+        raise SystemExit("non-finite particle state after the timed steps")
     prof = {}
     for _ in range(3):
         for kk, v in b.step_profiled(float(b.timesteps().min())).items():
@@ -295,7 +312,9 @@ def run_batch_closure_arm(args):
         e1.synchronize()
     ms = e0.elapsed_time(e1)
     launches = b.launch_count() - l0
-    b.health()
+    b.synchronize()
+    if b.health() != 0:
+        raise SystemExit("non-finite particle state after the timed steps")
     b.close()
     del b
     seq_ms = 0.0
@@ -336,22 +355,35 @@ def run_batch_closure_arm(args):
         print(json.dumps(line), flush=True)
 
 
+def plain_config(args, sc, world: int) -> dict:
+    """The config block of a single-simulation workload, shared by both arms
+    so that the two lines name the same workload with the same keys."""
+    n = len(sc.particles)
+    state_bytes = n * 4 * (16 * 6 + 8 * 2 + 4 * 6)
+    return {"workload": args.workload, "particles_per_gpu": n, "boundary_particles": len(sc.boundary),
+            "parallelism": f"replicas{world}", "dt": "device CFL each step",
+            "l2": f"inputs larger than L2 (state {state_bytes / 1e6:.0f} MB per GPU)",
+            "alpha": sc.alpha, "cell_order": "rows", "seed": args.seed}
+
+
 def run_reference_arm(args):
     rank, world, _ = dist_env()
     if rank != 0:
         return
     sc = build_scenario(args.workload, seed=args.seed)
     threads = os.cpu_count() or 1
-    value, done, el = cpu_reference_run(sc, args.steps, min(args.warmup, 1), args.ref_budget, threads)
+    value, done, el = cpu_reference_run(sc, args.steps, args.warmup, args.ref_budget, threads)
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
-        "steps": done, "warmup": min(args.warmup, 1), "ms_per_step": el / done * 1e3,
+        "steps": done, "warmup": args.warmup, "ms_per_step": el / done * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic (seeded dam break)",
-        "config": {"workload": args.workload, "particles": len(sc.particles), "boundary": len(sc.boundary)},
+        "data": "synthetic (seeded dam break, host-built)",
+        "config": plain_config(args, sc, 1),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
-                         "sample": f"{done} full steps of {args.workload} ({len(sc.particles)} particles), "
-                                   f"oracle tier G (reference arithmetic, grid-visited boundary terms)"},
+                         "sample": f"{done} of the {args.steps} requested full steps of {args.workload} "
+                                   f"({len(sc.particles)} particles) within {args.ref_budget:.0f} s, after "
+                                   f"{args.warmup} warm-up steps; oracle tier G (reference arithmetic, "
+                                   f"grid-visited boundary terms)"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -377,7 +409,6 @@ def run_cuda_arm(args):
     k = CudaKernel(*sc.kernel_args(), **kw)
     stream = torch.cuda.ExternalStream(k.stream())
     k.step_auto(args.warmup, want_dt=True)
-    state_bytes = n * 4 * (16 * 6 + 8 * 2 + 4 * 6)
     barrier()
     l0 = k.launch_count()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -387,6 +418,12 @@ def run_cuda_arm(args):
         e1.record(stream)
         e1.synchronize()
     launches = k.launch_count() - l0
+    # every kernel returns at once when the device error word is set, so a
+    # tripped capacity bound or a non-finite state would make the timed steps
+    # fast and meaningless: the run must end clean
+    k.synchronize()
+    if k.health() != 0:
+        raise SystemExit("non-finite particle state after the timed steps")
     barrier()
     value, ms = rep.whole_job_rate(n, args.steps, e0.elapsed_time(e1))
 
@@ -408,26 +445,55 @@ def run_cuda_arm(args):
                 "boundary_pressure_us": rb["SPH_BYTES_PER_BOUNDARY"] * len(sc.boundary),
                 "forces_us": rb["SPH_BYTES_FORCES"] * n}
     peak, peak_kind = measured_peaks()
-    achieved = bytes_of[dom] / (avg[dom] * 1e-6) / 1e9
-    traffic, l2_pct = None, None
+    hbm_achieved = bytes_of[dom] / (avg[dom] * 1e-6) / 1e9
+    ps = pair_stats(sc)
+    cand, inter = ps["candidates_per_particle"], ps["interactions_per_particle"]
+    # FP32 operations per particle of each neighbour kernel (sph_roofline.h)
+    flops_of = {"density_us": cand * rb["SPH_FLOPS_SCAN_PER_CANDIDATE"]
+                + inter * rb["SPH_FLOPS_DENSITY_PER_INTERACTION"],
+                "forces_us": inter * rb["SPH_FLOPS_FORCES_PER_INTERACTION"],
+                "xsph_drift_us": inter * rb["SPH_FLOPS_XSPH_PER_INTERACTION"]}
+    sm_mhz = clk.summary().get("sm_max_mhz") or 1965.0
+    fp32_peak = rb["SPH_FP32_LANES_PER_SM"] * rb["SPH_SM_COUNT"] * sm_mhz * 1e6 / 1e12  # TFLOP/s
+    prof_ncu, traffic, fresh = {}, None, False
     tfile = os.path.join(ROOT, "profiles", "ncu_traffic.json")
     if os.path.exists(tfile):
-        t = json.load(open(tfile)).get(dom.replace("_us", ""))
-        if t and "bytes_per_particle" in t:
-            traffic = t["bytes_per_particle"] * n
-            l2_pct = t.get("l2_pct_of_peak")
-    roofline = {"bound": "hbm", "kernel": dom.replace("_us", ""), "achieved": achieved, "peak": peak,
-                "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
-                "peak_source": peak_kind, "stage_us": {s.replace("_us", ""): round(avg[s], 2) for s in stage_keys},
-                "algorithmic_bytes_per_launch": bytes_of[dom]}
+        tj = json.load(open(tfile))
+        fresh = tj.get("kernel_sources_sha1") == kernel_sources_digest()
+        prof_ncu = tj.get(dom.replace("_us", ""), {})
+        if "bytes_per_particle" in prof_ncu:
+            traffic = prof_ncu["bytes_per_particle"] * n
+    hbm = {"achieved": hbm_achieved, "peak": peak, "unit": "GB/s", "frac": hbm_achieved / peak,
+           "peak_source": peak_kind, "algorithmic_bytes_per_launch": bytes_of[dom]}
     if traffic is not None:
-        # the neighbour kernels are bound by L1 and instruction issue, not HBM:
-        # the DRAM rate of the ncu-measured traffic at this run's launch time,
-        # and the L2 throughput share from the same capture
-        roofline["dram_gbs_of_measured_traffic"] = traffic / (avg[dom] * 1e-6) / 1e9
-        roofline["dram_frac_of_measured_traffic"] = roofline["dram_gbs_of_measured_traffic"] / peak
-        roofline["l2_pct_of_peak_ncu"] = l2_pct
-    ps = pair_stats(sc)
+        # DRAM rate of the ncu-measured traffic at this run's launch time
+        hbm["dram_gbs_of_measured_traffic"] = traffic / (avg[dom] * 1e-6) / 1e9
+        hbm["dram_frac_of_measured_traffic"] = hbm["dram_gbs_of_measured_traffic"] / peak
+    if dom in flops_of:
+        # neighbour kernels: bound by instruction issue (ncu), measured here as
+        # FP32 operations per second against the FP32 peak at this run's clock
+        achieved = n * flops_of[dom] / (avg[dom] * 1e-6) / 1e12
+        roofline = {"bound": "issue", "kernel": dom.replace("_us", ""), "achieved": achieved,
+                    "peak": fp32_peak, "unit": "TFLOP/s", "frac": achieved / fp32_peak,
+                    "peak_source": f"FP32 lanes x SMs x {sm_mhz:.0f} MHz (sph_roofline.h)",
+                    "flops_per_particle": flops_of[dom]}
+    else:
+        roofline = {"bound": "hbm", "kernel": dom.replace("_us", ""), "achieved": hbm_achieved, "peak": peak,
+                    "unit": "GB/s", "frac": hbm_achieved / peak, "peak_source": peak_kind}
+    roofline.update({
+        "traffic": traffic,
+        "traffic_source": ("profiles/ncu_traffic.json, captured on these kernel sources" if fresh else
+                           "profiles/ncu_traffic.json, captured on earlier kernel sources (stale)")
+        if traffic is not None else None,
+        "issue_active_pct_ncu": prof_ncu.get("issue_active_pct"),
+        "threads_active_per_warp_instruction_ncu": prof_ncu.get("threads_per_inst"),
+        "l2_pct_of_peak_ncu": prof_ncu.get("l2_pct_of_peak"),
+        "hbm": hbm,
+        "stage_us": {s.replace("_us", ""): round(avg[s], 2) for s in stage_keys},
+        "kernels": {s.replace("_us", ""): {"tflops": n * f / (avg[s] * 1e-6) / 1e12,
+                                           "fp32_frac": n * f / (avg[s] * 1e-6) / 1e12 / fp32_peak}
+                    for s, f in flops_of.items()},
+    })
     roofline["pairs"] = dict(ps, **{
         "density_candidate_tests_per_s": n * ps["candidates_per_particle"] / (avg["density_us"] * 1e-6),
         "density_interactions_per_s": n * ps["interactions_per_particle"] / (avg["density_us"] * 1e-6),
@@ -495,10 +561,7 @@ def run_cuda_arm(args):
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded dam break, host-built)",
-            "config": {"workload": args.workload, "particles_per_gpu": n, "boundary_particles": len(sc.boundary),
-                       "parallelism": f"replicas{world}", "dt": "device CFL each step",
-                       "l2": f"inputs larger than L2 (state {state_bytes / 1e6:.0f} MB per GPU)",
-                       "alpha": sc.alpha, "cell_order": "rows"},
+            "config": plain_config(args, sc, world),
             "clocks": clk.summary(), "gpu_launches": launches, "e2e": e2e,
             "roofline": roofline, "cpu_baseline": cpu, "domain_setup": setup,
         }
@@ -514,12 +577,12 @@ def main():
     ap.add_argument("--workload", default="dam_break_1mm_sphere", choices=sorted(WORKLOADS))
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--cpu-budget", type=float, default=25.0)
-    ap.add_argument("--ref-budget", type=float, default=120.0)
+    ap.add_argument("--ref-budget", type=float, default=150.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--shard", action="store_true",
                     help="batch workloads: bin-pack one draw of instances across the ranks (strong scaling)")
     args = ap.parse_args()
-    if args.warmup < 3 and args.impl == "cuda":
+    if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
         run_reference_arm(args)

@@ -419,9 +419,12 @@ int sph_neighbors(SphHandle *h, uint32_t id, uint32_t *out, size_t cap, size_t *
  * more than SPH_NOALLOC_MAX_CELLS cells, or a cell holding more than 1024
  * particles, return SPH_ERR_CAPACITY. The first call on a device looks up
  * the array's device address (with that device current); make that first
- * call before any stream capture. All calls share the one array, so calls
- * that overlap on the GPU (different streams or host threads, same device)
- * race and must be serialized by the caller. */
+ * call before any stream capture. `stream` must belong to the current
+ * device; since the call waits on the host for the stream, a stream of
+ * another device or a stream that is capturing is rejected with
+ * SPH_ERR_INVALID_ARG before anything is enqueued. All calls share the one
+ * array, so calls that overlap on the GPU (different streams or host
+ * threads, same device) race and must be serialized by the caller. */
 #define SPH_NOALLOC_MAX_CELLS (1u << 19)
 int sph_grid_sort_noalloc(const float *d_x, const float *d_y, const float *d_z, uint32_t n,
                           const float domain_min[3], const float domain_max[3], float cell_size,

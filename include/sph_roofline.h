@@ -31,4 +31,27 @@
 #define SPH_BYTES_PER_CELL 8
 #define SPH_BYTES_PER_BOUNDARY 20
 
+/*
+ * FP32 operations of the pair work, counted from the kernels' expressions
+ * (every IEEE add, subtract, multiply, compare, divide and square root counts
+ * one; --fmad=false forms no FMA). The neighbour kernels are bound by
+ * instruction issue, not by HBM, so their roofline is this count against
+ * the FP32 peak: 128 lanes per SM x 148 SMs x the SM clock.
+ *
+ *   candidate test of the 27-cell scan: 3 sub, 3 mul, 2 add, 1 compare     9
+ *   density interaction: distance 8, sqrt 1, gradient 17, r.gradW 5,
+ *     density difference 1, delta-SPH term 6, W 10, rho += m W 2           50
+ *   forces interaction: distance 8, sqrt 1, gradient 17, pressure factor 3,
+ *     pressure sum 6, dv 3, v.r 5, compare 1, viscous term 18 (counted
+ *     as always taken: an upper bound)                                     62
+ *   XSPH interaction: distance 8, sqrt 1, W 10, rho avg 2, factor 3,
+ *     velocity sum 9                                                       33
+ */
+#define SPH_FLOPS_SCAN_PER_CANDIDATE 9
+#define SPH_FLOPS_DENSITY_PER_INTERACTION 50
+#define SPH_FLOPS_FORCES_PER_INTERACTION 62
+#define SPH_FLOPS_XSPH_PER_INTERACTION 33
+#define SPH_FP32_LANES_PER_SM 128
+#define SPH_SM_COUNT 148
+
 #endif

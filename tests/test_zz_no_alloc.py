@@ -12,12 +12,13 @@ import ctypes as C
 import numpy as np
 import pytest
 
+from oracle import oracle as orc
 from ultraballpit_b200 import domain
 from ultraballpit_b200.kernel import CELL_ORDER_LINEAR, CudaKernel, load_library
 
 pytestmark = pytest.mark.gpu
 
-SPH_OK, SPH_ERR_CAPACITY = 0, 6
+SPH_OK, SPH_ERR_INVALID_ARG, SPH_ERR_CAPACITY = 0, 1, 6
 MAX_CELLS = 1 << 19
 
 
@@ -35,26 +36,47 @@ def _f3(v):
     return (C.c_float * 3)(*map(float, v))
 
 
-def grid_noalloc(x, y, z, sc):
-    """Run the entry point on device copies of x, y, z; return host arrays."""
+def _ncells(cell, dmin, dmax):
+    dims = [max(int(np.ceil(np.float32(np.float32(dmax[a]) - np.float32(dmin[a])) / np.float32(cell))), 1)
+            for a in range(3)]
+    return dims[0] * dims[1] * dims[2]
+
+
+def _call(x, y, z, dmin, dmax, cell, capacity=None, stream=None):
+    """Run the entry point on device copies of x, y, z: (status, host arrays)."""
     import torch
     dev = torch.device("cuda", 0)
     n = x.shape[0]
-    cell = np.float32(2.0) * np.float32(sc.h)
-    dims = [max(int(np.ceil(np.float32(np.float32(sc.domain_max[a]) - np.float32(sc.domain_min[a])) / cell)), 1)
-            for a in range(3)]
-    ncells = dims[0] * dims[1] * dims[2]
+    ncells = _ncells(cell, dmin, dmax)
     tx, ty, tz = (torch.from_numpy(np.ascontiguousarray(a, np.float32)).to(dev) for a in (x, y, z))
-    idx = torch.empty(n, dtype=torch.int32, device=dev)
+    idx = torch.empty(max(n, 1), dtype=torch.int32, device=dev)
     off = torch.empty(ncells, dtype=torch.int32, device=dev)
     cnt = torch.empty(ncells, dtype=torch.int32, device=dev)
-    srt = torch.empty(n, dtype=torch.int32, device=dev)
-    stream = torch.cuda.current_stream(dev).cuda_stream
-    st = _fn()(tx.data_ptr(), ty.data_ptr(), tz.data_ptr(), n, _f3(sc.domain_min), _f3(sc.domain_max),
-               float(cell), idx.data_ptr(), off.data_ptr(), cnt.data_ptr(), srt.data_ptr(), ncells, stream)
+    srt = torch.empty(max(n, 1), dtype=torch.int32, device=dev)
+    if stream is None:
+        stream = torch.cuda.current_stream(dev).cuda_stream
+    st = _fn()(tx.data_ptr(), ty.data_ptr(), tz.data_ptr(), n, _f3(dmin), _f3(dmax),
+               float(cell), idx.data_ptr(), off.data_ptr(), cnt.data_ptr(), srt.data_ptr(),
+               ncells if capacity is None else capacity, stream)
+    torch.cuda.synchronize(dev)
+    out = {k: t.cpu().numpy().view(np.uint32) for k, t in
+           dict(cell_index=idx[:n], offsets=off, counts=cnt, sorted=srt[:n]).items()}
+    return st, out
+
+
+def grid_noalloc(x, y, z, sc):
+    cell = np.float32(2.0) * np.float32(sc.h)
+    st, out = _call(x, y, z, sc.domain_min, sc.domain_max, cell)
     assert st == SPH_OK, st
-    return {k: t.cpu().numpy().view(np.uint32) for k, t in
-            dict(cell_index=idx, offsets=off, counts=cnt, sorted=srt).items()}
+    return out
+
+
+def _assert_oracle_equal(a, x, y, z, cell, dmin, dmax):
+    o = orc.grid_build(x, y, z, float(cell), dmin, dmax)
+    np.testing.assert_array_equal(a["cell_index"], o["cell_idx"])
+    np.testing.assert_array_equal(a["counts"], o["counts"])
+    np.testing.assert_array_equal(a["offsets"], o["offsets"])
+    np.testing.assert_array_equal(a["sorted"], o["sorted"])
 
 
 def _assert_grid_equal(a, g):
@@ -73,6 +95,8 @@ def test_noalloc_grid_matches_handle_grid_on_two_calls():
     q = k1.particles()  # positions of the last force computation's grid
     first = grid_noalloc(q.x, q.y, q.z, sc1)
     _assert_grid_equal(first, k1.read_grid())
+    _assert_oracle_equal(first, q.x, q.y, q.z, np.float32(2.0) * np.float32(sc1.h), sc1.domain_min,
+                         sc1.domain_max)
 
     sc2 = domain.dam_break(0.002, seed=78, block=(0.06, 0.05, 0.04), domain_max=(0.12, 0.1, 0.08),
                            with_sdf=False)
@@ -80,6 +104,8 @@ def test_noalloc_grid_matches_handle_grid_on_two_calls():
     p = sc2.particles
     second = grid_noalloc(p.x, p.y, p.z, sc2)
     _assert_grid_equal(second, k2.read_grid())
+    _assert_oracle_equal(second, p.x, p.y, p.z, np.float32(2.0) * np.float32(sc2.h), sc2.domain_min,
+                         sc2.domain_max)
     assert first["sorted"].shape != second["sorted"].shape
     assert first["counts"].shape != second["counts"].shape
 
@@ -90,3 +116,62 @@ def test_noalloc_rejects_grids_beyond_its_scratch():
     st = f(None, None, None, 0, _f3((0, 0, 0)), _f3((1, 1, 1)), 0.001, None,
            C.c_void_p(1), C.c_void_p(1), None, 10**9, None)
     assert st == SPH_ERR_CAPACITY
+
+
+def test_noalloc_adversarial_points_match_the_oracle():
+    """Points on cell faces, on the domain faces, outside the domain on every
+    side (clamped into the edge cells, neighbor.rs:57-71) and a crowded cell."""
+    rng = np.random.default_rng(5)
+    dmin, dmax, cell = (0.0, 0.0, 0.0), (0.1, 0.06, 0.05), np.float32(0.0104)
+    faces = [np.arange(0, 11, dtype=np.float32) * cell for _ in range(3)]
+    pts = [rng.uniform(-0.02, 0.12, 400), rng.uniform(-0.02, 0.08, 400), rng.uniform(-0.02, 0.07, 400)]
+    for a in range(3):  # exact multiples of the cell size along one axis
+        pts[a][:120] = rng.choice(faces[a], 120)
+    pts = [np.concatenate([p, np.full(300, v, np.float32)]) for p, v in zip(pts, (0.0311, 0.0205, 0.0102))]
+    x, y, z = (np.asarray(p, np.float32) for p in pts)
+    st, out = _call(x, y, z, dmin, dmax, cell)
+    assert st == SPH_OK, st
+    _assert_oracle_equal(out, x, y, z, cell, dmin, dmax)
+    assert out["counts"].max() >= 300
+
+
+def test_noalloc_reports_a_cell_beyond_its_sort_capacity():
+    """1025 particles at one point: more than one cell's sort buffer holds."""
+    x = np.full(1025, 0.013, np.float32)
+    st, _ = _call(x, x.copy(), x.copy(), (0, 0, 0), (0.05, 0.05, 0.05), np.float32(0.01))
+    assert st == SPH_ERR_CAPACITY
+    # the next call on the same scratch starts clean
+    x = np.full(1024, 0.013, np.float32)
+    st, out = _call(x, x.copy(), x.copy(), (0, 0, 0), (0.05, 0.05, 0.05), np.float32(0.01))
+    assert st == SPH_OK
+    np.testing.assert_array_equal(out["sorted"], np.arange(1024, dtype=np.uint32))
+
+
+def test_noalloc_rejects_output_arrays_smaller_than_the_grid():
+    x = np.linspace(0.0, 0.05, 64, dtype=np.float32)
+    nc = _ncells(np.float32(0.01), (0, 0, 0), (0.05, 0.05, 0.05))
+    st, _ = _call(x, x.copy(), x.copy(), (0, 0, 0), (0.05, 0.05, 0.05), np.float32(0.01), capacity=nc - 1)
+    assert st == SPH_ERR_INVALID_ARG
+
+
+def test_noalloc_rejects_a_capturing_stream():
+    """The call waits on the stream, so a stream in capture is refused
+    before anything is enqueued and the capture stays valid."""
+    import torch
+    x = np.linspace(0.0, 0.05, 64, dtype=np.float32)
+    st, _ = _call(x, x.copy(), x.copy(), (0, 0, 0), (0.05, 0.05, 0.05), np.float32(0.01))
+    assert st == SPH_OK  # the device's set-up is done outside the capture
+    t = torch.zeros(4, device="cuda")
+    g = torch.cuda.CUDAGraph()
+    s = torch.cuda.Stream()
+    sts = []
+    with torch.cuda.graph(g, stream=s):
+        t.add_(1.0)
+        # arrays made before the capture would be needed for a real call; the
+        # refusal happens before any pointer is used
+        sts.append(_fn()(None, None, None, 0, _f3((0, 0, 0)), _f3((0.05, 0.05, 0.05)), 0.01, None,
+                         C.c_void_p(1), C.c_void_p(1), None, 125, s.cuda_stream))
+    g.replay()
+    torch.cuda.synchronize()
+    assert sts == [SPH_ERR_INVALID_ARG]
+    assert float(t[0]) == 1.0

@@ -41,10 +41,12 @@ std::mutex g_mu;
 uint32_t* g_scratch_ptr[64] = {};  // device address of g_grid_scratch, per device
 
 // Once per device, with that device current: the host-side name of the
-// array is not a device address, so look the address up.
-int scratch_for_current_device(uint32_t** out) {
+// array is not a device address, so look the address up. *dev_out gets the
+// current device.
+int scratch_for_current_device(uint32_t** out, int* dev_out) {
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return SPH_ERR_NO_DEVICE;
+  *dev_out = dev;
   std::lock_guard<std::mutex> lock(g_mu);
   if (!g_scratch_ptr[dev]) {
     void* p = nullptr;
@@ -235,9 +237,27 @@ extern "C" int sph_grid_sort_noalloc(const float* d_x, const float* d_y, const f
   if (ncells > cells_capacity) return SPH_ERR_INVALID_ARG;
   uint32_t C = (uint32_t)ncells;
   uint32_t* scratch = nullptr;
-  int s = scratch_for_current_device(&scratch);
+  int dev = 0;
+  int s = scratch_for_current_device(&scratch, &dev);
   if (s != SPH_OK) return s;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
+  // The scratch address belongs to the current device, and the call ends
+  // with a host wait on the stream: a stream of another device, or one that
+  // is capturing, is rejected before anything is enqueued.
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(st, &cap) != cudaSuccess) {
+    cudaGetLastError();
+    return SPH_ERR_INVALID_ARG;
+  }
+  if (cap != cudaStreamCaptureStatusNone) return SPH_ERR_INVALID_ARG;
+  if (st) {
+    int sdev = -1;
+    if (cudaStreamGetDevice(st, &sdev) != cudaSuccess) {
+      cudaGetLastError();
+      return SPH_ERR_INVALID_ARG;
+    }
+    if (sdev != dev) return SPH_ERR_INVALID_ARG;
+  }
   uint32_t ntiles = (C + kTile - 1) / kTile;
   k_na_clear<<<blocks(C, 256), 256, 0, st>>>(d_cell_counts, C, scratch);
   if (n > 0) k_na_count<<<blocks(n, 256), 256, 0, st>>>(d_x, d_y, d_z, n, g, d_cell_index, d_cell_counts);
@@ -249,6 +269,9 @@ extern "C" int sph_grid_sort_noalloc(const float* d_x, const float* d_y, const f
     k_na_sort_cells<<<blocks(C, kSortWarps), kSortWarps * 32, 0, st>>>(d_cell_offsets, d_cell_counts, C,
                                                                         d_sorted, scratch);
   }
+  // a launch that failed leaves its outputs unwritten: report it here rather
+  // than leave the error pending for the caller's next call
+  if (cudaGetLastError() != cudaSuccess) return SPH_ERR_CUDA;
   uint32_t err = 0;
   cudaError_t e = cudaMemcpyAsync(&err, scratch + kErrOff, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
