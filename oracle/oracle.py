@@ -41,7 +41,7 @@ class OrcParams(C.Structure):
                 ("alpha", C.c_float), ("beta", C.c_float), ("tier", C.c_int),
                 ("threads", C.c_int), ("pow_mode", C.c_int), ("boundary_mode", C.c_int),
                 ("sdf_wall_coef", C.c_float), ("sdf_origin", C.c_float * 3), ("sdf_cell", C.c_float),
-                ("sdf_dims", C.c_uint32 * 3), ("sdf", C.POINTER(C.c_float))]
+                ("sdf_dims", C.c_uint32 * 3), ("sdf", C.POINTER(C.c_float)), ("flags", C.c_uint32)]
 
 
 def lib():
@@ -226,7 +226,8 @@ class OracleKernel:
     def __init__(self, particles: ParticleArrays, boundary: BoundaryParticles, h, gravity,
                  speed_of_sound, cfl_number, viscosity, domain_min, domain_max, *,
                  alpha: float = 1.0, beta: float = 2.0, tier: int = 1, threads: int = 1,
-                 pow_mode: int = 0, boundary_mode: int = 0, sdf=None, sdf_wall_coef: float = 0.981):
+                 pow_mode: int = 0, boundary_mode: int = 0, sdf=None, sdf_wall_coef: float = 0.981,
+                 flags: int = 0xF):
         particles.validate()
         self._n = len(particles)
         self._nb = len(boundary)
@@ -234,7 +235,7 @@ class OracleKernel:
                         cfl_number=cfl_number, viscosity=viscosity, domain_min=_f3(domain_min),
                         domain_max=_f3(domain_max), alpha=alpha, beta=beta, tier=tier,
                         threads=threads, pow_mode=pow_mode, boundary_mode=boundary_mode,
-                        sdf_wall_coef=sdf_wall_coef)
+                        sdf_wall_coef=sdf_wall_coef, flags=flags)
         if boundary_mode == 1 and sdf is not None:  # the obstacle; the box faces are walls anyway
             self._sdf = np.ascontiguousarray(sdf.distances, np.float32)
             prm.sdf_origin = _f3(sdf.origin)

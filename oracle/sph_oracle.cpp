@@ -266,7 +266,11 @@ struct OrcParams {
   float sdf_cell;
   uint32_t sdf_dims[3];
   const float* sdf;       // node grid, i*ny*nz + j*nz + k (copied at creation)
+  // stage switches, as SphFlags of the C ABI: 1 delta-SPH, 2 XSPH,
+  // 4 repulsion, 8 domain clamp (0xF = every reference stage)
+  uint32_t flags;
 };
+constexpr uint32_t kOrcDelta = 1, kOrcXsph = 2, kOrcRepulsion = 4, kOrcClamp = 8;
 
 // ---- Tier S: SDF wall (no reference counterpart; project definition) ----
 // The SDF wall stands in for the reference's 3 layers of wall particles
@@ -835,9 +839,13 @@ class Kernel {
     size_t n = p.len();
     vx_used = p.vx; vy_used = p.vy; vz_used = p.vz;
     grid.update(p.x.data(), p.y.data(), p.z.data(), n);
-    std::vector<float> diffusion = density_diffusion();
-    compute_density();
-    for (size_t i = 0; i < n; ++i) p.density[i] += diffusion[i] * dt;
+    if (prm.flags & kOrcDelta) {
+      std::vector<float> diffusion = density_diffusion();
+      compute_density();
+      for (size_t i = 0; i < n; ++i) p.density[i] += diffusion[i] * dt;
+    } else {
+      compute_density();
+    }
     compute_pressure();
     if (!sdf_mode()) update_boundary_pressures();
     for (size_t i = 0; i < n; ++i) { p.ax[i] = 0.0f; p.ay[i] = 0.0f; p.az[i] = 0.0f; }
@@ -849,7 +857,7 @@ class Kernel {
       p.az[i] += prm.gravity[2];
     }
     if (sdf_mode()) compute_sdf_wall_forces();
-    else compute_repulsive_forces();
+    else if (prm.flags & kOrcRepulsion) compute_repulsive_forces();
   }
 
   // Tier S wall force, after gravity: the energy-consistent counterpart of the
@@ -882,7 +890,7 @@ class Kernel {
         wa[2] += base * wall_lookup3(wall.grad3, wall.inv3, bf.d[2], bf.d[0], bf.d[1]) * bf.s[2];
       }
       for (int a = 0; a < 3; ++a)
-        if (bf.d[a] < r0) {
+        if ((prm.flags & kOrcRepulsion) && bf.d[a] < r0) {
           float s = 1.0f - fmaxf(bf.d[a], 0.0f) / r0;
           float fm = prm.sdf_wall_coef * s * s / r0;
           wa[a] += fm * bf.s[a];
@@ -899,7 +907,7 @@ class Kernel {
       p.ax[i] += coef * n[0];
       p.ay[i] += coef * n[1];
       p.az[i] += coef * n[2];
-      if (d < r0) {
+      if ((prm.flags & kOrcRepulsion) && d < r0) {
         float s = 1.0f - fmaxf(d, 0.0f) / r0;
         float fm = prm.sdf_wall_coef * s * s / r0;
         p.ax[i] += fm * n[0];
@@ -961,13 +969,17 @@ class Kernel {
       p.vz[i] += p.az[i] * half_dt;
     }
     std::vector<float> dvx, dvy, dvz;
-    xsph(dvx, dvy, dvz);
+    if (prm.flags & kOrcXsph) {
+      xsph(dvx, dvy, dvz);
+    } else {  // the drift adds a zero correction, as the CUDA step does
+      dvx.assign(n, 0.0f); dvy.assign(n, 0.0f); dvz.assign(n, 0.0f);
+    }
     for (size_t i = 0; i < n; ++i) {
       p.x[i] += (p.vx[i] + dvx[i]) * dt;
       p.y[i] += (p.vy[i] + dvy[i]) * dt;
       p.z[i] += (p.vz[i] + dvz[i]) * dt;
     }
-    enforce_no_penetration_domain();
+    if (prm.flags & kOrcClamp) enforce_no_penetration_domain();
     compute_forces(dt);
     for (size_t i = 0; i < n; ++i) {
       p.vx[i] += p.ax[i] * half_dt;
