@@ -172,3 +172,21 @@ def test_trained_closure_gain_over_the_plain_method():
     r = closure.compare(200, net.params(), steps=800, dt=DT)
     assert r["plain"]["all"] < 0.05 and r["closure"]["all"] < 0.05, r
     assert r["closure"]["all"] <= r["plain"]["all"] + 0.01, r
+
+
+def test_shipped_closure_lowers_the_near_wall_pressure_error_of_tanks_at_rest():
+    """The shipped network (trained on 64 tank pairs)
+    against the plain 4 mm method on two tanks at rest that training never
+    saw, both judged by the 2 mm run: the closure's mean near-wall pressure
+    error is below the plain method's. (In tanks set moving, the coarse
+    error is the sloshing phase, which near-wall features cannot predict;
+    there the closure gains nothing.)"""
+    import os
+    w = np.load(os.path.join(os.path.dirname(closure.__file__), "data", "closure_weights.npy")).astype(np.float32)
+    plain, corr = [], []
+    for seed in (1064, 1065):
+        r = closure.compare(seed, w, steps=800, dt=DT)
+        plain.append(r["plain"]["all"])
+        corr.append(r["closure"]["all"])
+    assert np.mean(corr) < np.mean(plain), (plain, corr)
+    assert max(corr) < 0.05

@@ -537,27 +537,28 @@ void enqueue_scan_fill(SphHandle* h) {
 void enqueue_density_only(SphHandle* h) {
   using namespace sph;
   int bs = h->bs_density;
-  sph::ClosureBufs cb{h->cl_count, h->cl_slot, h->cl_feat, h->cl_rho, h->corr, h->vel};
+  sph::ClosureBufs cb{h->cl_count, h->cl_slot, h->cl_feat, h->cl_rho, h->corr, h->vel, h->cl_wb, h->cl_wf};
   if (h->cl_mode) cudaMemsetAsync(h->cl_count, 0, sizeof(uint32_t), h->st);
+  const size_t smem = bs * kNbrChunk * sizeof(uint32_t);
+  // closure mode 2 adds a 16-sample network tile per warp (the fused inference)
+  const size_t smem_cl = smem + (bs / 32) * kClTileWords * sizeof(uint32_t);
   dispatch(h, false, [&](auto kp) {
     using KPT = decltype(kp);
-    if (h->cl_mode)
-      k_density<KPT, 1><<<grid_for(h->n, bs), bs, bs * kNbrChunk * sizeof(uint32_t), h->st>>>(kp, h->n, h->dt, h->pos, h->rv, h->id, h->ctab,
-                                                            h->bc_start, h->bc_list, h->bpos, h->rf, h->pr,
-                                                            h->err, h->nbr, h->ncount, h->sdf, h->wall_tab, cb);
+    if (h->cl_mode == 2)
+      k_density<KPT, 2><<<grid_for(h->n, bs), bs, smem_cl, h->st>>>(kp, h->n, h->dt, h->pos, h->rv, h->id, h->ctab,
+                                                                   h->bc_start, h->bc_list, h->bpos, h->rf, h->pr,
+                                                                   h->err, h->nbr, h->ncount, h->sdf, h->wall_tab,
+                                                                   cb);
+    else if (h->cl_mode)
+      k_density<KPT, 1><<<grid_for(h->n, bs), bs, smem, h->st>>>(kp, h->n, h->dt, h->pos, h->rv, h->id, h->ctab,
+                                                                h->bc_start, h->bc_list, h->bpos, h->rf, h->pr,
+                                                                h->err, h->nbr, h->ncount, h->sdf, h->wall_tab, cb);
     else
-      k_density<KPT, 0><<<grid_for(h->n, bs), bs, bs * kNbrChunk * sizeof(uint32_t), h->st>>>(kp, h->n, h->dt, h->pos, h->rv, h->id, h->ctab,
-                                                            h->bc_start, h->bc_list, h->bpos, h->rf, h->pr,
-                                                            h->err, h->nbr, h->ncount, h->sdf, h->wall_tab, cb);
+      k_density<KPT, 0><<<grid_for(h->n, bs), bs, smem, h->st>>>(kp, h->n, h->dt, h->pos, h->rv, h->id, h->ctab,
+                                                                h->bc_start, h->bc_list, h->bpos, h->rf, h->pr,
+                                                                h->err, h->nbr, h->ncount, h->sdf, h->wall_tab, cb);
   });
   h->launches += 1;
-  if (h->cl_mode == 2) {
-    dispatch(h, false, [&](auto kp) {
-      k_closure_apply<<<std::max(1, std::min(grid_for(h->n, 16 * kClWarps), 148 * 8)), kClWarps * 32, 0, h->st>>>(
-          kp, h->cl_wb, h->cl_wf, h->cl_count, h->cl_slot, h->cl_feat, h->cl_rho, h->id, h->rf, h->pr, h->corr);
-    });
-    h->launches += 1;
-  }
 }
 
 // boundary.rs:87-123: the Adami boundary pressure, for the boundary particles

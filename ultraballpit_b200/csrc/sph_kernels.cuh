@@ -850,10 +850,46 @@ struct ClosureBufs {
   float* rho;
   float4* corr;
   const float4* vel;
+  const __nv_bfloat16* wb;  // closure network (mode 2): BF16 weights
+  const float* wf;          // and FP32 master parameters (biases)
 };
 
+// The learned correction of one particle from the network output y[4]:
+// density += y0 rho0 1e-4 (EOS re-evaluated), acceleration correction
+// y1..3 |g| stored for k_forces. The outputs are clamped to
+// SPH_CLOSURE_MAX_DRHO units (0.3 % of rho0) and SPH_CLOSURE_MAX_ACC_G times
+// |g| per component, so a network queried outside its training data cannot
+// inject an arbitrarily large correction.
+constexpr float kClosureMaxDrho = SPH_CLOSURE_MAX_DRHO;
+constexpr float kClosureDrhoUnit = SPH_CLOSURE_DRHO_UNIT;
+constexpr float kClosureMaxAcc = SPH_CLOSURE_MAX_ACC_G;
+__device__ __forceinline__ void closure_apply_one(const SimConst& k, int i, bool air, float rho_pre, const float* y,
+                                                  float2* __restrict__ rf, float* __restrict__ pr,
+                                                  float4* __restrict__ corr) {
+  float rest = air ? kAirRho0 : kWaterRho0;
+  float gm = sqrtf(k.grav[0] * k.grav[0] + k.grav[1] * k.grav[1] + k.grav[2] * k.grav[2]);
+  float y0 = fminf(fmaxf(y[0], -kClosureMaxDrho), kClosureMaxDrho);
+  float rho = rho_pre + y0 * (rest * kClosureDrhoUnit);
+  float p = tait(rho, air, k);
+  rf[i] = make_float2(rho, p / (rho * rho));
+  pr[i] = p;
+  float c1 = fminf(fmaxf(y[1], -kClosureMaxAcc), kClosureMaxAcc);
+  float c2 = fminf(fmaxf(y[2], -kClosureMaxAcc), kClosureMaxAcc);
+  float c3 = fminf(fmaxf(y[3], -kClosureMaxAcc), kClosureMaxAcc);
+  corr[i] = make_float4(c1 * gm, c2 * gm, c3 * gm, 1.0f);
+}
+
+// CL = 0: plain step. CL = 1: the particles within 2h of the feature SDF
+// record their 16 closure features (capture mode). CL = 2: they also run the
+// network in the kernel's epilogue: each warp gathers its near-wall
+// particles' features into 16-sample tiles in shared memory and evaluates
+// the 16 -> 64 -> 64 -> 4 MLP on the tensor cores (register-resident
+// activations), so the corrected density and its EOS are written before the
+// kernel ends and no separate inference launch is needed. CL = 2 lifts the
+// register cap for the network's fragments.
+constexpr int kClTileWords = 16 * 16 / 2 + 16 * 4;  // BF16 x tile + FP32 y tile, in 32-bit words
 template <class KP, int CL>
-__global__ void __maxnreg__(48)
+__global__ void __maxnreg__(CL == 2 ? 96 : 48)
 k_density(KP kp, int n, const float* __restrict__ dtp, const float4* __restrict__ pos,
           const float2* __restrict__ rv, const uint32_t* __restrict__ id,
           const uint2* __restrict__ ctab, const uint32_t* __restrict__ bc_start,
@@ -862,7 +898,13 @@ k_density(KP kp, int n, const float* __restrict__ dtp, const float4* __restrict_
           uint32_t* __restrict__ nbr, uint32_t* __restrict__ ncount, const float* __restrict__ sdf,
           const float2* __restrict__ wall_tab, ClosureBufs cb) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n || *err) return;
+  const bool live = i < n && !*err;
+  // the fused network is a warp-wide epilogue: every lane reaches it
+  bool near_wall = false;
+  float f[16];
+  float rho_pre = 0.0f;
+  if (CL != 2 && !live) return;
+  if (live) {
   const SimConst& k = kp.at(i);
   float dt = dtp[k.inst];
   float ssum = 0.0f, rho_wall = 0.0f;  // closure: kernel sum, wall density
@@ -1007,7 +1049,6 @@ k_density(KP kp, int n, const float* __restrict__ dtp, const float4* __restrict_
       float lap = fsdf(pi.x + k.h, pi.y, pi.z) + fsdf(pi.x - k.h, pi.y, pi.z) + fsdf(pi.x, pi.y + k.h, pi.z) +
                   fsdf(pi.x, pi.y - k.h, pi.z) + fsdf(pi.x, pi.y, pi.z + k.h) + fsdf(pi.x, pi.y, pi.z - k.h) -
                   6.0f * d;
-      float f[16];
       f[0] = d / k.h;
       f[1] = nx; f[2] = ny; f[3] = nz;
       f[4] = 1.0f - (rv[i].y * k.norm_h3 + ssum);
@@ -1027,73 +1068,42 @@ k_density(KP kp, int n, const float* __restrict__ dtp, const float4* __restrict_
       cb.rho[q] = rho;
 #pragma unroll
       for (int a = 0; a < 16; ++a) cb.feat[(size_t)q * 16 + a] = f[a];
+      near_wall = true;
+      rho_pre = rho;
     }
   }
-}
-
-// Closure inference on the tensor cores for the particles the density pass
-// listed: y = MLP(features); density += y0 rho0 1e-4 (EOS re-evaluated),
-// acceleration correction y1..3 |g| stored for k_forces. The outputs are
-// clamped to SPH_CLOSURE_MAX_DRHO units (0.3 % of rho0) and
-// SPH_CLOSURE_MAX_ACC_G times |g| per component, so a network queried outside
-// its training data cannot inject an arbitrarily large correction.
-constexpr int kClWarps = 2;
-constexpr float kClosureMaxDrho = SPH_CLOSURE_MAX_DRHO;
-constexpr float kClosureDrhoUnit = SPH_CLOSURE_DRHO_UNIT;
-constexpr float kClosureMaxAcc = SPH_CLOSURE_MAX_ACC_G;
-struct ClSmem {
-  __nv_bfloat16 w1[64 * 16];
-  __nv_bfloat16 w2[64 * 64];
-  __nv_bfloat16 w3[16 * 64];
-  float b[sphmlp::kParamBias];
-  struct Tile {
-    __nv_bfloat16 x[16 * 16];
-    float z1[16 * 64];
-    __nv_bfloat16 h1[16 * 64];
-    float z2[16 * 64];
-    __nv_bfloat16 h2[16 * 64];
-    float y[16 * 4];
-  } t[kClWarps];
-};
-
-template <class KP>
-__global__ void __launch_bounds__(kClWarps * 32)
-k_closure_apply(KP kp, const __nv_bfloat16* __restrict__ wb, const float* __restrict__ wf,
-                const uint32_t* __restrict__ count, const uint32_t* __restrict__ slot,
-                const float* __restrict__ feat, const float* __restrict__ rho_pre,
-                const uint32_t* __restrict__ id, float2* __restrict__ rf, float* __restrict__ pr,
-                float4* __restrict__ corr) {
-  __shared__ ClSmem S;
-  int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  sphmlp::load_weights_smem(wb, wf, S.w1, S.w2, S.w3, S.b);
-  __syncthreads();
-  const uint32_t cnt = *count;
-  auto& T = S.t[warp];
-  for (uint32_t base = (blockIdx.x * kClWarps + warp) * 16; base < cnt; base += gridDim.x * kClWarps * 16) {
-    for (int q = lane; q < 256; q += 32) {
-      uint32_t r = base + (q >> 4);
-      T.x[q] = __float2bfloat16_rn(r < cnt ? feat[(size_t)r * 16 + (q & 15)] : 0.0f);
+  }  // live
+  if (CL == 2) {
+    // network epilogue: up to 16 of the warp's near-wall particles per tile
+    extern __shared__ uint32_t s_stage[];
+    const int lane = threadIdx.x & 31;
+    uint32_t* tile = s_stage + kNbrChunk * blockDim.x + (threadIdx.x >> 5) * kClTileWords;
+    __nv_bfloat16* xt = reinterpret_cast<__nv_bfloat16*>(tile);
+    float* yt = reinterpret_cast<float*>(tile + 16 * 16 / 2);
+    unsigned pending = __ballot_sync(0xffffffffu, near_wall);
+    while (pending) {
+      unsigned rest = pending;  // the lowest 16 pending lanes form this tile
+      for (int q = 0; q < 16 && rest; ++q) rest &= rest - 1u;
+      unsigned take = pending & ~rest;
+      pending = rest;
+      const bool mine = (take >> lane) & 1u;
+      const int row = __popc(take & ((1u << lane) - 1u));
+      const int cnt = __popc(take);
+      if (mine) {
+#pragma unroll
+        for (int a = 0; a < 16; ++a) xt[row * 16 + a] = __float2bfloat16_rn(f[a]);
+      }
+      for (int q = lane; q < 256; q += 32)
+        if ((q >> 4) >= cnt) xt[q] = __float2bfloat16_rn(0.0f);
+      __syncwarp();
+      sphmlp::forward_tile_regs(xt, cb.wb, cb.wf, yt, lane);
+      __syncwarp();
+      if (mine) {
+        const SimConst& k = kp.at(i);
+        closure_apply_one(k, i, (id[i] & kAirBit) != 0, rho_pre, yt + row * 4, rf, pr, cb.corr);
+      }
+      __syncwarp();
     }
-    __syncwarp();
-    sphmlp::forward_tile(T.x, S.w1, S.w2, S.w3, S.b, T.z1, T.h1, T.z2, T.h2, T.y, lane);
-    if (lane < 16 && base + lane < cnt) {
-      uint32_t q = base + lane;
-      int i = (int)slot[q];
-      const SimConst& k = kp.at(i);
-      bool air = (id[i] & kAirBit) != 0;
-      float rest = air ? kAirRho0 : kWaterRho0;
-      float gm = sqrtf(k.grav[0] * k.grav[0] + k.grav[1] * k.grav[1] + k.grav[2] * k.grav[2]);
-      float y0 = fminf(fmaxf(T.y[lane * 4], -kClosureMaxDrho), kClosureMaxDrho);
-      float rho = rho_pre[q] + y0 * (rest * kClosureDrhoUnit);
-      float p = tait(rho, air, k);
-      rf[i] = make_float2(rho, p / (rho * rho));
-      pr[i] = p;
-      float c1 = fminf(fmaxf(T.y[lane * 4 + 1], -kClosureMaxAcc), kClosureMaxAcc);
-      float c2 = fminf(fmaxf(T.y[lane * 4 + 2], -kClosureMaxAcc), kClosureMaxAcc);
-      float c3 = fminf(fmaxf(T.y[lane * 4 + 3], -kClosureMaxAcc), kClosureMaxAcc);
-      corr[i] = make_float4(c1 * gm, c2 * gm, c3 * gm, 1.0f);
-    }
-    __syncwarp();
   }
 }
 
@@ -1495,7 +1505,7 @@ k_forces(KP kp, int n, const float* __restrict__ dtp, float hdt_scale,
       }
       if (q < b1) rterm(__ldg(&bpos[__ldg(&bc_list[q])]));
     }
-    if (CL) {  // learned near-wall correction (k_closure_apply)
+    if (CL) {  // learned near-wall correction (the density kernel's network epilogue)
       float4 cr = corr[i];
       if (cr.w != 0.0f) { ax += cr.x; ay += cr.y; az += cr.z; }
     }

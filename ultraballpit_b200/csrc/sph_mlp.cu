@@ -30,6 +30,7 @@ struct SphMlp {
   int part_rows = 0;
   float* loss = nullptr;     // per-CTA loss partials
   int64_t step = 0;
+  int sms = 148;             // SMs of the device (queried at creation)
   std::vector<void*> allocs;
 };
 
@@ -225,6 +226,8 @@ int sph_mlp_create(int device, uint64_t seed, SphMlp** out) {
   SphMlp* h = new SphMlp();
   h->dev = device;
   cudaSetDevice(device);
+  int sms = 0;
+  if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) == cudaSuccess && sms > 0) h->sms = sms;
   cudaError_t e = cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = mal(h, &h->w, kParams);
   if (e == cudaSuccess) e = mal(h, &h->m, kParams);
@@ -302,7 +305,7 @@ int sph_mlp_forward(SphMlp* h, const float* x, size_t n, float* y) {
   int s = upload(h, x, n * kIn, &dx);
   cudaError_t e = s == SPH_OK ? cudaMalloc((void**)&dy, n * kOut * sizeof(float)) : cudaErrorUnknown;
   if (e == cudaSuccess) {
-    int blocks = (int)std::min<size_t>((n + kCtaSamples - 1) / kCtaSamples, 148 * 4);
+    int blocks = (int)std::min<size_t>((n + kCtaSamples - 1) / kCtaSamples, (size_t)h->sms * 4);
     k_mlp_forward<<<blocks, kWarps * 32, sizeof(CtaSmem), h->st>>>(h->wb, h->w, dx, (int)n, dy);
     e = cudaMemcpyAsync(y, dy, n * kOut * sizeof(float), cudaMemcpyDeviceToHost, h->st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(h->st);

@@ -112,6 +112,85 @@ __device__ __forceinline__ void forward_tile(const __nv_bfloat16* x, const __nv_
   __syncwarp();
 }
 
+// One m16n8k16 step with the operands already in registers.
+__device__ __forceinline__ void mma_regs(float c[4], uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3,
+                                         uint32_t b0, uint32_t b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};\n"
+      : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+      : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+}
+
+__device__ __forceinline__ uint32_t ldg_pair(const __nv_bfloat16* p) {
+  return __ldg(reinterpret_cast<const unsigned int*>(p));
+}
+
+// The forward pass of forward_tile with the activations kept in registers:
+// the C fragment of two adjacent n-tiles of one layer is the A fragment of
+// one k-tile of the next (rows g, g+8; columns 2t, 2t+1 and 2t+8, 2t+9), so
+// only the input tile x[16][16] (BF16, shared) and the output y[16][4]
+// (FP32, shared) leave the registers. The weights are read from global
+// memory (wb: BF16 W1 | W2 | W3; the master FP32 parameters wf for the
+// biases) and stay in L1. Same instructions, operands and rounding points as
+// forward_tile, so the outputs are identical.
+__device__ __forceinline__ void forward_tile_regs(const __nv_bfloat16* x, const __nv_bfloat16* __restrict__ wb,
+                                                  const float* __restrict__ wf, float* y, int lane) {
+  int g = lane >> 2, t = lane & 3;
+  int k0 = 2 * t;
+  uint32_t xa0 = pack2(x[g * 16 + k0], x[g * 16 + k0 + 1]);
+  uint32_t xa1 = pack2(x[(g + 8) * 16 + k0], x[(g + 8) * 16 + k0 + 1]);
+  uint32_t xa2 = pack2(x[g * 16 + k0 + 8], x[g * 16 + k0 + 9]);
+  uint32_t xa3 = pack2(x[(g + 8) * 16 + k0 + 8], x[(g + 8) * 16 + k0 + 9]);
+  const __nv_bfloat16* w1 = wb;
+  const __nv_bfloat16* w2 = wb + 1024;
+  const __nv_bfloat16* w3 = wb + 5120;
+  uint32_t h1[16];
+#pragma unroll
+  for (int nt = 0; nt < 8; ++nt) {
+    float c[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+    const __nv_bfloat16* wr = w1 + (nt * 8 + g) * 16 + k0;
+    mma_regs(c, xa0, xa1, xa2, xa3, ldg_pair(wr), ldg_pair(wr + 8));
+    float bl = __ldg(&wf[kOffB1 + nt * 8 + k0]), bh = __ldg(&wf[kOffB1 + nt * 8 + k0 + 1]);
+    h1[(nt >> 1) * 4 + (nt & 1) * 2] = pack2(__float2bfloat16_rn(silu(c[0] + bl)), __float2bfloat16_rn(silu(c[1] + bh)));
+    h1[(nt >> 1) * 4 + (nt & 1) * 2 + 1] =
+        pack2(__float2bfloat16_rn(silu(c[2] + bl)), __float2bfloat16_rn(silu(c[3] + bh)));
+  }
+  uint32_t h2[16];
+#pragma unroll
+  for (int nt = 0; nt < 8; ++nt) {
+    float c[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+#pragma unroll
+    for (int kt = 0; kt < 4; ++kt) {
+      const __nv_bfloat16* wr = w2 + (nt * 8 + g) * 64 + kt * 16 + k0;
+      mma_regs(c, h1[kt * 4], h1[kt * 4 + 1], h1[kt * 4 + 2], h1[kt * 4 + 3], ldg_pair(wr), ldg_pair(wr + 8));
+    }
+    float bl = __ldg(&wf[kOffB2 + nt * 8 + k0]), bh = __ldg(&wf[kOffB2 + nt * 8 + k0 + 1]);
+    h2[(nt >> 1) * 4 + (nt & 1) * 2] = pack2(__float2bfloat16_rn(silu(c[0] + bl)), __float2bfloat16_rn(silu(c[1] + bh)));
+    h2[(nt >> 1) * 4 + (nt & 1) * 2 + 1] =
+        pack2(__float2bfloat16_rn(silu(c[2] + bl)), __float2bfloat16_rn(silu(c[3] + bh)));
+  }
+  float c[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+#pragma unroll
+  for (int kt = 0; kt < 4; ++kt) {
+    // output columns 4..7 of the padded W3 are zero rows
+    uint32_t b0 = 0u, b1 = 0u;
+    if (g < 4) {
+      const __nv_bfloat16* wr = w3 + g * 64 + kt * 16 + k0;
+      b0 = ldg_pair(wr);
+      b1 = ldg_pair(wr + 8);
+    }
+    mma_regs(c, h2[kt * 4], h2[kt * 4 + 1], h2[kt * 4 + 2], h2[kt * 4 + 3], b0, b1);
+  }
+  if (t < 2) {
+    float bl = __ldg(&wf[kOffB3 + k0]), bh = __ldg(&wf[kOffB3 + k0 + 1]);
+    y[g * 4 + k0] = c[0] + bl;
+    y[g * 4 + k0 + 1] = c[1] + bh;
+    y[(g + 8) * 4 + k0] = c[2] + bl;
+    y[(g + 8) * 4 + k0 + 1] = c[3] + bh;
+  }
+}
+
 // Sum of a C-fragment column over the 16 rows (lanes with equal t), in lanes
 // 0..3 (columns 2t, 2t+1).
 __device__ __forceinline__ void colsum(float c[4], float& s0, float& s1) {
