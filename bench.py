@@ -194,36 +194,23 @@ def cpu_reference_run(sc, steps: int, warmup: int, budget_s: float, threads: int
     return len(sc.particles) * done / el, done, el
 
 
-def run_batch_arm(args):
-    """Batched step of independent boxes against the same instances solved
-    one after another (each through its own single-simulation handle)."""
+def measure_batch(scs, steps: int, warmup: int, local: int) -> dict:
+    """Batched step of independent simulations (one handle, one launch per
+    stage, graph-captured, CFL dt per instance on the device) against the same
+    instances solved one after another, each through its own single-simulation
+    handle with the same launch shapes: device times of ``steps`` steps."""
     import torch
-    from ultraballpit_b200 import domain
     from ultraballpit_b200.kernel import CudaBatch, CudaKernel
-    from ultraballpit_b200.replicas import Replicas
-    rank, world, local = dist_env()
-    torch.cuda.set_device(local)
-    rep = Replicas("nccl")
-    w = WORKLOADS[args.workload]
-    if args.shard:
-        # one draw shared by all ranks, instances bin-packed across the GPUs
-        from ultraballpit_b200.replicas import partition_lpt
-        allscs = domain.batch_boxes(w["batch"], seed=args.seed, draw=w.get("draw", "stated"))
-        mine = partition_lpt([len(s.particles) for s in allscs], world)[rank]
-        scs = [allscs[i] for i in mine]
-    else:
-        scs = domain.batch_boxes(w["batch"], seed=args.seed + rank, draw=w.get("draw", "stated"))
-    ntot = sum(len(s.particles) for s in scs)
     b = CudaBatch(scs, device=local)
     stream = torch.cuda.ExternalStream(b.stream())
     tuned = b.autotune(3)
-    b.step_auto(args.warmup, want_dt=True)
+    b.step_auto(warmup, want_dt=True)
     torch.cuda.synchronize()
     l0 = b.launch_count()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(local) as clk:
         e0.record(stream)
-        b.step_auto(args.steps, want_dt=False)
+        b.step_auto(steps, want_dt=False)
         e1.record(stream)
         e1.synchronize()
     ms = e0.elapsed_time(e1)
@@ -242,16 +229,40 @@ def run_batch_arm(args):
         k = CudaKernel(*sc.kernel_args(), alpha=sc.alpha, device=local)
         k.set_launch(**tuned)
         st = torch.cuda.ExternalStream(k.stream())
-        k.step_auto(args.warmup, want_dt=True)
+        k.step_auto(warmup, want_dt=True)
         a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         a0.record(st)
-        k.step_auto(args.steps, want_dt=False)
+        k.step_auto(steps, want_dt=False)
         a1.record(st)
         a1.synchronize()
         seq_ms += a0.elapsed_time(a1)
+        k.synchronize()
         k.close()
-    value, ms = rep.whole_job_rate(ntot, args.steps, ms)
-    seq_value, seq_ms = rep.whole_job_rate(ntot, args.steps, seq_ms)
+    return dict(ms=ms, seq_ms=seq_ms, launches=launches, tuned=tuned, prof=prof, clk=clk.summary())
+
+
+def run_batch_arm(args):
+    """Batched step of independent boxes against the same instances solved
+    one after another (each through its own single-simulation handle)."""
+    import torch
+    from ultraballpit_b200 import domain
+    from ultraballpit_b200.replicas import Replicas
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    rep = Replicas("nccl")
+    w = WORKLOADS[args.workload]
+    if args.shard:
+        # one draw shared by all ranks, instances bin-packed across the GPUs
+        from ultraballpit_b200.replicas import partition_lpt
+        allscs = domain.batch_boxes(w["batch"], seed=args.seed, draw=w.get("draw", "stated"))
+        mine = partition_lpt([len(s.particles) for s in allscs], world)[rank]
+        scs = [allscs[i] for i in mine]
+    else:
+        scs = domain.batch_boxes(w["batch"], seed=args.seed + rank, draw=w.get("draw", "stated"))
+    ntot = sum(len(s.particles) for s in scs)
+    m = measure_batch(scs, args.steps, args.warmup, local)
+    value, ms = rep.whole_job_rate(ntot, args.steps, m["ms"])
+    seq_value, seq_ms = rep.whole_job_rate(ntot, args.steps, m["seq_ms"])
     per_rank = rep.gather({"instances": len(scs), "particles": ntot})
     rep.close()
     counts = [len(s.particles) for s in scs]
@@ -265,16 +276,36 @@ def run_batch_arm(args):
                    "per_rank": per_rank,
                    "boundary_particles": sum(len(s.boundary) for s in scs),
                    "instance_particles_min_max": [min(counts), max(counts)],
-                   "size_histogram_log2": domain.size_histogram(scs), "launch": tuned,
+                   "size_histogram_log2": domain.size_histogram(scs), "launch": m["tuned"],
                    "dt": "device CFL per instance", "l2": "inputs larger than L2"},
         "sequential": {"value": seq_value, "unit": UNIT, "ms_per_step": seq_ms / args.steps,
                        "how": "each instance alone through sph_create, same launch shapes, graph-captured"},
         "batched_over_sequential": value / seq_value,
-        "stage_us": {kk: round(v, 1) for kk, v in prof.items()},
-        "clocks": clk.summary(), "gpu_launches": launches,
+        "stage_us": {kk: round(v, 1) for kk, v in m["prof"].items()},
+        "clocks": m["clk"], "gpu_launches": m["launches"],
     }
     if rank == 0:
         print(json.dumps(line), flush=True)
+
+
+def batched_subrecord(args, local: int) -> dict:
+    """The batched form beside the default line: a seeded draw of
+    ``--batch-instances`` boxes at dx = 2 mm with particle counts log-uniform
+    in [2k, 400k] (the batch workload's draw, fewer instances so the default
+    run stays short), batched against one after another."""
+    from ultraballpit_b200 import domain
+    scs = domain.batch_boxes(args.batch_instances, seed=args.seed, draw="loguniform")
+    ntot = sum(len(s.particles) for s in scs)
+    m = measure_batch(scs, args.steps, args.warmup, local)
+    counts = [len(s.particles) for s in scs]
+    value = ntot * args.steps / (m["ms"] / 1e3)
+    seq = ntot * args.steps / (m["seq_ms"] / 1e3)
+    return {"workload": "batch_boxes_2mm_loguniform", "instances": len(scs), "particles": ntot,
+            "instance_particles_min_max": [min(counts), max(counts)], "value": value, "unit": UNIT,
+            "ms_per_step": m["ms"] / args.steps, "sequential_value": seq,
+            "sequential_ms_per_step": m["seq_ms"] / args.steps, "batched_over_sequential": value / seq,
+            "launch": m["tuned"], "gpu_launches": m["launches"], "clocks": m["clk"],
+            "stage_us": {kk: round(v, 1) for kk, v in m["prof"].items()}}
 
 
 def run_batch_closure_arm(args):
@@ -539,6 +570,10 @@ def run_cuda_arm(args):
                              "pageable host arrays (two calls: count, then fill)"}
         del sp, sb
 
+    batched = None
+    if world == 1 and args.batch_instances > 0:
+        batched = batched_subrecord(args, local)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
@@ -563,7 +598,7 @@ def run_cuda_arm(args):
             "data": "synthetic (seeded dam break, host-built)",
             "config": plain_config(args, sc, world),
             "clocks": clk.summary(), "gpu_launches": launches, "e2e": e2e,
-            "roofline": roofline, "cpu_baseline": cpu, "domain_setup": setup,
+            "roofline": roofline, "cpu_baseline": cpu, "domain_setup": setup, "batched": batched,
         }
         print(json.dumps(line), flush=True)
 
@@ -579,6 +614,8 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=25.0)
     ap.add_argument("--ref-budget", type=float, default=150.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--batch-instances", type=int, default=64,
+                    help="default workload: instances of the batched sub-record (0: none)")
     ap.add_argument("--shard", action="store_true",
                     help="batch workloads: bin-pack one draw of instances across the ranks (strong scaling)")
     args = ap.parse_args()
