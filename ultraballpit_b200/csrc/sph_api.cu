@@ -82,6 +82,8 @@ struct SphHandle {
   uint32_t *nbr = nullptr, *ncount = nullptr;
   // XSPH gather records: (x, y, z, m), (v + a dt/2, rho) per particle
   float4* xrec = nullptr;
+  float* xyz = nullptr;     // sorted positions as x | y | z planes (the density scan's candidates)
+  size_t xyz_stride = 0;
   // viewer frames (sph_pack_frame): temperature on the device (uploaded on
   // the first call) and the packed particle records
   float* temp_dev = nullptr;
@@ -521,6 +523,8 @@ void dispatch(SphHandle* h, bool boundary, F&& f) {
   else f(sph::ManySim{h->ktab, boundary ? h->inst_b : h->inst_p});
 }
 
+sph::Planes planes(SphHandle* h) { return sph::Planes{h->xyz, h->xyz_stride}; }
+
 // Sorting scratch + binning of posU into the cell tables (k_bin or the
 // xsph kernel fill `hist` first).
 void enqueue_scan_fill(SphHandle* h) {
@@ -539,22 +543,22 @@ void enqueue_density_only(SphHandle* h) {
   int bs = h->bs_density;
   sph::ClosureBufs cb{h->cl_count, h->cl_slot, h->cl_feat, h->cl_rho, h->corr, h->vel, h->cl_wb, h->cl_wf};
   if (h->cl_mode) cudaMemsetAsync(h->cl_count, 0, sizeof(uint32_t), h->st);
-  const size_t smem = bs * kNbrChunk * sizeof(uint32_t);
+  const size_t smem = bs * kStageRing * sizeof(uint32_t);
   // closure mode 2 adds a 16-sample network tile per warp (the fused inference)
   const size_t smem_cl = smem + (bs / 32) * kClTileWords * sizeof(uint32_t);
   dispatch(h, false, [&](auto kp) {
     using KPT = decltype(kp);
     if (h->cl_mode == 2)
-      k_density<KPT, 2><<<grid_for(h->n, bs), bs, smem_cl, h->st>>>(kp, h->n, h->dt, h->pos, h->rv, h->id, h->ctab,
+      k_density<KPT, 2><<<grid_for(h->n, bs), bs, smem_cl, h->st>>>(kp, h->n, h->dt, h->pos, planes(h), h->rv, h->id, h->ctab,
                                                                    h->bc_start, h->bc_list, h->bpos, h->rf, h->pr,
                                                                    h->err, h->nbr, h->ncount, h->sdf, h->wall_tab,
                                                                    cb);
     else if (h->cl_mode)
-      k_density<KPT, 1><<<grid_for(h->n, bs), bs, smem, h->st>>>(kp, h->n, h->dt, h->pos, h->rv, h->id, h->ctab,
+      k_density<KPT, 1><<<grid_for(h->n, bs), bs, smem, h->st>>>(kp, h->n, h->dt, h->pos, planes(h), h->rv, h->id, h->ctab,
                                                                 h->bc_start, h->bc_list, h->bpos, h->rf, h->pr,
                                                                 h->err, h->nbr, h->ncount, h->sdf, h->wall_tab, cb);
     else
-      k_density<KPT, 0><<<grid_for(h->n, bs), bs, smem, h->st>>>(kp, h->n, h->dt, h->pos, h->rv, h->id, h->ctab,
+      k_density<KPT, 0><<<grid_for(h->n, bs), bs, smem, h->st>>>(kp, h->n, h->dt, h->pos, planes(h), h->rv, h->id, h->ctab,
                                                                 h->bc_start, h->bc_list, h->bpos, h->rf, h->pr,
                                                                 h->err, h->nbr, h->ncount, h->sdf, h->wall_tab, cb);
   });
@@ -624,7 +628,7 @@ void enqueue_sort(SphHandle* h) {
   enqueue_scan_fill(h);
   k_reorder<<<grid_for(h->n, 256), 256, 0, h->st>>>(h->n, h->tmp, h->tmpid, h->keyU, h->cstart, h->ccount,
                                                     h->posU, h->velU, h->pos, h->vel, h->rv, h->id, h->err,
-                                                    nullptr, nullptr, nullptr, nullptr, nullptr);
+                                                    nullptr, nullptr, nullptr, nullptr, nullptr, planes(h));
   h->launches += 1;
 }
 
@@ -846,6 +850,8 @@ int create_impl(int ninst, const SphParams* PP, const SphParticlesView* pvs,
     ALLOC(var, 1); ALLOC(bad, 1);
     ALLOC(stage, 12 * n); ALLOC(stage_ft, n); ALLOC(diag, 2);
     ALLOC(nbr, (size_t)sph::kNbrCap * n); ALLOC(ncount, n); ALLOC(xrec, 2 * n);
+    h->xyz_stride = ((size_t)n + 3) / 4 * 4 + 4;  // aligned groups of 4 may read past the last slot
+    ALLOC(xyz, 3 * h->xyz_stride);
     if (ninst > 1) {
       ALLOC(ktab, ninst); ALLOC(inst_p, n); ALLOC(inst_b, nb);
     }
@@ -1043,6 +1049,7 @@ int create_impl(int ninst, const SphParams* PP, const SphParticlesView* pvs,
   if (e == cudaSuccess) e = cudaMemsetAsync(h->bpress, 0, std::max<size_t>(1, nb) * sizeof(float), h->st);
   if (e == cudaSuccess) e = cudaMemsetAsync(h->err, 0, sizeof(uint32_t), h->st);
   if (e == cudaSuccess) e = cudaMemsetAsync(h->ctab, 0, C * sizeof(uint2), h->st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(h->xyz, 0, 3 * h->xyz_stride * sizeof(float), h->st);
   if (e == cudaSuccess && n > 0) {
     using namespace sph;
     dispatch(h, false, [&](auto kp) {
@@ -1052,7 +1059,8 @@ int create_impl(int ninst, const SphParams* PP, const SphParticlesView* pvs,
     enqueue_scan_fill(h);
     k_reorder<<<grid_for(h->n, 256), 256, 0, h->st>>>(h->n, h->tmp, h->tmpid, h->keyU, h->cstart,
                                                       h->ccount, h->posU, h->velU, h->pos, h->vel, h->rv,
-                                                      h->id, h->err, accU, h->acc, prU, h->pr, h->velout);
+                                                      h->id, h->err, accU, h->acc, prU, h->pr, h->velout,
+                                                      planes(h));
     h->launches += 1;
     e = cudaGetLastError();
   }
@@ -1321,7 +1329,8 @@ void enqueue_save_ck(SphHandle* h) {
 
 void enqueue_restore_ck(SphHandle* h) {
   sph::k_restore<<<grid_for(h->n, 256), 256, 0, h->st>>>(h->n, h->id, h->ck_slot, h->ck_pos, h->ck_velout,
-                                                        h->ck_acc, h->ck_pr, h->pos, h->velout, h->acc, h->pr);
+                                                        h->ck_acc, h->ck_pr, h->pos, h->velout, h->acc, h->pr,
+                                                        planes(h));
   h->launches += 1;
 }
 }  // namespace

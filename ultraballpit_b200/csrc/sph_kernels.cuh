@@ -34,6 +34,7 @@ constexpr int kAdamiCap = 256;         // fluid terms per boundary particle
 constexpr int kCellCap = 4096;         // particles per cell for the id ranking
 constexpr uint32_t kNbrCap = 128;      // listed neighbours per particle
 constexpr uint32_t kNbrChunk = 8;      // list entries per 32-byte chunk
+constexpr uint32_t kStageRing = 16;    // staged list entries per thread (two chunks)
 // The neighbour kernels are latency-bound on gathered loads, so occupancy
 // pays more than registers: k_density is capped at 48 registers, k_forces
 // and k_xsph_drift (whose replays put two neighbours' gathers in flight
@@ -453,15 +454,28 @@ __device__ __forceinline__ void dist2_pair(unsigned long long X, unsigned long l
   f2_unpack(f2_add(f2_add(f2_mul(dx, dx), f2_mul(dy, dy)), f2_mul(dz, dz)), da, db);
 }
 
-// The visit of for_each_neighbor reduced to the support test, for recording:
-// rec(slot, ok) for every candidate in the same order, ok = in support;
-// `self` is never offered (the home cell's range is split around it).
-// Calling rec for every candidate (not only the kept ones) lets the caller
-// record without a divergent branch per candidate.
-template <class R>
-__device__ __forceinline__ void scan_support(float px, float py, float pz, int self,
-                                             const float4* __restrict__ pos, const uint2* __restrict__ ctab,
-                                             const SimConst& k, R&& rec) {
+// Positions in the sorted order as three planes (x, y, z) of `stride` floats
+// each, stride a multiple of 4 with zero padding past the last slot, so that
+// four consecutive candidates' coordinates are one aligned 16-byte load and
+// come packed for the f32x2 arithmetic. Written by k_reorder and k_restore
+// beside the float4 state.
+struct Planes {
+  float* __restrict__ xyz;
+  size_t stride;
+};
+
+// The density pass's recording scan over the SoA planes: the candidates of a
+// range are taken in aligned groups of four (lanes outside [s, e) masked),
+// each group's distances in two f32x2 pairs rounded exactly as the scalar
+// expression, and the in-support slots appended in visit order to a 16-entry
+// ring of this thread's shared-memory column; every full chunk of 8 goes out
+// as one 32-byte store (entry c of slot i at nbr_index(c, n, i); at most
+// kNbrCap entries are stored, the count is returned in full). The cells and
+// rows visited, and the order, are scan_support's.
+__device__ __forceinline__ uint32_t record_neighbors(float px, float py, float pz, int self, Planes pl,
+                                                     const uint2* __restrict__ ctab, const SimConst& k,
+                                                     uint32_t* __restrict__ nbr, int n, uint32_t* stage,
+                                                     unsigned bsz) {
   int cx = axis_cell(px, k.gmin[0], k.cell, k.dims[0]);
   int cy = axis_cell(py, k.gmin[1], k.cell, k.dims[1]);
   int cz = axis_cell(pz, k.gmin[2], k.cell, k.dims[2]);
@@ -479,8 +493,52 @@ __device__ __forceinline__ void scan_support(float px, float py, float pz, int s
       hi2[a] = dh * dh;
     }
   }
+  const float* xs = pl.xyz;
+  const float* ys = pl.xyz + pl.stride;
+  const float* zs = pl.xyz + 2 * pl.stride;
   const unsigned long long X = f2_pack(px, px), Y = f2_pack(py, py), Z = f2_pack(pz, pz);
   const float r2 = k.radius_sq;
+  uint32_t listed = 0, flushed = 0;
+  auto flush = [&](uint32_t m) {  // the ring's chunk at `flushed`, m entries valid
+    const uint32_t* r = stage + (flushed & (kStageRing - 1u)) * bsz;
+    uint4* dst = reinterpret_cast<uint4*>(nbr + ((size_t)(flushed / kNbrChunk) * (size_t)n + (size_t)self) *
+                                          kNbrChunk);
+    dst[0] = make_uint4(r[0], m > 1 ? r[bsz] : 0u, m > 2 ? r[2 * bsz] : 0u, m > 3 ? r[3 * bsz] : 0u);
+    dst[1] = make_uint4(m > 4 ? r[4 * bsz] : 0u, m > 5 ? r[5 * bsz] : 0u, m > 6 ? r[6 * bsz] : 0u,
+                        m > 7 ? r[7 * bsz] : 0u);
+  };
+  auto range = [&](int s, int e) {
+    for (int g = s & ~3; g < e; g += 4) {
+      float4 qx = __ldg(reinterpret_cast<const float4*>(xs + g));
+      float4 qy = __ldg(reinterpret_cast<const float4*>(ys + g));
+      float4 qz = __ldg(reinterpret_cast<const float4*>(zs + g));
+      unsigned long long dx01 = f2_sub(X, f2_pack(qx.x, qx.y)), dx23 = f2_sub(X, f2_pack(qx.z, qx.w));
+      unsigned long long dy01 = f2_sub(Y, f2_pack(qy.x, qy.y)), dy23 = f2_sub(Y, f2_pack(qy.z, qy.w));
+      unsigned long long dz01 = f2_sub(Z, f2_pack(qz.x, qz.y)), dz23 = f2_sub(Z, f2_pack(qz.z, qz.w));
+      float d0, d1, d2, d3;
+      f2_unpack(f2_add(f2_add(f2_mul(dx01, dx01), f2_mul(dy01, dy01)), f2_mul(dz01, dz01)), d0, d1);
+      f2_unpack(f2_add(f2_add(f2_mul(dx23, dx23), f2_mul(dy23, dy23)), f2_mul(dz23, dz23)), d2, d3);
+      const int lo = s - g, hi = e - g;
+      const bool ok0 = d0 <= r2 && 0 >= lo && 0 < hi;
+      const bool ok1 = d1 <= r2 && 1 >= lo && 1 < hi;
+      const bool ok2 = d2 <= r2 && 2 >= lo && 2 < hi;
+      const bool ok3 = d3 <= r2 && 3 >= lo && 3 < hi;
+      // each slot is written at the ring's next entry and kept only if the
+      // entry advances
+      stage[(listed & (kStageRing - 1u)) * bsz] = (uint32_t)g;
+      listed += ok0 ? 1u : 0u;
+      stage[(listed & (kStageRing - 1u)) * bsz] = (uint32_t)(g + 1);
+      listed += ok1 ? 1u : 0u;
+      stage[(listed & (kStageRing - 1u)) * bsz] = (uint32_t)(g + 2);
+      listed += ok2 ? 1u : 0u;
+      stage[(listed & (kStageRing - 1u)) * bsz] = (uint32_t)(g + 3);
+      listed += ok3 ? 1u : 0u;
+      if (listed - flushed >= kNbrChunk) {  // a group adds at most 4: one chunk at a time
+        if (flushed + kNbrChunk <= kNbrCap) flush(kNbrChunk);
+        flushed += kNbrChunk;
+      }
+    }
+  };
   for (int dz = -1; dz <= 1; ++dz) {
     int nz = cz + dz;
     if (nz < 0 || nz >= k.dims[2]) continue;
@@ -491,27 +549,7 @@ __device__ __forceinline__ void scan_support(float px, float py, float pz, int s
       float ey = ez + (dy < 0 ? lo2[1] : (dy > 0 ? hi2[1] : 0.0f));
       if (ey > r2) continue;
       int row = k.coff + (ny + nz * k.dims[1]) * k.dims[0];
-      auto range = [&](int s, int end) {
-        for (; s + 3 < end; s += 4) {
-          float4 q0 = __ldg(&pos[s]), q1 = __ldg(&pos[s + 1]), q2 = __ldg(&pos[s + 2]), q3 = __ldg(&pos[s + 3]);
-          float d0, d1, d2, d3;
-          dist2_pair(X, Y, Z, q0, q1, d0, d1);
-          dist2_pair(X, Y, Z, q2, q3, d2, d3);
-          rec(s, d0 <= r2);
-          rec(s + 1, d1 <= r2);
-          rec(s + 2, d2 <= r2);
-          rec(s + 3, d3 <= r2);
-        }
-        for (; s < end; ++s) {
-          float4 q = __ldg(&pos[s]);
-          float ax = px - q.x, ay = py - q.y, az = pz - q.z;
-          rec(s, ax * ax + ay * ay + az * az <= r2);
-        }
-      };
       if (k.rows) {
-        // the row's surviving cells are consecutive (the home column always
-        // survives once the row does), and so are their particles: one range
-        // in the same order as three cell visits
         int xa = (cx > 0 && ey + lo2[0] <= r2) ? cx - 1 : cx;
         int xb = (cx + 1 < k.dims[0] && ey + hi2[0] <= r2) ? cx + 1 : cx;
         uint2 sa = __ldg(&ctab[row + xa]), sb = __ldg(&ctab[row + xb]);
@@ -537,6 +575,8 @@ __device__ __forceinline__ void scan_support(float px, float py, float pz, int s
       }
     }
   }
+  if (listed > flushed && flushed + kNbrChunk <= kNbrCap) flush(listed - flushed);  // the open chunk
+  return listed;
 }
 
 // Neighbour lists: entry c of slot i lies in chunk c / 8 of the slot, and the
@@ -809,7 +849,7 @@ k_reorder(int n, const uint32_t* __restrict__ tmp, const uint32_t* __restrict__ 
           const float4* __restrict__ velU, float4* __restrict__ pos, float4* __restrict__ vel,
           float2* __restrict__ rv, uint32_t* __restrict__ id, uint32_t* __restrict__ err,
           const float4* __restrict__ accU, float4* __restrict__ acc,
-          const float* __restrict__ prU, float* __restrict__ pr, float4* __restrict__ velout) {
+          const float* __restrict__ prU, float* __restrict__ pr, float4* __restrict__ velout, Planes pl) {
   int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= n) return;
   uint32_t i = tmp[s];
@@ -828,6 +868,9 @@ k_reorder(int n, const uint32_t* __restrict__ tmp, const uint32_t* __restrict__ 
   float4 p = posU[i];
   float4 v = velU[i];
   pos[d] = p;
+  pl.xyz[d] = p.x;
+  pl.xyz[pl.stride + d] = p.y;
+  pl.xyz[2 * pl.stride + d] = p.z;
   vel[d] = v;
   rv[d] = make_float2(v.w, p.w / v.w);
   id[d] = myid;
@@ -890,7 +933,7 @@ __device__ __forceinline__ void closure_apply_one(const SimConst& k, int i, bool
 constexpr int kClTileWords = 16 * 16 / 2 + 16 * 4;  // BF16 x tile + FP32 y tile, in 32-bit words
 template <class KP, int CL>
 __global__ void __maxnreg__(CL == 2 ? 96 : 48)
-k_density(KP kp, int n, const float* __restrict__ dtp, const float4* __restrict__ pos,
+k_density(KP kp, int n, const float* __restrict__ dtp, const float4* __restrict__ pos, Planes pl,
           const float2* __restrict__ rv, const uint32_t* __restrict__ id,
           const uint2* __restrict__ ctab, const uint32_t* __restrict__ bc_start,
           const uint32_t* __restrict__ bc_list, const float4* __restrict__ bpos,
@@ -914,33 +957,12 @@ k_density(KP kp, int n, const float* __restrict__ dtp, const float4* __restrict_
   float rho = pi.w * k.norm_h3;
   float diff_sum = 0.0f;
   bool delta = (k.flags & kFlagDelta) != 0;
-  // Phase 1: the 27-cell scan only records in-support slots, in visit order;
-  // entry j of the open chunk is staged at stage[j * blockDim.x] (this
-  // thread's column of the block's dynamic shared memory) and each full chunk
-  // goes out as one 32-byte store.
-  uint32_t listed = 0;
+  // Phase 1: the 27-cell scan records the in-support slots, in visit order,
+  // through this thread's column of the block's dynamic shared memory
+  // (entry j of the ring at s_stage[j * blockDim.x + threadIdx.x]).
   extern __shared__ uint32_t s_stage[];
-  uint32_t* stage = s_stage + threadIdx.x;
-  const unsigned bsz = blockDim.x;
-  auto flush = [&](uint32_t chunk) {
-    uint4* dst = reinterpret_cast<uint4*>(nbr + ((size_t)chunk * (size_t)n + (size_t)i) * kNbrChunk);
-    dst[0] = make_uint4(stage[0], stage[bsz], stage[2 * bsz], stage[3 * bsz]);
-    dst[1] = make_uint4(stage[4 * bsz], stage[5 * bsz], stage[6 * bsz], stage[7 * bsz]);
-  };
-  uint32_t* sp = stage;  // the open chunk's next entry
-  uint32_t* const chunk_end = stage + kNbrChunk * bsz;
-  scan_support(pi.x, pi.y, pi.z, i, pos, ctab, k, [&](int s, bool ok) {
-    *sp = (uint32_t)s;  // kept only if ok advances the entry
-    if (ok) {
-      sp += bsz;
-      ++listed;
-      if (sp == chunk_end) {
-        if (listed <= kNbrCap) flush((listed - 1) / kNbrChunk);
-        sp = stage;
-      }
-    }
-  });
-  if (listed < kNbrCap && listed % kNbrChunk != 0) flush(listed / kNbrChunk);  // the open chunk
+  const uint32_t listed = record_neighbors(pi.x, pi.y, pi.z, i, pl, ctab, k, nbr, n, s_stage + threadIdx.x,
+                                           blockDim.x);
   ncount[i] = listed;
   // Phase 2: density and delta-SPH terms over the list, same order.
   auto term_rv = [&](const float4& pj, const float2& rvj, float dx, float dy, float dz, float d2) {
@@ -1077,7 +1099,7 @@ k_density(KP kp, int n, const float* __restrict__ dtp, const float4* __restrict_
     // network epilogue: up to 16 of the warp's near-wall particles per tile
     extern __shared__ uint32_t s_stage[];
     const int lane = threadIdx.x & 31;
-    uint32_t* tile = s_stage + kNbrChunk * blockDim.x + (threadIdx.x >> 5) * kClTileWords;
+    uint32_t* tile = s_stage + kStageRing * blockDim.x + (threadIdx.x >> 5) * kClTileWords;
     __nv_bfloat16* xt = reinterpret_cast<__nv_bfloat16*>(tile);
     float* yt = reinterpret_cast<float*>(tile + 16 * 16 / 2);
     unsigned pending = __ballot_sync(0xffffffffu, near_wall);
@@ -1759,11 +1781,15 @@ __global__ void k_restore(int n, const uint32_t* __restrict__ id, const uint32_t
                           const float4* __restrict__ ck_pos, const float4* __restrict__ ck_velout,
                           const float4* __restrict__ ck_acc, const float* __restrict__ ck_pr,
                           float4* __restrict__ pos, float4* __restrict__ velout,
-                          float4* __restrict__ acc, float* __restrict__ pr) {
+                          float4* __restrict__ acc, float* __restrict__ pr, Planes pl) {
   int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= n) return;
   uint32_t c = ck_slot[id[s] & kIdMask];
-  pos[s] = ck_pos[c];
+  float4 p = ck_pos[c];
+  pos[s] = p;
+  pl.xyz[s] = p.x;
+  pl.xyz[pl.stride + s] = p.y;
+  pl.xyz[2 * pl.stride + s] = p.z;
   velout[s] = ck_velout[c];
   acc[s] = ck_acc[c];
   pr[s] = ck_pr[c];
