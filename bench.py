@@ -34,6 +34,7 @@ UNIT = "particle-steps/s"
 WORKLOADS = {
     "dam_break_1mm_sphere": dict(dx=0.001, sphere=True),   # 2,000,000 particles
     "dam_break_4mm": dict(dx=0.004, sphere=False),          # 31,250 particles
+    "dam_break_2mm": dict(dx=0.002, sphere=False),          # 250,000 particles (profiling case)
     "batch_boxes_2mm": dict(batch=256),                     # 256 instances, about 51M particles
     "batch_boxes_2mm_loguniform": dict(batch=256, draw="loguniform"),  # 256 instances, about 20M
     # 64 sphere-in-tank flows at 4 mm with the learned closure (about 8.6M particles)
