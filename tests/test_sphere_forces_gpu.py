@@ -3,7 +3,10 @@ against the CPU oracle: the first 10 steps of the 2,000,000-particle dam
 break with the sphere, sampled every 5 steps. The states are bit-identical
 (correctly rounded x^7 in both); the FP64 integrals on the sphere (the
 fluid's reaction on the sphere's boundary particles, and force.rs's surface
-integral) differ only in summation order: within 1e-9 relative."""
+integral) differ only in summation order: within 1e-9 relative. (The
+water front reaches the sphere only after several thousand steps, so these
+early samples check the plumbing of the series; the integrals themselves are
+checked against the oracle on a submerged sphere in test_parity_gpu.)"""
 import os
 
 import numpy as np
@@ -36,4 +39,3 @@ def test_sphere_force_series_matches_the_oracle():
             a, b = np.asarray(s[key]), np.asarray(w[key])
             assert np.allclose(a, b, rtol=1e-9, atol=1e-12 * max(1.0, np.abs(b).max())), (key, a, b)
         assert s["surface_force_f32"] == w["surface_force_f32"]
-    assert np.linalg.norm(res["samples"][-1]["pressure_force"]) > 0.0
