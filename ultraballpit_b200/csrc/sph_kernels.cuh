@@ -41,6 +41,16 @@ constexpr uint32_t kStageRing = 16;    // staged list entries per thread (two ch
 // before using them) at 56 (__maxnreg__ below; each measured at 2M particles
 // against caps from 40 to 72 and the compiler's choice, same results).
 
+#ifndef SPH_MAXNREG_DENSITY
+#define SPH_MAXNREG_DENSITY 48
+#endif
+#ifndef SPH_MAXNREG_FORCES
+#define SPH_MAXNREG_FORCES 56
+#endif
+#ifndef SPH_MAXNREG_XSPH
+#define SPH_MAXNREG_XSPH 56
+#endif
+
 enum : uint32_t { kFlagDelta = 1, kFlagXsph = 2, kFlagRepulsion = 4, kFlagClamp = 8 };
 enum : uint32_t { kErrCellCap = 1, kErrAdamiCap = 2 };
 
@@ -632,7 +642,7 @@ k_xsph_prep(KP kp, int n, const float* __restrict__ dtp, const float4* __restric
 // (neighbor.rs:89-101) into a rank-indexed histogram. Reads the sorted state,
 // writes the unsorted "U" arrays in the same slot order.
 template <class KP>
-__global__ void __maxnreg__(56)
+__global__ void __maxnreg__(SPH_MAXNREG_XSPH)
 k_xsph_drift(KP kp, int n, const float* __restrict__ dtp, const float4* __restrict__ pos,
              const float4* __restrict__ velout, const float4* __restrict__ acc, const float4* __restrict__ rec,
              const uint32_t* __restrict__ id, const uint2* __restrict__ ctab,
@@ -932,7 +942,7 @@ __device__ __forceinline__ void closure_apply_one(const SimConst& k, int i, bool
 // register cap for the network's fragments.
 constexpr int kClTileWords = 16 * 16 / 2 + 16 * 4;  // BF16 x tile + FP32 y tile, in 32-bit words
 template <class KP, int CL>
-__global__ void __maxnreg__(CL == 2 ? 96 : 48)
+__global__ void __maxnreg__(CL == 2 ? 96 : SPH_MAXNREG_DENSITY)
 k_density(KP kp, int n, const float* __restrict__ dtp, const float4* __restrict__ pos, Planes pl,
           const float2* __restrict__ rv, const uint32_t* __restrict__ id,
           const uint2* __restrict__ ctab, const uint32_t* __restrict__ bc_start,
@@ -1347,7 +1357,7 @@ k_adami(KP kp, int nb, const float4* __restrict__ bpos, float* __restrict__ bpre
 // repulsion (lib.rs:247-282; sph.rs:322-508; boundary.rs:143-181), then
 // kick 2 (lib.rs:330-334) and the dt reduction inputs (sph.rs:597-616).
 template <class KP, int CL>
-__global__ void __maxnreg__(56)
+__global__ void __maxnreg__(SPH_MAXNREG_FORCES)
 k_forces(KP kp, int n, const float* __restrict__ dtp, float hdt_scale,
          const float4* __restrict__ pos, const float4* __restrict__ vel,
          const float2* __restrict__ rf, const float* __restrict__ pr,
