@@ -1274,53 +1274,30 @@ k_adami(KP kp, int nb, const float4* __restrict__ bpos, float* __restrict__ bpre
     if (lane == 0) atomicOr(err, kErrAdamiCap);
     return;
   }
-  if (count <= 64) {
-    // up to 64 terms in registers, term e in lane e % 32 (half e / 32): a
-    // bitonic sort by fluid index across the lanes (exchanges between the
-    // halves of one lane when j = 32), then the sum in that order (the same
-    // additions as the shared-memory path below). A wall particle in the
-    // first layer beside full water has about 40 terms.
+  if (count <= 32) {
+    // up to 32 terms: one per lane, bitonic-sorted by fluid index across the
+    // lanes, then summed in that order (the same additions as below)
     __syncwarp();
-    uint32_t key[2];
-    float w[2], wp[2];
-#pragma unroll
-    for (int hh = 0; hh < 2; ++hh) {
-      int e = lane + 32 * hh;
-      key[hh] = e < count ? s_id[warp][e] : 0xffffffffu;
-      w[hh] = e < count ? s_w[warp][e] : 0.0f;
-      wp[hh] = e < count ? s_wp[warp][e] : 0.0f;
-    }
-    const int width = count <= 32 ? 32 : 64;
-    for (int kk = 2; kk <= width; kk <<= 1) {
+    uint32_t key = lane < count ? s_id[warp][lane] : 0xffffffffu;
+    float w = lane < count ? s_w[warp][lane] : 0.0f;
+    float wp = lane < count ? s_wp[warp][lane] : 0.0f;
+    for (int kk = 2; kk <= 32; kk <<= 1) {
       for (int j = kk >> 1; j > 0; j >>= 1) {
-        if (j == 32) {  // kk = 64: lane-local pair (lane, lane + 32), ascending
-          if (key[1] < key[0]) {
-            uint32_t tk = key[0]; key[0] = key[1]; key[1] = tk;
-            float t = w[0]; w[0] = w[1]; w[1] = t;
-            t = wp[0]; wp[0] = wp[1]; wp[1] = t;
-          }
-          continue;
-        }
-#pragma unroll
-        for (int hh = 0; hh < 2; ++hh) {
-          if (hh == 1 && width == 32) break;
-          int e = lane + 32 * hh;
-          uint32_t ok = __shfl_xor_sync(0xffffffffu, key[hh], j);
-          float ow = __shfl_xor_sync(0xffffffffu, w[hh], j);
-          float owp = __shfl_xor_sync(0xffffffffu, wp[hh], j);
-          bool up = (e & kk) == 0, lower = (lane & j) == 0;
-          if (lower == up ? ok < key[hh] : ok > key[hh]) {
-            key[hh] = ok;
-            w[hh] = ow;
-            wp[hh] = owp;
-          }
+        uint32_t ok = __shfl_xor_sync(0xffffffffu, key, j);
+        float ow = __shfl_xor_sync(0xffffffffu, w, j);
+        float owp = __shfl_xor_sync(0xffffffffu, wp, j);
+        bool up = (lane & kk) == 0, lower = (lane & j) == 0;
+        if (lower == up ? ok < key : ok > key) {
+          key = ok;
+          w = ow;
+          wp = owp;
         }
       }
     }
     float weighted_pressure = 0.0f, weight_sum = 0.0f;
     for (int q = 0; q < count; ++q) {
-      weighted_pressure += __shfl_sync(0xffffffffu, q < 32 ? wp[0] : wp[1], q & 31);
-      weight_sum += __shfl_sync(0xffffffffu, q < 32 ? w[0] : w[1], q & 31);
+      weighted_pressure += __shfl_sync(0xffffffffu, wp, q);
+      weight_sum += __shfl_sync(0xffffffffu, w, q);
     }
     if (lane == 0) bpress[b] = weight_sum > 1.0e-12f ? fmaxf(weighted_pressure / weight_sum, 0.0f) : 0.0f;
     return;
