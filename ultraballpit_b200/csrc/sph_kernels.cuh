@@ -42,7 +42,7 @@ constexpr uint32_t kStageRing = 16;    // staged list entries per thread (two ch
 // against caps from 40 to 72 and the compiler's choice, same results).
 
 #ifndef SPH_MAXNREG_DENSITY
-#define SPH_MAXNREG_DENSITY 48
+#define SPH_MAXNREG_DENSITY 40
 #endif
 #ifndef SPH_MAXNREG_FORCES
 #define SPH_MAXNREG_FORCES 56
