@@ -54,7 +54,7 @@ struct SphHandle {
   // launch shapes (threads per block of the neighbour kernels)
   // threads per block of the neighbour kernels (sph_set_launch / sph_autotune
   // change them): the fastest shapes measured on the 2M dam break
-  int bs_xsph = 128, bs_density = 256, bs_forces = 128;
+  int bs_xsph = 128, bs_density = 128, bs_forces = 128;
   std::vector<float> temperature;
   double init_energy = 0.0, init_mass = 0.0;
   bool needs_init = true;

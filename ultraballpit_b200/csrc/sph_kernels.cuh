@@ -47,9 +47,6 @@ constexpr uint32_t kStageRing = 16;    // staged list entries per thread (two ch
 #ifndef SPH_MAXNREG_FORCES
 #define SPH_MAXNREG_FORCES 56
 #endif
-#ifndef SPH_FORCES_BRANCHLESS_VISC
-#define SPH_FORCES_BRANCHLESS_VISC 0
-#endif
 #ifndef SPH_MAXNREG_XSPH
 #define SPH_MAXNREG_XSPH 56
 #endif
@@ -1374,9 +1371,10 @@ k_forces(KP kp, int n, const float* __restrict__ dtp, float hdt_scale,
       fpz += factor * gz;
       float dvx = vi.x - vj.x, dvy = vi.y - vj.y, dvz = vi.z - vj.z;
       float vr_dot = dvx * dx + dvy * dy + dvz * dz;
-#if SPH_FORCES_BRANCHLESS_VISC
-      // every pair evaluates the term; a receding pair adds a signed zero,
-      // which leaves the sums unchanged (they start at +0 and never become -0)
+      // every pair evaluates the viscous term (no divergent branch, -2.4 %
+      // forces); a receding pair (v.r >= 0, sph.rs:460) adds a signed zero,
+      // which leaves the sums unchanged: they start at +0 and a sum that
+      // rounds to zero is +0, so they never hold -0
       float r_sq = r * r;
       float mu = k.h * vr_dot / (r_sq + k.eta_sq);
       float rho_avg = 0.5f * (rho_i + rfj.x);
@@ -1385,18 +1383,6 @@ k_forces(KP kp, int n, const float* __restrict__ dtp, float hdt_scale,
       fvx += fv * gx;
       fvy += fv * gy;
       fvz += fv * gz;
-#else
-      if (vr_dot < 0.0f) {
-        float r_sq = r * r;
-        float mu = k.h * vr_dot / (r_sq + k.eta_sq);
-        float rho_avg = 0.5f * (rho_i + rfj.x);
-        float pi_ij = (k.neg_alpha_c * mu + k.beta * mu * mu) / rho_avg;
-        float fv = -pj.w * pi_ij;
-        fvx += fv * gx;
-        fvy += fv * gy;
-        fvz += fv * gz;
-      }
-#endif
     };
     uint32_t cnt = nbr ? __ldg(&ncount[i]) : 0xffffffffu;
     if (cnt <= kNbrCap) {
