@@ -779,8 +779,9 @@ int create_impl(int ninst, const SphParams* PP, const SphParticlesView* pvs,
     cudaGetLastError();
     return SPH_ERR_NO_DEVICE;
   }
-  cudaDeviceProp prop;
-  if (cudaGetDeviceProperties(&prop, P0.device) != cudaSuccess || prop.major != 10) {
+  int major = 0;  // one attribute, not the whole property table (tens of ms)
+  if (cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, P0.device) != cudaSuccess ||
+      major != 10) {
     cudaGetLastError();
     return SPH_ERR_NO_DEVICE;
   }

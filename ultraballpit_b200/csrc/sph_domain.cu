@@ -316,8 +316,8 @@ int sph_setup_domain(int device, const SphDomainSpec* spec, const SphSdfView* sd
     cudaGetLastError();
     return SPH_ERR_NO_DEVICE;
   }
-  cudaDeviceProp prop;
-  if (cudaGetDeviceProperties(&prop, device) != cudaSuccess || prop.major != 10) {
+  int major = 0;
+  if (cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, device) != cudaSuccess || major != 10) {
     cudaGetLastError();
     return SPH_ERR_NO_DEVICE;
   }
