@@ -20,6 +20,7 @@ against the CPU oracle.
 from __future__ import annotations
 
 import argparse
+import hashlib
 import json
 import time
 
@@ -27,6 +28,9 @@ import numpy as np
 
 from . import domain
 from .kernel import CudaKernel
+
+
+STATE_FIELDS = ("x", "y", "z", "vx", "vy", "vz", "ax", "ay", "az", "density", "pressure")
 
 
 def record(step, t, body, surf):
@@ -43,9 +47,11 @@ def scenario(seed: int = 2024):
     return sc, len(sc.boundary) - nb_geo, nb_geo
 
 
-def run(steps: int = 2000, every: int = 50, seed: int = 2024, device: int = 0, on_sample=None) -> dict:
+def run(steps: int = 2000, every: int = 50, seed: int = 2024, device: int = 0, on_sample=None,
+        state_digest: bool = False) -> dict:
     """The run; ``on_sample(step, dt)`` (optional) is called after every step
-    with the step's dt, before that step's sample is taken."""
+    with the step's dt, before that step's sample is taken. ``state_digest``
+    adds the SHA-256 of the final state (STATE_FIELDS, original order)."""
     sc, first, nb_geo = scenario(seed)
     k = CudaKernel(*sc.kernel_args(), alpha=sc.alpha, beta=sc.beta, device=device)
     k.set_geometry_sdf(sc.obstacle_sdf)
@@ -63,6 +69,12 @@ def run(steps: int = 2000, every: int = 50, seed: int = 2024, device: int = 0, o
         if s % every == 0 or s == steps:
             out["samples"].append(record(s, t, k.body_force(first, nb_geo), k.surface_forces()))
     out["wall_s"] = time.perf_counter() - t0
+    if state_digest:
+        p = k.particles()
+        h = hashlib.sha256()
+        for f in STATE_FIELDS:
+            h.update(np.ascontiguousarray(getattr(p, f), np.float32).tobytes())
+        out["state_sha256"] = h.hexdigest()
     k.synchronize()
     out["health_nonfinite"] = k.health()
     k.close()
