@@ -362,3 +362,27 @@ def test_sdf_mode_tank_at_rest_stays_quiet_at_edges_and_corners():
         assert v[m].mean() < 0.12, (name, v[m].mean())
     assert p.z.max() < closure.FILL + 0.01
     k.close()
+
+
+def test_device_capacity_bounds_are_reported_not_exceeded():
+    """The kernels' own bounds end in an error status, never in an access
+    past a buffer: more than 4096 particles in one cell (the id ranking of
+    the sort) fails the creation, and a boundary particle with more than 256
+    fluid particles in support (the Adami term buffer) fails the next call
+    that reads the device flags."""
+    h = 0.01
+    n = 4097
+    p = ParticleArrays.from_positions(np.full(n, 0.5), np.full(n, 0.5), np.full(n, 0.5), 1e-6)
+    with pytest.raises(SphError) as e:
+        CudaKernel(p, None, h, (0, 0, -9.81), 20.0, 0.25, 0.0, (0, 0, 0), (1, 1, 1))
+    assert e.value.status == 6
+    rng = np.random.default_rng(3)
+    q = rng.uniform(0.497, 0.503, size=(300, 3)).astype(np.float32)
+    p = ParticleArrays.from_positions(q[:, 0], q[:, 1], q[:, 2], 1e-6)
+    b = BoundaryParticles.from_arrays([0.5], [0.5], [0.49], [1e-6], [0.0], [0.0], [1.0])
+    k = CudaKernel(p, b, h, (0, 0, -9.81), 20.0, 0.25, 0.0, (0, 0, 0), (1, 1, 1))
+    k.step(1e-6)
+    with pytest.raises(SphError) as e:
+        k.compute_timestep()
+    assert e.value.status == 6
+    k.close()

@@ -548,19 +548,19 @@ void enqueue_density_only(SphHandle* h) {
   const size_t smem_cl = smem + (bs / 32) * kClTileWords * sizeof(uint32_t);
   dispatch(h, false, [&](auto kp) {
     using KPT = decltype(kp);
+    const int grid = grid_for(h->n, bs);
     if (h->cl_mode == 2)
-      k_density<KPT, 2><<<grid_for(h->n, bs), bs, smem_cl, h->st>>>(kp, h->n, h->dt, h->pos, planes(h), h->rv, h->id, h->ctab,
-                                                                   h->bc_start, h->bc_list, h->bpos, h->rf, h->pr,
-                                                                   h->err, h->nbr, h->ncount, h->sdf, h->wall_tab,
-                                                                   cb);
+      k_density<KPT, 2><<<grid, bs, smem_cl, h->st>>>(kp, h->n, h->dt, h->pos, planes(h), h->rv, h->id, h->ctab,
+                                                     h->bc_start, h->bc_list, h->bpos, h->rf, h->pr, h->err,
+                                                     h->nbr, h->ncount, h->sdf, h->wall_tab, cb);
     else if (h->cl_mode)
-      k_density<KPT, 1><<<grid_for(h->n, bs), bs, smem, h->st>>>(kp, h->n, h->dt, h->pos, planes(h), h->rv, h->id, h->ctab,
-                                                                h->bc_start, h->bc_list, h->bpos, h->rf, h->pr,
-                                                                h->err, h->nbr, h->ncount, h->sdf, h->wall_tab, cb);
+      k_density<KPT, 1><<<grid, bs, smem, h->st>>>(kp, h->n, h->dt, h->pos, planes(h), h->rv, h->id, h->ctab,
+                                                  h->bc_start, h->bc_list, h->bpos, h->rf, h->pr, h->err,
+                                                  h->nbr, h->ncount, h->sdf, h->wall_tab, cb);
     else
-      k_density<KPT, 0><<<grid_for(h->n, bs), bs, smem, h->st>>>(kp, h->n, h->dt, h->pos, planes(h), h->rv, h->id, h->ctab,
-                                                                h->bc_start, h->bc_list, h->bpos, h->rf, h->pr,
-                                                                h->err, h->nbr, h->ncount, h->sdf, h->wall_tab, cb);
+      k_density<KPT, 0><<<grid, bs, smem, h->st>>>(kp, h->n, h->dt, h->pos, planes(h), h->rv, h->id, h->ctab,
+                                                  h->bc_start, h->bc_list, h->bpos, h->rf, h->pr, h->err,
+                                                  h->nbr, h->ncount, h->sdf, h->wall_tab, cb);
   });
   h->launches += 1;
 }

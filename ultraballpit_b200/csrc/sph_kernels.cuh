@@ -958,152 +958,152 @@ k_density(KP kp, int n, const float* __restrict__ dtp, const float4* __restrict_
   float rho_pre = 0.0f;
   if (CL != 2 && !live) return;
   if (live) {
-  const SimConst& k = kp.at(i);
-  float dt = dtp[k.inst];
-  float ssum = 0.0f, rho_wall = 0.0f;  // closure: kernel sum, wall density
-  uint32_t nwall = 0;
-  float4 pi = pos[i];
-  float rho_old_i = rv[i].x;
-  float rho = pi.w * k.norm_h3;
-  float diff_sum = 0.0f;
-  bool delta = (k.flags & kFlagDelta) != 0;
-  // Phase 1: the 27-cell scan records the in-support slots, in visit order,
-  // through this thread's column of the block's dynamic shared memory
-  // (entry j of the ring at s_stage[j * blockDim.x + threadIdx.x]).
-  extern __shared__ uint32_t s_stage[];
-  const uint32_t listed = record_neighbors(pi.x, pi.y, pi.z, i, pl, ctab, k, nbr, n, s_stage + threadIdx.x,
-                                           blockDim.x);
-  ncount[i] = listed;
-  // Phase 2: density and delta-SPH terms over the list, same order.
-  auto term_rv = [&](const float4& pj, const float2& rvj, float dx, float dy, float dz, float d2) {
-    float r = sqrtf(d2);
+    const SimConst& k = kp.at(i);
+    float dt = dtp[k.inst];
+    float ssum = 0.0f, rho_wall = 0.0f;  // closure: kernel sum, wall density
+    uint32_t nwall = 0;
+    float4 pi = pos[i];
+    float rho_old_i = rv[i].x;
+    float rho = pi.w * k.norm_h3;
+    float diff_sum = 0.0f;
+    bool delta = (k.flags & kFlagDelta) != 0;
+    // Phase 1: the 27-cell scan records the in-support slots, in visit order,
+    // through this thread's column of the block's dynamic shared memory
+    // (entry j of the ring at s_stage[j * blockDim.x + threadIdx.x]).
+    extern __shared__ uint32_t s_stage[];
+    const uint32_t listed = record_neighbors(pi.x, pi.y, pi.z, i, pl, ctab, k, nbr, n, s_stage + threadIdx.x,
+                                             blockDim.x);
+    ncount[i] = listed;
+    // Phase 2: density and delta-SPH terms over the list, same order.
+    auto term_rv = [&](const float4& pj, const float2& rvj, float dx, float dy, float dz, float d2) {
+      float r = sqrtf(d2);
+      if (delta) {
+        float gx, gy, gz;
+        grad_c2(dx, dy, dz, r, k, gx, gy, gz);
+        float r_dot_grad = dx * gx + dy * gy + dz * gz;
+        float density_diff = rho_old_i - rvj.x;
+        diff_sum += rvj.y * density_diff * 2.0f * r_dot_grad / (d2 + k.eta_sq);
+      }
+      float w = w_c2(r, k);
+      rho += pj.w * w;
+      if (CL) ssum += rvj.y * w;
+    };
+    auto term = [&](int s, const float4& pj, float dx, float dy, float dz, float d2) {
+      term_rv(pj, __ldg(&rv[s]), dx, dy, dz, d2);
+    };
+    if (listed <= kNbrCap) {
+      auto pair = [&](int s0, int s1) {  // both neighbours' gathers in flight before either term
+        float4 p0 = __ldg(&pos[s0]), p1 = __ldg(&pos[s1]);
+        float2 r0 = __ldg(&rv[s0]), r1 = __ldg(&rv[s1]);
+        float ax = pi.x - p0.x, ay = pi.y - p0.y, az = pi.z - p0.z;
+        term_rv(p0, r0, ax, ay, az, ax * ax + ay * ay + az * az);
+        float bx = pi.x - p1.x, by = pi.y - p1.y, bz = pi.z - p1.z;
+        term_rv(p1, r1, bx, by, bz, bx * bx + by * by + bz * bz);
+      };
+      // the list was written above by this thread: plain (coherent) loads
+      uint32_t c = 0;
+      for (; c + 3 < listed; c += 4) {
+        uint4 e = *reinterpret_cast<const uint4*>(nbr + nbr_index(c, n, i));
+        pair((int)e.x, (int)e.y);
+        pair((int)e.z, (int)e.w);
+      }
+      for (; c + 1 < listed; c += 2) {
+        uint2 e = *reinterpret_cast<const uint2*>(nbr + nbr_index(c, n, i));
+        pair((int)e.x, (int)e.y);
+      }
+      if (c < listed) {
+        int s = (int)nbr[nbr_index(c, n, i)];
+        float4 pj = __ldg(&pos[s]);
+        float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
+        term(s, pj, dx, dy, dz, dx * dx + dy * dy + dz * dz);
+      }
+    } else {
+      for_each_neighbor(pi.x, pi.y, pi.z, i, pos, ctab, k, term);
+    }
+    int lin = cell_hash(axis_cell(pi.x, k.gmin[0], k.cell, k.dims[0]),
+                        axis_cell(pi.y, k.gmin[1], k.cell, k.dims[1]),
+                        axis_cell(pi.z, k.gmin[2], k.cell, k.dims[2]), k);
+    uint32_t b0 = __ldg(&bc_start[k.coff + lin]), b1 = __ldg(&bc_start[k.coff + lin + 1]);
+    auto bterm = [&](const float4& bp) {
+      float dx = pi.x - bp.x, dy = pi.y - bp.y, dz = pi.z - bp.z;
+      float d2 = dx * dx + dy * dy + dz * dz;
+      if (d2 <= k.sup_d2) {
+        float wb = bp.w * w_c2(sqrtf(d2), k);
+        rho += wb;
+        if (CL) { rho_wall += wb; ++nwall; }
+      }
+    };
+    uint32_t q = b0;
+    for (; q + 1 < b1; q += 2) {  // two candidates' loads in flight, terms in order
+      uint32_t i0 = __ldg(&bc_list[q]), i1 = __ldg(&bc_list[q + 1]);
+      float4 bp0 = __ldg(&bpos[i0]), bp1 = __ldg(&bpos[i1]);
+      bterm(bp0);
+      bterm(bp1);
+    }
+    if (q < b1) bterm(__ldg(&bpos[__ldg(&bc_list[q])]));
+    bool air = (id[i] & kAirBit) != 0;
+    float wall_m = 0.0f;
+    if (k.sdf_mode) {  // kernel mass of the walls: box faces and obstacle
+      BoxFaces bf = box_faces(k, pi.x, pi.y, pi.z);
+      float dgeo = k.has_geo ? sdf_sample_clamped(sdf, k, pi.x, pi.y, pi.z) : k.support;
+      wall_m = sdf_wall_mass(k, wall_tab, bf, dgeo);
+      rho += (air ? kAirRho0 : kWaterRho0) * k.wall_scale * wall_m;
+    }
     if (delta) {
-      float gx, gy, gz;
-      grad_c2(dx, dy, dz, r, k, gx, gy, gz);
-      float r_dot_grad = dx * gx + dy * gy + dz * gz;
-      float density_diff = rho_old_i - rvj.x;
-      diff_sum += rvj.y * density_diff * 2.0f * r_dot_grad / (d2 + k.eta_sq);
+      float diffusion = k.delta_coef * diff_sum;
+      rho += diffusion * dt;
     }
-    float w = w_c2(r, k);
-    rho += pj.w * w;
-    if (CL) ssum += rvj.y * w;
-  };
-  auto term = [&](int s, const float4& pj, float dx, float dy, float dz, float d2) {
-    term_rv(pj, __ldg(&rv[s]), dx, dy, dz, d2);
-  };
-  if (listed <= kNbrCap) {
-    auto pair = [&](int s0, int s1) {  // both neighbours' gathers in flight before either term
-      float4 p0 = __ldg(&pos[s0]), p1 = __ldg(&pos[s1]);
-      float2 r0 = __ldg(&rv[s0]), r1 = __ldg(&rv[s1]);
-      float ax = pi.x - p0.x, ay = pi.y - p0.y, az = pi.z - p0.z;
-      term_rv(p0, r0, ax, ay, az, ax * ax + ay * ay + az * az);
-      float bx = pi.x - p1.x, by = pi.y - p1.y, bz = pi.z - p1.z;
-      term_rv(p1, r1, bx, by, bz, bx * bx + by * by + bz * bz);
-    };
-    // the list was written above by this thread: plain (coherent) loads
-    uint32_t c = 0;
-    for (; c + 3 < listed; c += 4) {
-      uint4 e = *reinterpret_cast<const uint4*>(nbr + nbr_index(c, n, i));
-      pair((int)e.x, (int)e.y);
-      pair((int)e.z, (int)e.w);
-    }
-    for (; c + 1 < listed; c += 2) {
-      uint2 e = *reinterpret_cast<const uint2*>(nbr + nbr_index(c, n, i));
-      pair((int)e.x, (int)e.y);
-    }
-    if (c < listed) {
-      int s = (int)nbr[nbr_index(c, n, i)];
-      float4 pj = __ldg(&pos[s]);
-      float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
-      term(s, pj, dx, dy, dz, dx * dx + dy * dy + dz * dz);
-    }
-  } else {
-    for_each_neighbor(pi.x, pi.y, pi.z, i, pos, ctab, k, term);
-  }
-  int lin = cell_hash(axis_cell(pi.x, k.gmin[0], k.cell, k.dims[0]),
-                      axis_cell(pi.y, k.gmin[1], k.cell, k.dims[1]),
-                      axis_cell(pi.z, k.gmin[2], k.cell, k.dims[2]), k);
-  uint32_t b0 = __ldg(&bc_start[k.coff + lin]), b1 = __ldg(&bc_start[k.coff + lin + 1]);
-  auto bterm = [&](const float4& bp) {
-    float dx = pi.x - bp.x, dy = pi.y - bp.y, dz = pi.z - bp.z;
-    float d2 = dx * dx + dy * dy + dz * dz;
-    if (d2 <= k.sup_d2) {
-      float wb = bp.w * w_c2(sqrtf(d2), k);
-      rho += wb;
-      if (CL) { rho_wall += wb; ++nwall; }
-    }
-  };
-  uint32_t q = b0;
-  for (; q + 1 < b1; q += 2) {  // two candidates' loads in flight, terms in order
-    uint32_t i0 = __ldg(&bc_list[q]), i1 = __ldg(&bc_list[q + 1]);
-    float4 bp0 = __ldg(&bpos[i0]), bp1 = __ldg(&bpos[i1]);
-    bterm(bp0);
-    bterm(bp1);
-  }
-  if (q < b1) bterm(__ldg(&bpos[__ldg(&bc_list[q])]));
-  bool air = (id[i] & kAirBit) != 0;
-  float wall_m = 0.0f;
-  if (k.sdf_mode) {  // kernel mass of the walls: box faces and obstacle
-    BoxFaces bf = box_faces(k, pi.x, pi.y, pi.z);
-    float dgeo = k.has_geo ? sdf_sample_clamped(sdf, k, pi.x, pi.y, pi.z) : k.support;
-    wall_m = sdf_wall_mass(k, wall_tab, bf, dgeo);
-    rho += (air ? kAirRho0 : kWaterRho0) * k.wall_scale * wall_m;
-  }
-  if (delta) {
-    float diffusion = k.delta_coef * diff_sum;
-    rho += diffusion * dt;
-  }
-  float p = tait(rho, air, k);
-  rf[i] = make_float2(rho, p / (rho * rho));
-  pr[i] = p;
-  if (CL) {
-    cb.corr[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-    // feature SDF: the given geometry SDF, or in SDF wall mode the distance
-    // to the nearest wall (box face or obstacle)
-    auto fsdf = [&](float x, float y, float z) {
-      return k.sdf_mode ? wall_distance(k, sdf, x, y, z) : sdf_sample_clamped(sdf, k, x, y, z);
-    };
-    float d = k.feat_sdf ? fsdf(pi.x, pi.y, pi.z) : k.support;
-    if (k.feat_sdf && d < k.support) {
-      // Geometry and kinematics only: the particle's own density is not a
-      // feature, so the correction cannot soften the equation of state.
-      float nx, ny, nz;
-      if (k.sdf_mode)
-        wall_normal(k, sdf, pi.x, pi.y, pi.z, nx, ny, nz);
-      else
-        sdf_gradient_clamped(sdf, k, pi.x, pi.y, pi.z, nx, ny, nz);
-      float4 v = cb.vel[i];
-      float rest = air ? kAirRho0 : kWaterRho0;
-      float gm = sqrtf(k.grav[0] * k.grav[0] + k.grav[1] * k.grav[1] + k.grav[2] * k.grav[2]);
-      // h * Laplacian of the SDF (sum of the principal curvatures) by second
-      // differences at step h; the trilinear field is piecewise linear, so a
-      // step of one SDF cell would only see its kinks.
-      float lap = fsdf(pi.x + k.h, pi.y, pi.z) + fsdf(pi.x - k.h, pi.y, pi.z) + fsdf(pi.x, pi.y + k.h, pi.z) +
-                  fsdf(pi.x, pi.y - k.h, pi.z) + fsdf(pi.x, pi.y, pi.z + k.h) + fsdf(pi.x, pi.y, pi.z - k.h) -
-                  6.0f * d;
-      f[0] = d / k.h;
-      f[1] = nx; f[2] = ny; f[3] = nz;
-      f[4] = 1.0f - (rv[i].y * k.norm_h3 + ssum);
-      f[5] = (float)listed / 73.0f;
-      f[6] = sqrtf(v.x * v.x + v.y * v.y + v.z * v.z) / k.c;
-      f[7] = dt * k.c / k.h;
-      f[8] = fminf(fmaxf(lap / k.h, -4.0f), 4.0f);
-      f[9] = k.sdf_mode ? k.wall_scale * wall_m : rho_wall / rest;
-      f[10] = gm > 0.0f ? (k.grav[0] * nx + k.grav[1] * ny + k.grav[2] * nz) / gm : 0.0f;
-      f[11] = f[0] * f[0];
-      f[12] = f[8] * f[0];
-      f[13] = f[10] * f[0];
-      f[14] = (float)nwall / 30.0f;
-      f[15] = 1.0f;
-      uint32_t q = atomicAdd(cb.count, 1u);
-      cb.slot[q] = (uint32_t)i;
-      cb.rho[q] = rho;
+    float p = tait(rho, air, k);
+    rf[i] = make_float2(rho, p / (rho * rho));
+    pr[i] = p;
+    if (CL) {
+      cb.corr[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+      // feature SDF: the given geometry SDF, or in SDF wall mode the distance
+      // to the nearest wall (box face or obstacle)
+      auto fsdf = [&](float x, float y, float z) {
+        return k.sdf_mode ? wall_distance(k, sdf, x, y, z) : sdf_sample_clamped(sdf, k, x, y, z);
+      };
+      float d = k.feat_sdf ? fsdf(pi.x, pi.y, pi.z) : k.support;
+      if (k.feat_sdf && d < k.support) {
+        // Geometry and kinematics only: the particle's own density is not a
+        // feature, so the correction cannot soften the equation of state.
+        float nx, ny, nz;
+        if (k.sdf_mode)
+          wall_normal(k, sdf, pi.x, pi.y, pi.z, nx, ny, nz);
+        else
+          sdf_gradient_clamped(sdf, k, pi.x, pi.y, pi.z, nx, ny, nz);
+        float4 v = cb.vel[i];
+        float rest = air ? kAirRho0 : kWaterRho0;
+        float gm = sqrtf(k.grav[0] * k.grav[0] + k.grav[1] * k.grav[1] + k.grav[2] * k.grav[2]);
+        // h * Laplacian of the SDF (sum of the principal curvatures) by second
+        // differences at step h; the trilinear field is piecewise linear, so a
+        // step of one SDF cell would only see its kinks.
+        float lap = fsdf(pi.x + k.h, pi.y, pi.z) + fsdf(pi.x - k.h, pi.y, pi.z) + fsdf(pi.x, pi.y + k.h, pi.z) +
+                    fsdf(pi.x, pi.y - k.h, pi.z) + fsdf(pi.x, pi.y, pi.z + k.h) + fsdf(pi.x, pi.y, pi.z - k.h) -
+                    6.0f * d;
+        f[0] = d / k.h;
+        f[1] = nx; f[2] = ny; f[3] = nz;
+        f[4] = 1.0f - (rv[i].y * k.norm_h3 + ssum);
+        f[5] = (float)listed / 73.0f;
+        f[6] = sqrtf(v.x * v.x + v.y * v.y + v.z * v.z) / k.c;
+        f[7] = dt * k.c / k.h;
+        f[8] = fminf(fmaxf(lap / k.h, -4.0f), 4.0f);
+        f[9] = k.sdf_mode ? k.wall_scale * wall_m : rho_wall / rest;
+        f[10] = gm > 0.0f ? (k.grav[0] * nx + k.grav[1] * ny + k.grav[2] * nz) / gm : 0.0f;
+        f[11] = f[0] * f[0];
+        f[12] = f[8] * f[0];
+        f[13] = f[10] * f[0];
+        f[14] = (float)nwall / 30.0f;
+        f[15] = 1.0f;
+        uint32_t q = atomicAdd(cb.count, 1u);
+        cb.slot[q] = (uint32_t)i;
+        cb.rho[q] = rho;
 #pragma unroll
-      for (int a = 0; a < 16; ++a) cb.feat[(size_t)q * 16 + a] = f[a];
-      near_wall = true;
-      rho_pre = rho;
+        for (int a = 0; a < 16; ++a) cb.feat[(size_t)q * 16 + a] = f[a];
+        near_wall = true;
+        rho_pre = rho;
+      }
     }
-  }
   }  // live
   if (CL == 2) {
     // network epilogue: up to 16 of the warp's near-wall particles per tile
