@@ -4,7 +4,9 @@
 // buffers and CUDA graphs. The step body (9 kernels) is captured once into a
 // graph and replayed; dt lives in device memory so the graph never changes.
 #include <algorithm>
+#include <chrono>
 #include <cmath>
+#include <cstdlib>
 #include <cstdio>
 #include <cstring>
 #include <map>
@@ -735,6 +737,23 @@ int check_views(const SphParams& P, const SphParticlesView* pv, const SphBoundar
 // instance keeps its own grid, constants, boundary lists and dt; instances
 // occupy disjoint ranges of the global cell ranks, so the global counting
 // sort keeps every instance in a fixed contiguous slot range.
+// Phase times of a host-side call on stderr when the environment sets
+// SPH_TRACE (the creation's host tables, packing, allocation, uploads).
+struct PhaseTrace {
+  const char* what;
+  bool on = std::getenv("SPH_TRACE") != nullptr;
+  std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now(), last = t0;
+  explicit PhaseTrace(const char* w) : what(w) {}
+  void mark(const char* phase) {
+    if (!on) return;
+    auto now = std::chrono::steady_clock::now();
+    fprintf(stderr, "%s: %-24s %8.2f ms (total %8.2f ms)\n", what, phase,
+            std::chrono::duration<double, std::milli>(now - last).count(),
+            std::chrono::duration<double, std::milli>(now - t0).count());
+    last = now;
+  }
+};
+
 int create_impl(int ninst, const SphParams* PP, const SphParticlesView* pvs,
                 const SphBoundaryView* const* bvs, const SphSdfView* sdfs, SphHandle** out) {
   if (!out) return SPH_ERR_INVALID_ARG;
@@ -786,6 +805,7 @@ int create_impl(int ninst, const SphParams* PP, const SphParticlesView* pvs,
     return SPH_ERR_NO_DEVICE;
   }
 
+  PhaseTrace trace("sph_create");
   SphHandle* h = new (std::nothrow) SphHandle();
   if (!h) return SPH_ERR_OOM;
   h->prm = P0;
@@ -957,6 +977,7 @@ int create_impl(int ninst, const SphParams* PP, const SphParticlesView* pvs,
     h->init_e[q] = e;
     C += Cq;
   }
+  trace.mark("cell ranks, lists, totals");
   h->k = h->ktab_h[0];
   h->C = (int)C;
   h->boundary_candidates = blist.size();
@@ -1010,7 +1031,9 @@ int create_impl(int ninst, const SphParams* PP, const SphParticlesView* pvs,
       if (ninst > 1) hib[bo + i] = (uint16_t)q;
     }
   }
+  trace.mark("staging packed");
   allocator.join();
+  trace.mark("allocation joined");
   cudaError_t e = ae;
   if (e == cudaSuccess) e = dalloc(h, &h->bc_list, blist.size());
   if (e == cudaSuccess) e = dalloc(h, &h->bc_cells, bcells.size());
@@ -1046,6 +1069,7 @@ int create_impl(int ninst, const SphParams* PP, const SphParticlesView* pvs,
     if (sdf_off[q + 1] > sdf_off[q])
       up(h->sdf + sdf_off[q], sdfs[q].distances, (sdf_off[q + 1] - sdf_off[q]) * sizeof(float));
   if (sdf_mode) up(h->wall_tab, wall_host.data(), wall_host.size() * sizeof(float2));
+  trace.mark("uploads issued");
   if (e == cudaSuccess) e = cudaMemsetAsync(h->hist, 0, C * sizeof(uint32_t), h->st);
   if (e == cudaSuccess) e = cudaMemsetAsync(h->bpress, 0, std::max<size_t>(1, nb) * sizeof(float), h->st);
   if (e == cudaSuccess) e = cudaMemsetAsync(h->err, 0, sizeof(uint32_t), h->st);
@@ -1066,6 +1090,7 @@ int create_impl(int ninst, const SphParams* PP, const SphParticlesView* pvs,
     e = cudaGetLastError();
   }
   if (e == cudaSuccess) e = cudaStreamSynchronize(h->st);
+  trace.mark("sort and sync");
   if (accU) cudaFree(accU);
   if (prU) cudaFree(prU);
   if (e != cudaSuccess) {
@@ -1075,6 +1100,7 @@ int create_impl(int ninst, const SphParams* PP, const SphParticlesView* pvs,
   ensure_red(h);
   int st = check_device_flags(h);
   if (st != SPH_OK) return fail(st);
+  trace.mark("done");
   *out = h;
   return SPH_OK;
 }
