@@ -490,16 +490,21 @@ void build_boundary_lists(const SimConst& k, const SphBoundaryView* b, int C,
     std::lock_guard<std::mutex> lock(mu);
     used = std::max(used, t + 1);
   });
-  // per-thread counts, then per-thread write offsets within each cell
-  std::vector<std::vector<uint32_t>> at(used, std::vector<uint32_t>((size_t)C, 0u));
+  // per-thread counts (each thread zeroes and fills its own array), per-cell
+  // totals in parallel, one scan, then per-thread write offsets within each cell
+  std::vector<std::vector<uint32_t>> at(used);
   run_threads(used, [&](unsigned t) {
+    at[t].assign((size_t)C, 0u);
     for (uint64_t pr : pairs[t]) at[t][pr >> 32]++;
   });
-  for (int c = 0; c < C; ++c) {
-    uint32_t run = 0;
-    for (unsigned t = 0; t < used; ++t) run += at[t][c];
-    start[(size_t)c + 1] = start[c] + run;
-  }
+  parallel_chunks((size_t)C, kHostThreads, [&](unsigned, size_t c0, size_t c1) {
+    for (size_t c = c0; c < c1; ++c) {
+      uint32_t run = 0;
+      for (unsigned t = 0; t < used; ++t) run += at[t][c];
+      start[c + 1] = run;
+    }
+  });
+  for (int c = 0; c < C; ++c) start[(size_t)c + 1] += start[c];
   list.resize(start[C]);
   parallel_chunks((size_t)C, kHostThreads, [&](unsigned, size_t c0, size_t c1) {
     for (size_t c = c0; c < c1; ++c) {
@@ -884,6 +889,107 @@ int create_impl(int ninst, const SphParams* PP, const SphParticlesView* pvs,
   } catch (...) {  // no thread to be had: allocate here, before the host tables
     allocate_all();
   }
+  for (int q = 0; q < ninst; ++q) {
+    const SphBoundaryView* bv = (sdf_mode || !bvs) ? nullptr : bvs[q];
+    h->poff[q + 1] = h->poff[q] + pvs[q].n;
+    h->boff[q + 1] = h->boff[q] + (bv ? bv->n : 0);
+  }
+  // upload staging (particles of instance q at [poff[q], poff[q+1]), ids
+  // global), left uninitialised: every entry is written below, by host
+  // threads that also take the first-touch page faults, while the device
+  // arrays are being allocated
+  std::unique_ptr<float4[]> hpos(new float4[n]), hvel(new float4[n]), hacc(new float4[n]), hb(new float4[nb]);
+  std::unique_ptr<uint32_t[]> hid(new uint32_t[n]);
+  std::unique_ptr<float[]> hpr(new float[n]);
+  std::vector<uint16_t> hip(ninst > 1 ? n : 0), hib(ninst > 1 ? nb : 0);
+  h->temperature.resize(n);
+  for (int q = 0; q < ninst; ++q) {
+    const SphParticlesView* pv = &pvs[q];
+    size_t o = h->poff[q];
+    parallel_chunks(pv->n, kHostThreads, [&](unsigned, size_t i0, size_t i1) {
+      for (size_t i = i0; i < i1; ++i) {
+        hpos[o + i] = make_float4(pv->x[i], pv->y[i], pv->z[i], pv->mass[i]);
+        hvel[o + i] = make_float4(pv->vx[i], pv->vy[i], pv->vz[i], pv->density[i]);
+        hacc[o + i] = make_float4(pv->ax[i], pv->ay[i], pv->az[i], 0.0f);
+        hid[o + i] = (uint32_t)(o + i) | (pv->fluid_type[i] ? sph::kAirBit : 0u);
+        hpr[o + i] = pv->pressure[i];
+        h->temperature[o + i] = pv->temperature[i];
+        if (ninst > 1) hip[o + i] = (uint16_t)q;
+      }
+    });
+    const SphBoundaryView* bv = (sdf_mode || !bvs) ? nullptr : bvs[q];
+    size_t bo = h->boff[q];
+    for (size_t i = 0; bv && i < bv->n; ++i) {
+      hb[bo + i] = make_float4(bv->x[i], bv->y[i], bv->z[i], bv->mass[i]);
+      if (ninst > 1) hib[bo + i] = (uint16_t)q;
+    }
+  }
+  trace.mark("staging packed");
+  allocator.join();
+  trace.mark("allocation joined");
+  cudaError_t e = ae;
+  if (e != cudaSuccess) return fail(e == cudaErrorMemoryAllocation ? SPH_ERR_OOM : SPH_ERR_CUDA);
+  float4* accU = nullptr;
+  float* prU = nullptr;
+  if (e == cudaSuccess) e = cudaMalloc(&accU, std::max<size_t>(1, n) * sizeof(float4));
+  if (e == cudaSuccess) e = cudaMalloc(&prU, std::max<size_t>(1, n) * sizeof(float));
+  if (e != cudaSuccess) {
+    if (accU) cudaFree(accU);
+    return fail(SPH_ERR_OOM);
+  }
+  // the particle uploads (pageable copies hold the issuing thread) run on a
+  // thread of their own while this one builds the cell tables
+  cudaError_t ue = cudaSuccess;
+  auto upload_particles = [&] {
+    auto upq = [&](void* d, const void* src, size_t bytes) {
+      if (ue == cudaSuccess && bytes) ue = cudaMemcpyAsync(d, src, bytes, cudaMemcpyHostToDevice, h->st);
+    };
+    if (cudaSetDevice(h->dev) != cudaSuccess) {
+      ue = cudaErrorInvalidDevice;
+      return;
+    }
+    upq(h->posU, hpos.get(), n * sizeof(float4));
+    upq(h->velU, hvel.get(), n * sizeof(float4));
+    upq(accU, hacc.get(), n * sizeof(float4));
+    upq(prU, hpr.get(), n * sizeof(float));
+    upq(h->idU, hid.get(), n * sizeof(uint32_t));
+    upq(h->bpos, hb.get(), nb * sizeof(float4));
+    if (ninst > 1) {
+      upq(h->inst_p, hip.data(), n * sizeof(uint16_t));
+      upq(h->inst_b, hib.data(), nb * sizeof(uint16_t));
+    }
+  };
+  std::thread uploader;
+  try {
+    uploader = std::thread(upload_particles);
+  } catch (...) {  // no thread to be had: upload here, before the tables
+    upload_particles();
+  }
+  // initial conservation totals, in the reference's order (lib.rs:152-156),
+  // on a thread of their own while this one builds the tables
+  auto initial_totals = [&] {
+    for (int q = 0; q < ninst; ++q) {
+      const SphParticlesView* pv = &pvs[q];
+      const SphParams& P = PP[q];
+      double m = 0.0, e = 0.0;
+      for (size_t i = 0; i < pv->n; ++i) {  // two sums, each in index order
+        double mi = (double)pv->mass[i];
+        m += mi;
+        double vx = pv->vx[i], vy = pv->vy[i], vz = pv->vz[i];
+        e += 0.5 * mi * (vx * vx + vy * vy + vz * vz);
+        double x = pv->x[i], y = pv->y[i], z = pv->z[i];
+        e -= mi * ((double)P.gravity[0] * x + (double)P.gravity[1] * y + (double)P.gravity[2] * z);
+      }
+      h->init_m[q] = m;
+      h->init_e[q] = e;
+    }
+  };
+  std::thread totals;
+  try {
+    totals = std::thread(initial_totals);
+  } catch (...) {  // no thread to be had: compute them here
+    initial_totals();
+  }
   uint64_t C = 0;
   bstart.push_back(0);
   for (int q = 0; q < ninst; ++q) {
@@ -961,22 +1067,9 @@ int create_impl(int ninst, const SphParams* PP, const SphParticlesView* pvs,
       blist.reserve(blist.size() + l1.size());
       for (uint32_t b : l1) blist.push_back(bbase + b);
     }
-    h->poff[q + 1] = h->poff[q] + pv->n;
-    h->boff[q + 1] = h->boff[q] + (bv ? bv->n : 0);
-    // initial conservation totals, in the reference's order (lib.rs:152-156)
-    double m = 0.0, e = 0.0;
-    for (size_t i = 0; i < pv->n; ++i) {  // two sums, each in index order
-      double mi = (double)pv->mass[i];
-      m += mi;
-      double vx = pv->vx[i], vy = pv->vy[i], vz = pv->vz[i];
-      e += 0.5 * mi * (vx * vx + vy * vy + vz * vz);
-      double x = pv->x[i], y = pv->y[i], z = pv->z[i];
-      e -= mi * ((double)P.gravity[0] * x + (double)P.gravity[1] * y + (double)P.gravity[2] * z);
-    }
-    h->init_m[q] = m;
-    h->init_e[q] = e;
     C += Cq;
   }
+  if (totals.joinable()) totals.join();
   trace.mark("cell ranks, lists, totals");
   h->k = h->ktab_h[0];
   h->C = (int)C;
@@ -1001,70 +1094,28 @@ int create_impl(int ninst, const SphParams* PP, const SphParticlesView* pvs,
   }
   h->k = h->ktab_h[0];
 
-  // upload staging (particles of instance q at [poff[q], poff[q+1]), ids
-  // global), left uninitialised: every entry is written below, by host
-  // threads that also take the first-touch page faults, while the device
-  // arrays are being allocated
-  std::unique_ptr<float4[]> hpos(new float4[n]), hvel(new float4[n]), hacc(new float4[n]), hb(new float4[nb]);
-  std::unique_ptr<uint32_t[]> hid(new uint32_t[n]);
-  std::unique_ptr<float[]> hpr(new float[n]);
-  std::vector<uint16_t> hip(ninst > 1 ? n : 0), hib(ninst > 1 ? nb : 0);
-  h->temperature.resize(n);
-  for (int q = 0; q < ninst; ++q) {
-    const SphParticlesView* pv = &pvs[q];
-    size_t o = h->poff[q];
-    parallel_chunks(pv->n, kHostThreads, [&](unsigned, size_t i0, size_t i1) {
-      for (size_t i = i0; i < i1; ++i) {
-        hpos[o + i] = make_float4(pv->x[i], pv->y[i], pv->z[i], pv->mass[i]);
-        hvel[o + i] = make_float4(pv->vx[i], pv->vy[i], pv->vz[i], pv->density[i]);
-        hacc[o + i] = make_float4(pv->ax[i], pv->ay[i], pv->az[i], 0.0f);
-        hid[o + i] = (uint32_t)(o + i) | (pv->fluid_type[i] ? sph::kAirBit : 0u);
-        hpr[o + i] = pv->pressure[i];
-        h->temperature[o + i] = pv->temperature[i];
-        if (ninst > 1) hip[o + i] = (uint16_t)q;
-      }
-    });
-    const SphBoundaryView* bv = (sdf_mode || !bvs) ? nullptr : bvs[q];
-    size_t bo = h->boff[q];
-    for (size_t i = 0; bv && i < bv->n; ++i) {
-      hb[bo + i] = make_float4(bv->x[i], bv->y[i], bv->z[i], bv->mass[i]);
-      if (ninst > 1) hib[bo + i] = (uint16_t)q;
-    }
-  }
-  trace.mark("staging packed");
-  allocator.join();
-  trace.mark("allocation joined");
-  cudaError_t e = ae;
+  if (uploader.joinable()) uploader.join();
+  trace.mark("particle uploads joined");
+  if (e == cudaSuccess) e = ue;
   if (e == cudaSuccess) e = dalloc(h, &h->bc_list, blist.size());
   if (e == cudaSuccess) e = dalloc(h, &h->bc_cells, bcells.size());
   h->nbc_cells = (int)bcells.size();
   if (e == cudaSuccess && sdf_mode) e = dalloc(h, &h->wall_tab, wall_host.size());
-  if (e != cudaSuccess) return fail(e == cudaErrorMemoryAllocation ? SPH_ERR_OOM : SPH_ERR_CUDA);
-
-  float4* accU = nullptr;
-  float* prU = nullptr;
+  if (e != cudaSuccess) {
+    cudaFree(accU);
+    cudaFree(prU);
+    return fail(e == cudaErrorMemoryAllocation ? SPH_ERR_OOM : SPH_ERR_CUDA);
+  }
   auto up = [&](void* d, const void* src, size_t bytes) {
     if (e == cudaSuccess && bytes) e = cudaMemcpyAsync(d, src, bytes, cudaMemcpyHostToDevice, h->st);
   };
-  if (e == cudaSuccess) e = cudaMalloc(&accU, std::max<size_t>(1, n) * sizeof(float4));
-  if (e == cudaSuccess) e = cudaMalloc(&prU, std::max<size_t>(1, n) * sizeof(float));
-  up(h->posU, hpos.get(), n * sizeof(float4));
-  up(h->velU, hvel.get(), n * sizeof(float4));
-  up(accU, hacc.get(), n * sizeof(float4));
-  up(prU, hpr.get(), n * sizeof(float));
-  up(h->idU, hid.get(), n * sizeof(uint32_t));
-  up(h->bpos, hb.get(), nb * sizeof(float4));
   up(h->rank_of_lin, rank_of_lin.data(), C * sizeof(uint32_t));
   up(h->lin_of_rank, lin_of_rank.data(), C * sizeof(uint32_t));
   up(h->bc_start, bstart.data(), (C + 1) * sizeof(uint32_t));
   up(h->bc_list, blist.data(), blist.size() * sizeof(uint32_t));
   up(h->bc_cells, bcells.data(), bcells.size() * sizeof(uint32_t));
   up(h->hcc, hcc.data(), ninst * sizeof(float4));
-  if (ninst > 1) {
-    up(h->ktab, h->ktab_h.data(), ninst * sizeof(SimConst));
-    up(h->inst_p, hip.data(), n * sizeof(uint16_t));
-    up(h->inst_b, hib.data(), nb * sizeof(uint16_t));
-  }
+  if (ninst > 1) up(h->ktab, h->ktab_h.data(), ninst * sizeof(SimConst));
   for (int q = 0; sdf_mode && q < ninst; ++q)
     if (sdf_off[q + 1] > sdf_off[q])
       up(h->sdf + sdf_off[q], sdfs[q].distances, (sdf_off[q + 1] - sdf_off[q]) * sizeof(float));
