@@ -87,12 +87,13 @@ KERNEL_SOURCES = ["ultraballpit_b200/csrc/sph_kernels.cuh", "ultraballpit_b200/c
 
 
 def kernel_sources_digest() -> str:
-    """sha1 over the step's kernel sources and the default launch shapes: an
-    ncu figure recorded with the same digest was captured on these kernels."""
+    """sha1 over the step's kernel sources (whitespace removed, so a change of
+    layout alone keeps it) and the default launch shapes: an ncu figure
+    recorded with the same digest was captured on these kernels."""
     import hashlib
     h = hashlib.sha1()
     for f in KERNEL_SOURCES:
-        h.update(open(os.path.join(ROOT, f), "rb").read())
+        h.update(re.sub(rb"\s+", b"", open(os.path.join(ROOT, f), "rb").read()))
     api = open(os.path.join(ROOT, "ultraballpit_b200", "csrc", "sph_api.cu")).read()
     h.update(re.search(r"int bs_xsph = \d+, bs_density = \d+, bs_forces = \d+;", api).group(0).encode())
     return h.hexdigest()
