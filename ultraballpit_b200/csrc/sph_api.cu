@@ -80,7 +80,7 @@ struct SphHandle {
   uint32_t *rank_of_lin = nullptr, *lin_of_rank = nullptr;
   uint2* ctab = nullptr;
   int nbsum = 0;
-  // neighbour lists recorded by k_density (chunked, sph::nbr_index), count per particle
+  // neighbour lists recorded by k_density (entry-major, sph::nbr_index), count per particle
   uint32_t *nbr = nullptr, *ncount = nullptr;
   // XSPH gather records: (x, y, z, m), (v + a dt/2, rho) per particle
   float4* xrec = nullptr;
@@ -532,6 +532,22 @@ void dispatch(SphHandle* h, bool boundary, F&& f) {
 
 sph::Planes planes(SphHandle* h) { return sph::Planes{h->xyz, h->xyz_stride}; }
 
+// Lets the density kernels take up to 128 KiB of dynamic shared memory (the
+// warp scan's per-warp scratch passes the default 48 KiB at 512 threads) on
+// the current device. Set at handle creation, before any graph capture.
+void allow_density_smem() {
+  using namespace sph;
+  auto set = [](const void* f) {
+    cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, 128 * 1024);
+  };
+  set(reinterpret_cast<const void*>(k_density<OneSim, 0>));
+  set(reinterpret_cast<const void*>(k_density<OneSim, 1>));
+  set(reinterpret_cast<const void*>(k_density<OneSim, 2>));
+  set(reinterpret_cast<const void*>(k_density<ManySim, 0>));
+  set(reinterpret_cast<const void*>(k_density<ManySim, 1>));
+  set(reinterpret_cast<const void*>(k_density<ManySim, 2>));
+}
+
 // Sorting scratch + binning of posU into the cell tables (k_bin or the
 // xsph kernel fill `hist` first).
 void enqueue_scan_fill(SphHandle* h) {
@@ -550,8 +566,9 @@ void enqueue_density_only(SphHandle* h) {
   int bs = h->bs_density;
   sph::ClosureBufs cb{h->cl_count, h->cl_slot, h->cl_feat, h->cl_rho, h->corr, h->vel, h->cl_wb, h->cl_wf};
   if (h->cl_mode) cudaMemsetAsync(h->cl_count, 0, sizeof(uint32_t), h->st);
-  const size_t smem = bs * kStageRing * sizeof(uint32_t);
-  // closure mode 2 adds a 16-sample network tile per warp (the fused inference)
+  // the warp scan's scratch per warp; closure mode 2 adds a 16-sample network
+  // tile per warp (the fused inference)
+  const size_t smem = (bs / 32) * sizeof(ScanWarp);
   const size_t smem_cl = smem + (bs / 32) * kClTileWords * sizeof(uint32_t);
   dispatch(h, false, [&](auto kp) {
     using KPT = decltype(kp);
@@ -863,6 +880,7 @@ int create_impl(int ninst, const SphParams* PP, const SphParticlesView* pvs,
       return;
     }
     ae = cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking);
+    allow_density_smem();
 #define ALLOC(ptr, cnt) \
   if (ae == cudaSuccess) ae = dalloc(h, &h->ptr, (cnt))
     ALLOC(pos, n); ALLOC(vel, n); ALLOC(velout, n); ALLOC(acc, n);

@@ -17,6 +17,7 @@
 //   vel    (v after kick 1, -)    acc    (a, 0)
 //   rv     (rho_old, m/rho_old)   rf     (rho_new, p/rho_new^2)
 #pragma once
+#include <cstddef>
 #include <cstdint>
 #include <cuda_runtime.h>
 
@@ -33,16 +34,14 @@ constexpr float kAirRho0 = 1.204f;     // eos.rs:10
 constexpr int kAdamiCap = 256;         // fluid terms per boundary particle
 constexpr int kCellCap = 4096;         // particles per cell for the id ranking
 constexpr uint32_t kNbrCap = 128;      // listed neighbours per particle
-constexpr uint32_t kNbrChunk = 8;      // list entries per 32-byte chunk
-constexpr uint32_t kStageRing = 16;    // staged list entries per thread (two chunks)
 // The neighbour kernels are latency-bound on gathered loads, so occupancy
-// pays more than registers: k_density is capped at 48 registers, k_forces
-// and k_xsph_drift (whose replays put two neighbours' gathers in flight
-// before using them) at 56 (__maxnreg__ below; each measured at 2M particles
-// against caps from 40 to 72 and the compiler's choice, same results).
+// pays more than registers: k_forces and k_xsph_drift (whose replays put two
+// neighbours' gathers in flight before using them) are capped at 56
+// registers, k_density (whose warp scan holds its shared scratch per warp) at
+// SPH_MAXNREG_DENSITY (__maxnreg__ below; each measured at 2M particles).
 
 #ifndef SPH_MAXNREG_DENSITY
-#define SPH_MAXNREG_DENSITY 40
+#define SPH_MAXNREG_DENSITY 56
 #endif
 #ifndef SPH_MAXNREG_FORCES
 #define SPH_MAXNREG_FORCES 56
@@ -474,18 +473,36 @@ struct Planes {
   size_t stride;
 };
 
-// The density pass's recording scan over the SoA planes: the candidates of a
-// range are taken in aligned groups of four (lanes outside [s, e) masked),
-// each group's distances in two f32x2 pairs rounded exactly as the scalar
-// expression, and the in-support slots appended in visit order to a 16-entry
-// ring of this thread's shared-memory column; every full chunk of 8 goes out
-// as one 32-byte store (entry c of slot i at nbr_index(c, n, i); at most
-// kNbrCap entries are stored, the count is returned in full). The cells and
-// rows visited, and the order, are scan_support's.
-__device__ __forceinline__ uint32_t record_neighbors(float px, float py, float pz, int self, Planes pl,
-                                                     const uint2* __restrict__ ctab, const SimConst& k,
-                                                     uint32_t* __restrict__ nbr, int n, uint32_t* stage,
-                                                     unsigned bsz) {
+// Neighbour lists are entry-major: entry c of slot i at nbr[c n + i]. The
+// warp-cooperative scan below emits one entry per lane per step, so the
+// lanes' stores of one step fill whole lines, and the replays read entry c of
+// 32 consecutive slots with one coalesced load.
+__device__ __forceinline__ size_t nbr_index(uint32_t c, int n, int i) {
+  return (size_t)c * (size_t)n + (size_t)i;
+}
+
+// The per-thread form of the density pass's scan over the SoA planes, for a
+// cell whose 27-cell neighbourhood holds more candidates than the warp scan's
+// masks cover: the candidates of a range are taken in aligned groups of four
+// (lanes outside [s, e) masked), each group's distances in two f32x2 pairs
+// rounded exactly as the scalar expression, and the in-support slots stored
+// in visit order (at most kNbrCap; the count is returned in full). The cells,
+// rows and order visited are for_each_neighbor's.
+// The grid constants record_neighbors reads (passed by value: a reference to
+// a single simulation's constants would move them from the parameter space
+// to the stack of every thread).
+struct ScanGeo {
+  float gmin[3];
+  float cell, radius_sq;
+  int dims[3];
+  int coff, rows;
+  __device__ __forceinline__ explicit ScanGeo(const SimConst& k)
+      : gmin{k.gmin[0], k.gmin[1], k.gmin[2]}, cell(k.cell), radius_sq(k.radius_sq),
+        dims{k.dims[0], k.dims[1], k.dims[2]}, coff(k.coff), rows(k.rows) {}
+};
+__device__ __noinline__ uint32_t record_neighbors(float px, float py, float pz, int self, Planes pl,
+                                                  const uint2* __restrict__ ctab, const ScanGeo k,
+                                                  uint32_t* __restrict__ nbr, int n) {
   int cx = axis_cell(px, k.gmin[0], k.cell, k.dims[0]);
   int cy = axis_cell(py, k.gmin[1], k.cell, k.dims[1]);
   int cz = axis_cell(pz, k.gmin[2], k.cell, k.dims[2]);
@@ -508,14 +525,12 @@ __device__ __forceinline__ uint32_t record_neighbors(float px, float py, float p
   const float* zs = pl.xyz + 2 * pl.stride;
   const unsigned long long X = f2_pack(px, px), Y = f2_pack(py, py), Z = f2_pack(pz, pz);
   const float r2 = k.radius_sq;
-  uint32_t listed = 0, flushed = 0;
-  auto flush = [&](uint32_t m) {  // the ring's chunk at `flushed`, m entries valid
-    const uint32_t* r = stage + (flushed & (kStageRing - 1u)) * bsz;
-    uint4* dst = reinterpret_cast<uint4*>(nbr + ((size_t)(flushed / kNbrChunk) * (size_t)n + (size_t)self) *
-                                          kNbrChunk);
-    dst[0] = make_uint4(r[0], m > 1 ? r[bsz] : 0u, m > 2 ? r[2 * bsz] : 0u, m > 3 ? r[3 * bsz] : 0u);
-    dst[1] = make_uint4(m > 4 ? r[4 * bsz] : 0u, m > 5 ? r[5 * bsz] : 0u, m > 6 ? r[6 * bsz] : 0u,
-                        m > 7 ? r[7 * bsz] : 0u);
+  uint32_t listed = 0;
+  auto put = [&](bool ok, int slot) {
+    if (ok) {
+      if (listed < kNbrCap) nbr[nbr_index(listed, n, self)] = (uint32_t)slot;
+      ++listed;
+    }
   };
   auto range = [&](int s, int e) {
     for (int g = s & ~3; g < e; g += 4) {
@@ -529,24 +544,10 @@ __device__ __forceinline__ uint32_t record_neighbors(float px, float py, float p
       f2_unpack(f2_add(f2_add(f2_mul(dx01, dx01), f2_mul(dy01, dy01)), f2_mul(dz01, dz01)), d0, d1);
       f2_unpack(f2_add(f2_add(f2_mul(dx23, dx23), f2_mul(dy23, dy23)), f2_mul(dz23, dz23)), d2, d3);
       const int lo = s - g, hi = e - g;
-      const bool ok0 = d0 <= r2 && 0 >= lo && 0 < hi;
-      const bool ok1 = d1 <= r2 && 1 >= lo && 1 < hi;
-      const bool ok2 = d2 <= r2 && 2 >= lo && 2 < hi;
-      const bool ok3 = d3 <= r2 && 3 >= lo && 3 < hi;
-      // each slot is written at the ring's next entry and kept only if the
-      // entry advances
-      stage[(listed & (kStageRing - 1u)) * bsz] = (uint32_t)g;
-      listed += ok0 ? 1u : 0u;
-      stage[(listed & (kStageRing - 1u)) * bsz] = (uint32_t)(g + 1);
-      listed += ok1 ? 1u : 0u;
-      stage[(listed & (kStageRing - 1u)) * bsz] = (uint32_t)(g + 2);
-      listed += ok2 ? 1u : 0u;
-      stage[(listed & (kStageRing - 1u)) * bsz] = (uint32_t)(g + 3);
-      listed += ok3 ? 1u : 0u;
-      if (listed - flushed >= kNbrChunk) {  // a group adds at most 4: one chunk at a time
-        if (flushed + kNbrChunk <= kNbrCap) flush(kNbrChunk);
-        flushed += kNbrChunk;
-      }
+      put(d0 <= r2 && 0 >= lo && 0 < hi, g);
+      put(d1 <= r2 && 1 >= lo && 1 < hi, g + 1);
+      put(d2 <= r2 && 2 >= lo && 2 < hi, g + 2);
+      put(d3 <= r2 && 3 >= lo && 3 < hi, g + 3);
     }
   };
   for (int dz = -1; dz <= 1; ++dz) {
@@ -585,22 +586,219 @@ __device__ __forceinline__ uint32_t record_neighbors(float px, float py, float p
       }
     }
   }
-  if (listed > flushed && flushed + kNbrChunk <= kNbrCap) flush(listed - flushed);  // the open chunk
   return listed;
 }
 
-// Neighbour lists: entry c of slot i lies in chunk c / 8 of the slot, and the
-// chunks of consecutive slots lie side by side: nbr[((c / 8) n + i) 8 + c % 8].
-// k_density writes each chunk as one whole 32-byte sector (its entries are
-// staged in shared memory); entry-by-entry stores across a warp scatter into
-// partial sectors and cost more than the 27-cell scan itself. The replays read
-// two entries at a time.
-__device__ __forceinline__ size_t nbr_index(uint32_t c, int n, int i) {
-  return ((size_t)(c / kNbrChunk) * (size_t)n + (size_t)i) * kNbrChunk + (c % kNbrChunk);
-}
-// entries c and c + 1 of slot i, c even (one 8-byte load)
-__device__ __forceinline__ uint2 nbr_pair(const uint32_t* __restrict__ nbr, uint32_t c, int n, int i) {
-  return __ldg(reinterpret_cast<const uint2*>(nbr + nbr_index(c, n, i)));
+// Warp-cooperative neighbour scan of the density pass. The particles of one
+// cell share one candidate sequence: its 27-cell neighbourhood as 9 x-row
+// ranges (row cell order, where a row's cells are consecutive) or 27 cell
+// ranges, concatenated in the reference's visit order (dz, dy, dx, then slot,
+// i.e. ascending id within a cell). A warp takes its 32 slots cell by cell (a
+// "segment" is the run of its slots in one cell): the lanes load 32
+// consecutive candidates of the sequence at once, and for four of the
+// segment's particles at a time every lane computes its candidate's squared
+// distance to each (two f32x2 chains, rounded as the scalar expression); a
+// ballot per particle gives that particle's 32-bit in-support mask for the
+// word, which the particle's own lane keeps. The particle's own slot is
+// cleared from its masks, and each lane then turns its masks into its list,
+// one entry per step, so that every active lane stores entry c at the same
+// step (entry-major: the stores of a step coalesce). The list and its order
+// equal for_each_neighbor's: a candidate outside support sets no bit, and the
+// sequence visits the neighbourhood's cells in the reference's order.
+constexpr int kScanWords = 24;   // mask words per particle: up to 768 candidates per neighbourhood
+constexpr int kScanSegs = 4;     // segments whose masks are held at once
+constexpr int kScanRanges = 27;  // candidate ranges per segment (9 in row order)
+constexpr int kMaskStride = kScanWords + 1;  // per lane, odd: conflict-free column reads
+struct __align__(16) ScanWarp {
+  float px[36], py[36], pz[36];                  // the segment's particles, padded to quads with NaN
+  uint32_t mask[32 * kMaskStride];               // [lane][word]
+  uint32_t vstart[kScanSegs][kScanRanges + 1];   // sequence index of each range's first candidate; [R] = total
+  uint32_t sstart[kScanSegs][kScanRanges];       // slot of each range's first candidate
+};
+static_assert(sizeof(ScanWarp) % 16 == 0, "per-warp scratch keeps 16-byte alignment");
+static_assert(offsetof(ScanWarp, py) % 16 == 0 && offsetof(ScanWarp, pz) % 16 == 0, "quad loads");
+
+// Returns this lane's neighbour count (entries stored up to kNbrCap). Every
+// lane of the warp calls it, `live` or not.
+template <class KP>
+__device__ __forceinline__ uint32_t scan_warp(const KP& kp, int i, bool live, Planes pl,
+                                              const uint2* __restrict__ ctab, ScanWarp& S,
+                                              uint32_t* __restrict__ nbr, int n) {
+  constexpr unsigned kAll = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  const float* xs = pl.xyz;
+  const float* ys = xs + pl.stride;
+  const float* zs = ys + pl.stride;
+  const float nan = __int_as_float(0x7fc00000);
+  float qx = 0.0f, qy = 0.0f, qz = 0.0f;
+  int cx = 0, cy = 0, cz = 0;
+  uint32_t key = 0xffffffffu;
+  if (live) {
+    const SimConst& k = kp.at(i);
+    qx = xs[i];
+    qy = ys[i];
+    qz = zs[i];
+    cx = axis_cell(qx, k.gmin[0], k.cell, k.dims[0]);
+    cy = axis_cell(qy, k.gmin[1], k.cell, k.dims[1]);
+    cz = axis_cell(qz, k.gmin[2], k.cell, k.dims[2]);
+    key = (uint32_t)(k.coff + cell_hash(cx, cy, cz, k));  // global cell: instances never share one
+  }
+  const uint32_t prev = __shfl_up_sync(kAll, key, 1);
+  const uint32_t heads = __ballot_sync(kAll, live && (lane == 0 || prev != key));
+  const uint32_t livemask = __ballot_sync(kAll, live);  // a prefix of the lanes
+  const int myhead = live ? 31 - __clz(heads & (lane == 31 ? kAll : (2u << lane) - 1u)) : 0;
+  uint32_t listed = 0;
+  uint32_t rem = heads;
+  while (rem) {
+    uint32_t batch = 0, t = rem;  // the next kScanSegs segments
+    for (int q = 0; q < kScanSegs && t; ++q) {
+      batch |= t & (0u - t);
+      t &= t - 1u;
+    }
+    rem = t;
+    __syncwarp();
+    int seg = 0;
+    for (uint32_t bb = batch; bb; bb &= bb - 1u, ++seg) {
+      const int hl = __ffs(bb) - 1;
+      const uint32_t after = heads & ~(hl == 31 ? kAll : (2u << hl) - 1u);
+      const int he = after ? __ffs(after) - 1 : 32 - __clz(livemask);
+      const int m = he - hl;
+      const int scx = __shfl_sync(kAll, cx, hl), scy = __shfl_sync(kAll, cy, hl), scz = __shfl_sync(kAll, cz, hl);
+      const SimConst& k = kp.at(__shfl_sync(kAll, i, hl));
+      const int R = k.rows ? 9 : 27;
+      uint32_t len = 0, st = 0;
+      if (lane < R) {  // lane r: range r of the sequence
+        const int dz = k.rows ? lane / 3 - 1 : lane / 9 - 1;
+        const int dy = k.rows ? lane % 3 - 1 : (lane / 3) % 3 - 1;
+        const int nz = scz + dz, ny = scy + dy;
+        if (nz >= 0 && nz < k.dims[2] && ny >= 0 && ny < k.dims[1]) {
+          const int row = k.coff + (ny + nz * k.dims[1]) * k.dims[0];
+          if (k.rows) {
+            const int xa = scx > 0 ? scx - 1 : scx, xb = scx + 1 < k.dims[0] ? scx + 1 : scx;
+            const uint2 sa = __ldg(&ctab[row + xa]), sb = __ldg(&ctab[row + xb]);
+            st = sa.x;
+            len = sb.x + sb.y - sa.x;
+          } else {
+            const int nx = scx + lane % 3 - 1;
+            if (nx >= 0 && nx < k.dims[0]) {
+              const uint2 se = __ldg(&ctab[row + nx]);
+              st = se.x;
+              len = se.y;
+            }
+          }
+        }
+      }
+      uint32_t incl = len;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t v = __shfl_up_sync(kAll, incl, o);
+        if (lane >= o) incl += v;
+      }
+      const uint32_t total = __shfl_sync(kAll, incl, 31);
+      if (lane < R) {
+        S.vstart[seg][lane] = incl - len;
+        S.sstart[seg][lane] = st;
+      }
+      if (lane == 0) S.vstart[seg][R] = total;
+      const bool in_seg = lane >= hl && lane < he;
+      if (in_seg) {
+        S.px[lane - hl] = qx;
+        S.py[lane - hl] = qy;
+        S.pz[lane - hl] = qz;
+      }
+      if (lane >= m && lane < ((m + 3) & ~3)) {
+        S.px[lane] = nan;
+        S.py[lane] = nan;
+        S.pz[lane] = nan;
+      }
+      __syncwarp();
+      const int nw = (int)((total + 31u) / 32u);
+      if (nw <= kScanWords) {
+        const float r2 = k.radius_sq;
+        // this lane's own slot in the sequence (its home range is range R/2)
+        const uint32_t vself = S.vstart[seg][R / 2] + ((uint32_t)i - S.sstart[seg][R / 2]);
+        const int mp = lane - hl;
+        int r = 0;
+        float nxv = nan, nyv = nan, nzv = nan;
+        auto fetch = [&](int w) {  // candidate 32 w + lane (NaN past the end: in no particle's support)
+          const uint32_t v = (uint32_t)(w * 32 + lane);
+          nxv = nan;
+          nyv = nan;
+          nzv = nan;
+          if (v < total) {
+            while (v >= S.vstart[seg][r + 1]) ++r;
+            const uint32_t slot = S.sstart[seg][r] + (v - S.vstart[seg][r]);
+            nxv = __ldg(&xs[slot]);
+            nyv = __ldg(&ys[slot]);
+            nzv = __ldg(&zs[slot]);
+          }
+        };
+        fetch(0);
+        for (int w = 0; w < nw; ++w) {
+          const unsigned long long CX = f2_pack(nxv, nxv), CY = f2_pack(nyv, nyv), CZ = f2_pack(nzv, nzv);
+          if (w + 1 < nw) fetch(w + 1);  // next word's candidates in flight
+          uint32_t mine = 0;
+          for (int p = 0; p < m; p += 4) {
+            const float4 ax = *reinterpret_cast<const float4*>(&S.px[p]);
+            const float4 ay = *reinterpret_cast<const float4*>(&S.py[p]);
+            const float4 az = *reinterpret_cast<const float4*>(&S.pz[p]);
+            const unsigned long long dx0 = f2_sub(f2_pack(ax.x, ax.y), CX), dx1 = f2_sub(f2_pack(ax.z, ax.w), CX);
+            const unsigned long long dy0 = f2_sub(f2_pack(ay.x, ay.y), CY), dy1 = f2_sub(f2_pack(ay.z, ay.w), CY);
+            const unsigned long long dz0 = f2_sub(f2_pack(az.x, az.y), CZ), dz1 = f2_sub(f2_pack(az.z, az.w), CZ);
+            float d0, d1, d2, d3;
+            f2_unpack(f2_add(f2_add(f2_mul(dx0, dx0), f2_mul(dy0, dy0)), f2_mul(dz0, dz0)), d0, d1);
+            f2_unpack(f2_add(f2_add(f2_mul(dx1, dx1), f2_mul(dy1, dy1)), f2_mul(dz1, dz1)), d2, d3);
+            const uint32_t M0 = __ballot_sync(kAll, d0 <= r2), M1 = __ballot_sync(kAll, d1 <= r2);
+            const uint32_t M2 = __ballot_sync(kAll, d2 <= r2), M3 = __ballot_sync(kAll, d3 <= r2);
+            const int d = mp - p;
+            mine = d == 0 ? M0 : mine;
+            mine = d == 1 ? M1 : mine;
+            mine = d == 2 ? M2 : mine;
+            mine = d == 3 ? M3 : mine;
+          }
+          if (in_seg) {
+            if ((vself >> 5) == (uint32_t)w) mine &= ~(1u << (vself & 31u));
+            S.mask[lane * kMaskStride + w] = mine;
+          }
+        }
+      }
+      __syncwarp();
+    }
+    // the batch's lanes turn their masks into their lists
+    if (live && ((batch >> myhead) & 1u)) {
+      const SimConst& k = kp.at(i);
+      const int R = k.rows ? 9 : 27;
+      const int s = __popc(batch & ((1u << myhead) - 1u));
+      const uint32_t total = S.vstart[s][R];
+      const int nw = (int)((total + 31u) / 32u);
+      if (nw > kScanWords) {
+        listed = record_neighbors(qx, qy, qz, i, pl, ctab, ScanGeo(k), nbr, n);
+      } else {
+        const uint32_t* words = S.mask + lane * kMaskStride;
+        int w = 0, r = 0;
+        uint32_t M = words[0];
+        uint32_t vnext = S.vstart[s][1];
+        uint32_t delta = S.sstart[s][0] - S.vstart[s][0];  // slot - sequence index within range r
+        size_t at = (size_t)i;
+        for (;;) {
+          while (M == 0u && w + 1 < nw) M = words[++w];
+          if (M == 0u) break;
+          const uint32_t v = (uint32_t)(w * 32 + __ffs(M) - 1);
+          M &= M - 1u;
+          while (v >= vnext) {
+            ++r;
+            vnext = S.vstart[s][r + 1];
+            delta = S.sstart[s][r] - S.vstart[s][r];
+          }
+          if (listed < kNbrCap) nbr[at] = v + delta;
+          at += (size_t)n;
+          ++listed;
+        }
+      }
+    }
+    __syncwarp();
+  }
+  return listed;
 }
 
 // ---------------------------------------------------------------------------
@@ -687,17 +885,21 @@ k_xsph_drift(KP kp, int n, const float* __restrict__ dtp, const float4* __restri
         float bx = pi.x - p1.x, by = pi.y - p1.y, bz = pi.z - p1.z;
         term(p1, h1, bx, by, bz, bx * bx + by * by + bz * bz);
       };
+      const uint32_t* e = nbr + i;  // entry c at e[c n]
       for (; c + 3 < cnt; c += 4) {
-        uint4 e = __ldg(reinterpret_cast<const uint4*>(nbr + nbr_index(c, n, i)));
-        pair((int)e.x, (int)e.y);
-        pair((int)e.z, (int)e.w);
+        const int s0 = (int)__ldg(e), s1 = (int)__ldg(e + n), s2 = (int)__ldg(e + 2 * (size_t)n),
+                  s3 = (int)__ldg(e + 3 * (size_t)n);
+        e += 4 * (size_t)n;
+        pair(s0, s1);
+        pair(s2, s3);
       }
       for (; c + 1 < cnt; c += 2) {
-        uint2 e = nbr_pair(nbr, c, n, i);
-        pair((int)e.x, (int)e.y);
+        const int s0 = (int)__ldg(e), s1 = (int)__ldg(e + n);
+        e += 2 * (size_t)n;
+        pair(s0, s1);
       }
       if (c < cnt) {
-        int s = (int)__ldg(&nbr[nbr_index(c, n, i)]);
+        int s = (int)__ldg(e);
         float4 pj, vh;
         ld_record(rec + 2 * s, pj, vh);
         float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
@@ -950,9 +1152,15 @@ k_density(KP kp, int n, const float* __restrict__ dtp, const float4* __restrict_
           float2* __restrict__ rf, float* __restrict__ pr, const uint32_t* __restrict__ err,
           uint32_t* __restrict__ nbr, uint32_t* __restrict__ ncount, const float* __restrict__ sdf,
           const float2* __restrict__ wall_tab, ClosureBufs cb) {
+  // a warp wholly past the end leaves at once; every other lane takes part
+  // in the warp scan (and, with CL = 2, in the network epilogue)
+  if (blockIdx.x * blockDim.x + (threadIdx.x & ~31u) >= (unsigned)n) return;
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   const bool live = i < n && !*err;
-  // the fused network is a warp-wide epilogue: every lane reaches it
+  extern __shared__ __align__(16) unsigned char s_dyn[];
+  // Phase 1: the warp scan lists every lane's in-support slots in visit order.
+  const uint32_t listed = scan_warp(kp, i, live, pl, ctab, reinterpret_cast<ScanWarp*>(s_dyn)[threadIdx.x >> 5],
+                                    nbr, n);
   bool near_wall = false;
   float f[16];
   float rho_pre = 0.0f;
@@ -967,12 +1175,6 @@ k_density(KP kp, int n, const float* __restrict__ dtp, const float4* __restrict_
     float rho = pi.w * k.norm_h3;
     float diff_sum = 0.0f;
     bool delta = (k.flags & kFlagDelta) != 0;
-    // Phase 1: the 27-cell scan records the in-support slots, in visit order,
-    // through this thread's column of the block's dynamic shared memory
-    // (entry j of the ring at s_stage[j * blockDim.x + threadIdx.x]).
-    extern __shared__ uint32_t s_stage[];
-    const uint32_t listed = record_neighbors(pi.x, pi.y, pi.z, i, pl, ctab, k, nbr, n, s_stage + threadIdx.x,
-                                             blockDim.x);
     ncount[i] = listed;
     // Phase 2: density and delta-SPH terms over the list, same order.
     auto term_rv = [&](const float4& pj, const float2& rvj, float dx, float dy, float dz, float d2) {
@@ -1002,17 +1204,20 @@ k_density(KP kp, int n, const float* __restrict__ dtp, const float4* __restrict_
       };
       // the list was written above by this thread: plain (coherent) loads
       uint32_t c = 0;
+      const uint32_t* e = nbr + i;  // entry c at e[c n]
       for (; c + 3 < listed; c += 4) {
-        uint4 e = *reinterpret_cast<const uint4*>(nbr + nbr_index(c, n, i));
-        pair((int)e.x, (int)e.y);
-        pair((int)e.z, (int)e.w);
+        const int s0 = (int)e[0], s1 = (int)e[n], s2 = (int)e[2 * (size_t)n], s3 = (int)e[3 * (size_t)n];
+        e += 4 * (size_t)n;
+        pair(s0, s1);
+        pair(s2, s3);
       }
       for (; c + 1 < listed; c += 2) {
-        uint2 e = *reinterpret_cast<const uint2*>(nbr + nbr_index(c, n, i));
-        pair((int)e.x, (int)e.y);
+        const int s0 = (int)e[0], s1 = (int)e[n];
+        e += 2 * (size_t)n;
+        pair(s0, s1);
       }
       if (c < listed) {
-        int s = (int)nbr[nbr_index(c, n, i)];
+        int s = (int)e[0];
         float4 pj = __ldg(&pos[s]);
         float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
         term(s, pj, dx, dy, dz, dx * dx + dy * dy + dz * dz);
@@ -1107,9 +1312,9 @@ k_density(KP kp, int n, const float* __restrict__ dtp, const float4* __restrict_
   }  // live
   if (CL == 2) {
     // network epilogue: up to 16 of the warp's near-wall particles per tile
-    extern __shared__ uint32_t s_stage[];
     const int lane = threadIdx.x & 31;
-    uint32_t* tile = s_stage + kStageRing * blockDim.x + (threadIdx.x >> 5) * kClTileWords;
+    uint32_t* tile = reinterpret_cast<uint32_t*>(s_dyn + (blockDim.x >> 5) * sizeof(ScanWarp)) +
+                     (threadIdx.x >> 5) * kClTileWords;
     __nv_bfloat16* xt = reinterpret_cast<__nv_bfloat16*>(tile);
     float* yt = reinterpret_cast<float*>(tile + 16 * 16 / 2);
     unsigned pending = __ballot_sync(0xffffffffu, near_wall);
@@ -1397,17 +1602,21 @@ k_forces(KP kp, int n, const float* __restrict__ dtp, float hdt_scale,
         term(p1, v1, f1, bx, by, bz, bx * bx + by * by + bz * bz);
       };
       uint32_t c = 0;
+      const uint32_t* e = nbr + i;  // entry c at e[c n]
       for (; c + 3 < cnt; c += 4) {
-        uint4 e = __ldg(reinterpret_cast<const uint4*>(nbr + nbr_index(c, n, i)));
-        pair((int)e.x, (int)e.y);
-        pair((int)e.z, (int)e.w);
+        const int s0 = (int)__ldg(e), s1 = (int)__ldg(e + n), s2 = (int)__ldg(e + 2 * (size_t)n),
+                  s3 = (int)__ldg(e + 3 * (size_t)n);
+        e += 4 * (size_t)n;
+        pair(s0, s1);
+        pair(s2, s3);
       }
       for (; c + 1 < cnt; c += 2) {
-        uint2 e = nbr_pair(nbr, c, n, i);
-        pair((int)e.x, (int)e.y);
+        const int s0 = (int)__ldg(e), s1 = (int)__ldg(e + n);
+        e += 2 * (size_t)n;
+        pair(s0, s1);
       }
       if (c < cnt) {
-        int s = (int)__ldg(&nbr[nbr_index(c, n, i)]);
+        int s = (int)__ldg(e);
         float4 pj = __ldg(&pos[s]);
         float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
         term(pj, __ldg(&vel[s]), __ldg(&rf[s]), dx, dy, dz, dx * dx + dy * dy + dz * dz);
