@@ -211,6 +211,8 @@ SimConst make_const(const SphParams& p, const uint32_t dims[3]) {
   SimConst k{};
   float h = p.h;
   k.h = h;
+  volatile float one = 1.0f;
+  k.inv_h = one / h;  // RN(1/h), the divisor's reciprocal for sph::div_h
   k.support = 2.0f * h;
   k.radius_sq = k.support * k.support;
   k.cell = 2.0f * h;

@@ -41,7 +41,7 @@ constexpr uint32_t kNbrCap = 128;      // listed neighbours per particle
 // SPH_MAXNREG_DENSITY (__maxnreg__ below; each measured at 2M particles).
 
 #ifndef SPH_MAXNREG_DENSITY
-#define SPH_MAXNREG_DENSITY 56
+#define SPH_MAXNREG_DENSITY 64
 #endif
 #ifndef SPH_MAXNREG_FORCES
 #define SPH_MAXNREG_FORCES 56
@@ -56,6 +56,7 @@ enum : uint32_t { kErrCellCap = 1, kErrAdamiCap = 2 };
 // Step constants, each rounded in f32 exactly as the reference evaluates it.
 struct SimConst {
   float h, support, radius_sq, cell;
+  float inv_h;       // RN(1 / h)
   float gmin[3];
   int dims[3];
   float norm_h3;     // NORM / (h*h*h)        (sph.rs:45)
@@ -129,9 +130,25 @@ __device__ __forceinline__ int cell_hash(int cx, int cy, int cz, const SimConst&
   return cx + cy * k.dims[0] + cz * k.dims[0] * k.dims[1];
 }
 
+// r / h correctly rounded, from inv_h = RN(1/h) and two FMA residual
+// corrections (Markstein's division by the fused multiply-add; Muller et al.,
+// Handbook of Floating-Point Arithmetic, "Division using the FMA"): q1 =
+// RN(q0 + RN(r - h q0) inv_h) is within an ulp of r / h, so its residual
+// r - h q1 is exact and RN(q1 + (r - h q1) inv_h) is the correctly rounded
+// quotient. That holds while the residuals do not underflow, i.e. for every
+// r above 2^-100 or so (checked exhaustively against IEEE division for the
+// smoothing lengths the tests use); the Wendland kernel and its gradient do
+// not depend on q's low bits below r = 2^-36 (q < 2^-26 rounds out of
+// 1 - q/2 and 1 + 2q, and the gradient is zero below r = 1e-12).
+__device__ __forceinline__ float div_h(float r, const SimConst& k) {
+  const float q0 = __fmul_rn(r, k.inv_h);
+  const float q1 = __fmaf_rn(__fmaf_rn(-q0, k.h, r), k.inv_h, q0);
+  return __fmaf_rn(__fmaf_rn(-q1, k.h, r), k.inv_h, q1);
+}
+
 // sph.rs:35-46 with NORM/h^3 precomputed (same rounding).
 __device__ __forceinline__ float w_c2(float r, const SimConst& k) {
-  float q = r / k.h;
+  float q = div_h(r, k);
   if (q >= 2.0f) return 0.0f;
   float omq = 1.0f - 0.5f * q;
   float t = omq * omq;
@@ -142,7 +159,7 @@ __device__ __forceinline__ float w_c2(float r, const SimConst& k) {
 // sph.rs:68-85
 __device__ __forceinline__ void grad_c2(float dx, float dy, float dz, float r, const SimConst& k,
                                         float& gx, float& gy, float& gz) {
-  float q = r / k.h;
+  float q = div_h(r, k);
   if (q >= 2.0f || r < 1.0e-12f) {
     gx = 0.0f; gy = 0.0f; gz = 0.0f;
     return;
@@ -619,11 +636,16 @@ static_assert(sizeof(ScanWarp) % 16 == 0, "per-warp scratch keeps 16-byte alignm
 static_assert(offsetof(ScanWarp, py) % 16 == 0 && offsetof(ScanWarp, pz) % 16 == 0, "quad loads");
 
 // Returns this lane's neighbour count (entries stored up to kNbrCap). Every
-// lane of the warp calls it, `live` or not.
-template <class KP>
+// lane of the warp calls it, `live` or not. A lane whose list comes from its
+// masks also hands every neighbour, in list order, to two(s0, s1) (two at a
+// time, their gathers in flight together) or one(s) (the last of an odd
+// count), and sets `fed`; a lane of a neighbourhood too large for the masks
+// takes the per-thread scan, and its caller replays the list.
+template <class KP, class Two, class One>
 __device__ __forceinline__ uint32_t scan_warp(const KP& kp, int i, bool live, Planes pl,
                                               const uint2* __restrict__ ctab, ScanWarp& S,
-                                              uint32_t* __restrict__ nbr, int n) {
+                                              uint32_t* __restrict__ nbr, int n, Two&& two, One&& one,
+                                              bool& fed) {
   constexpr unsigned kAll = 0xffffffffu;
   const int lane = threadIdx.x & 31;
   const float* xs = pl.xyz;
@@ -774,15 +796,17 @@ __device__ __forceinline__ uint32_t scan_warp(const KP& kp, int i, bool live, Pl
       if (nw > kScanWords) {
         listed = record_neighbors(qx, qy, qz, i, pl, ctab, ScanGeo(k), nbr, n);
       } else {
+        fed = true;
         const uint32_t* words = S.mask + lane * kMaskStride;
         int w = 0, r = 0;
         uint32_t M = words[0];
         uint32_t vnext = S.vstart[s][1];
         uint32_t delta = S.sstart[s][0] - S.vstart[s][0];  // slot - sequence index within range r
         size_t at = (size_t)i;
-        for (;;) {
+        // the next neighbour's slot, stored as the next entry; false when none is left
+        auto next = [&](uint32_t& slot) {
           while (M == 0u && w + 1 < nw) M = words[++w];
-          if (M == 0u) break;
+          if (M == 0u) return false;
           const uint32_t v = (uint32_t)(w * 32 + __ffs(M) - 1);
           M &= M - 1u;
           while (v >= vnext) {
@@ -790,9 +814,19 @@ __device__ __forceinline__ uint32_t scan_warp(const KP& kp, int i, bool live, Pl
             vnext = S.vstart[s][r + 1];
             delta = S.sstart[s][r] - S.vstart[s][r];
           }
-          if (listed < kNbrCap) nbr[at] = v + delta;
+          slot = v + delta;
+          if (listed < kNbrCap) nbr[at] = slot;
           at += (size_t)n;
           ++listed;
+          return true;
+        };
+        uint32_t sa, sb;
+        while (next(sa)) {
+          if (!next(sb)) {
+            one((int)sa);
+            break;
+          }
+          two((int)sa, (int)sb);
         }
       }
     }
@@ -1158,72 +1192,75 @@ k_density(KP kp, int n, const float* __restrict__ dtp, const float4* __restrict_
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   const bool live = i < n && !*err;
   extern __shared__ __align__(16) unsigned char s_dyn[];
-  // Phase 1: the warp scan lists every lane's in-support slots in visit order.
+  // the lane's state (a lane past the end holds slot 0's, unused)
+  const int iv = live ? i : 0;
+  const SimConst& k = kp.at(iv);
+  const float4 pi = pos[iv];
+  const float rho_old_i = rv[iv].x;
+  float rho = pi.w * k.norm_h3;
+  float diff_sum = 0.0f;
+  float ssum = 0.0f;  // closure: kernel sum
+  const bool delta = (k.flags & kFlagDelta) != 0;
+  // density and delta-SPH terms of one neighbour, in list order
+  auto term_rv = [&](const float4& pj, const float2& rvj, float dx, float dy, float dz, float d2) {
+    float r = sqrtf(d2);
+    if (delta) {
+      float gx, gy, gz;
+      grad_c2(dx, dy, dz, r, k, gx, gy, gz);
+      float r_dot_grad = dx * gx + dy * gy + dz * gz;
+      float density_diff = rho_old_i - rvj.x;
+      diff_sum += rvj.y * density_diff * 2.0f * r_dot_grad / (d2 + k.eta_sq);
+    }
+    float w = w_c2(r, k);
+    rho += pj.w * w;
+    if (CL) ssum += rvj.y * w;
+  };
+  auto term = [&](int s, const float4& pj, float dx, float dy, float dz, float d2) {
+    term_rv(pj, __ldg(&rv[s]), dx, dy, dz, d2);
+  };
+  auto pair = [&](int s0, int s1) {  // both neighbours' gathers in flight before either term
+    float4 p0 = __ldg(&pos[s0]), p1 = __ldg(&pos[s1]);
+    float2 r0 = __ldg(&rv[s0]), r1 = __ldg(&rv[s1]);
+    float ax = pi.x - p0.x, ay = pi.y - p0.y, az = pi.z - p0.z;
+    term_rv(p0, r0, ax, ay, az, ax * ax + ay * ay + az * az);
+    float bx = pi.x - p1.x, by = pi.y - p1.y, bz = pi.z - p1.z;
+    term_rv(p1, r1, bx, by, bz, bx * bx + by * by + bz * bz);
+  };
+  auto single = [&](int s) {
+    float4 pj = __ldg(&pos[s]);
+    float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
+    term(s, pj, dx, dy, dz, dx * dx + dy * dy + dz * dz);
+  };
+  // Phase 1: the warp scan lists every lane's in-support slots in visit order
+  // and feeds them to the terms as it lists them.
+  bool fed = false;
   const uint32_t listed = scan_warp(kp, i, live, pl, ctab, reinterpret_cast<ScanWarp*>(s_dyn)[threadIdx.x >> 5],
-                                    nbr, n);
+                                    nbr, n, pair, single, fed);
   bool near_wall = false;
   float f[16];
   float rho_pre = 0.0f;
   if (CL != 2 && !live) return;
   if (live) {
-    const SimConst& k = kp.at(i);
     float dt = dtp[k.inst];
-    float ssum = 0.0f, rho_wall = 0.0f;  // closure: kernel sum, wall density
+    float rho_wall = 0.0f;  // closure: wall density
     uint32_t nwall = 0;
-    float4 pi = pos[i];
-    float rho_old_i = rv[i].x;
-    float rho = pi.w * k.norm_h3;
-    float diff_sum = 0.0f;
-    bool delta = (k.flags & kFlagDelta) != 0;
     ncount[i] = listed;
-    // Phase 2: density and delta-SPH terms over the list, same order.
-    auto term_rv = [&](const float4& pj, const float2& rvj, float dx, float dy, float dz, float d2) {
-      float r = sqrtf(d2);
-      if (delta) {
-        float gx, gy, gz;
-        grad_c2(dx, dy, dz, r, k, gx, gy, gz);
-        float r_dot_grad = dx * gx + dy * gy + dz * gz;
-        float density_diff = rho_old_i - rvj.x;
-        diff_sum += rvj.y * density_diff * 2.0f * r_dot_grad / (d2 + k.eta_sq);
+    // Phase 2 (a neighbourhood too large for the warp scan's masks): the
+    // terms over the list just stored, or over the cells past its capacity.
+    if (!fed) {
+      if (listed <= kNbrCap) {
+        // the list was written above by this thread: plain (coherent) loads
+        uint32_t c = 0;
+        const uint32_t* e = nbr + i;  // entry c at e[c n]
+        for (; c + 1 < listed; c += 2) {
+          const int s0 = (int)e[0], s1 = (int)e[n];
+          e += 2 * (size_t)n;
+          pair(s0, s1);
+        }
+        if (c < listed) single((int)e[0]);
+      } else {
+        for_each_neighbor(pi.x, pi.y, pi.z, i, pos, ctab, k, term);
       }
-      float w = w_c2(r, k);
-      rho += pj.w * w;
-      if (CL) ssum += rvj.y * w;
-    };
-    auto term = [&](int s, const float4& pj, float dx, float dy, float dz, float d2) {
-      term_rv(pj, __ldg(&rv[s]), dx, dy, dz, d2);
-    };
-    if (listed <= kNbrCap) {
-      auto pair = [&](int s0, int s1) {  // both neighbours' gathers in flight before either term
-        float4 p0 = __ldg(&pos[s0]), p1 = __ldg(&pos[s1]);
-        float2 r0 = __ldg(&rv[s0]), r1 = __ldg(&rv[s1]);
-        float ax = pi.x - p0.x, ay = pi.y - p0.y, az = pi.z - p0.z;
-        term_rv(p0, r0, ax, ay, az, ax * ax + ay * ay + az * az);
-        float bx = pi.x - p1.x, by = pi.y - p1.y, bz = pi.z - p1.z;
-        term_rv(p1, r1, bx, by, bz, bx * bx + by * by + bz * bz);
-      };
-      // the list was written above by this thread: plain (coherent) loads
-      uint32_t c = 0;
-      const uint32_t* e = nbr + i;  // entry c at e[c n]
-      for (; c + 3 < listed; c += 4) {
-        const int s0 = (int)e[0], s1 = (int)e[n], s2 = (int)e[2 * (size_t)n], s3 = (int)e[3 * (size_t)n];
-        e += 4 * (size_t)n;
-        pair(s0, s1);
-        pair(s2, s3);
-      }
-      for (; c + 1 < listed; c += 2) {
-        const int s0 = (int)e[0], s1 = (int)e[n];
-        e += 2 * (size_t)n;
-        pair(s0, s1);
-      }
-      if (c < listed) {
-        int s = (int)e[0];
-        float4 pj = __ldg(&pos[s]);
-        float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
-        term(s, pj, dx, dy, dz, dx * dx + dy * dy + dz * dz);
-      }
-    } else {
-      for_each_neighbor(pi.x, pi.y, pi.z, i, pos, ctab, k, term);
     }
     int lin = cell_hash(axis_cell(pi.x, k.gmin[0], k.cell, k.dims[0]),
                         axis_cell(pi.y, k.gmin[1], k.cell, k.dims[1]),
