@@ -616,8 +616,10 @@ __device__ __noinline__ uint32_t record_neighbors(float px, float py, float pz, 
 // segment's particles at a time every lane computes its candidate's squared
 // distance to each (two f32x2 chains, rounded as the scalar expression); a
 // ballot per particle gives that particle's 32-bit in-support mask for the
-// word, which the particle's own lane keeps. The particle's own slot is
-// cleared from its masks, and each lane then turns its masks into its list,
+// word, and one lane stores the quad's four masks with one 16-byte store
+// (per segment the masks lie word-major: word w of the segment's particle p
+// at mask[base + w q + p], q its particle count rounded up to a quad). Each
+// lane then turns its particle's masks, its own slot cleared, into its list,
 // one entry per step, so that every active lane stores entry c at the same
 // step (entry-major: the stores of a step coalesce). The list and its order
 // equal for_each_neighbor's: a candidate outside support sets no bit, and the
@@ -625,12 +627,15 @@ __device__ __noinline__ uint32_t record_neighbors(float px, float py, float pz, 
 constexpr int kScanWords = 24;   // mask words per particle: up to 768 candidates per neighbourhood
 constexpr int kScanSegs = 4;     // segments whose masks are held at once
 constexpr int kScanRanges = 27;  // candidate ranges per segment (9 in row order)
-constexpr int kMaskStride = kScanWords + 1;  // per lane, odd: conflict-free column reads
+// masks of one batch: at most kScanWords words per quad-padded particle, and
+// the batch's segments hold 32 particles plus at most 3 pads each
+constexpr int kMaskWords = kScanWords * (32 + 3 * kScanSegs);
 struct __align__(16) ScanWarp {
   float px[36], py[36], pz[36];                  // the segment's particles, padded to quads with NaN
-  uint32_t mask[32 * kMaskStride];               // [lane][word]
+  uint32_t mask[kMaskWords];                     // per segment [word][particle]
   uint32_t vstart[kScanSegs][kScanRanges + 1];   // sequence index of each range's first candidate; [R] = total
   uint32_t sstart[kScanSegs][kScanRanges];       // slot of each range's first candidate
+  uint32_t mbase[kScanSegs], mquad[kScanSegs];   // each segment's mask base and particle stride
 };
 static_assert(sizeof(ScanWarp) % 16 == 0, "per-warp scratch keeps 16-byte alignment");
 static_assert(offsetof(ScanWarp, py) % 16 == 0 && offsetof(ScanWarp, pz) % 16 == 0, "quad loads");
@@ -680,6 +685,7 @@ __device__ __forceinline__ uint32_t scan_warp(const KP& kp, int i, bool live, Pl
     rem = t;
     __syncwarp();
     int seg = 0;
+    uint32_t mbase = 0;  // the next segment's mask base (a multiple of 4 words)
     for (uint32_t bb = batch; bb; bb &= bb - 1u, ++seg) {
       const int hl = __ffs(bb) - 1;
       const uint32_t after = heads & ~(hl == 31 ? kAll : (2u << hl) - 1u);
@@ -733,13 +739,16 @@ __device__ __forceinline__ uint32_t scan_warp(const KP& kp, int i, bool live, Pl
         S.py[lane] = nan;
         S.pz[lane] = nan;
       }
-      __syncwarp();
       const int nw = (int)((total + 31u) / 32u);
+      const int q4 = (m + 3) & ~3;
+      if (lane == 0) {
+        S.mbase[seg] = mbase;
+        S.mquad[seg] = (uint32_t)q4;
+      }
+      __syncwarp();
       if (nw <= kScanWords) {
         const float r2 = k.radius_sq;
-        // this lane's own slot in the sequence (its home range is range R/2)
-        const uint32_t vself = S.vstart[seg][R / 2] + ((uint32_t)i - S.sstart[seg][R / 2]);
-        const int mp = lane - hl;
+        uint32_t* const mw = S.mask + mbase;
         int r = 0;
         float nxv = nan, nyv = nan, nzv = nan;
         auto fetch = [&](int w) {  // candidate 32 w + lane (NaN past the end: in no particle's support)
@@ -759,7 +768,7 @@ __device__ __forceinline__ uint32_t scan_warp(const KP& kp, int i, bool live, Pl
         for (int w = 0; w < nw; ++w) {
           const unsigned long long CX = f2_pack(nxv, nxv), CY = f2_pack(nyv, nyv), CZ = f2_pack(nzv, nzv);
           if (w + 1 < nw) fetch(w + 1);  // next word's candidates in flight
-          uint32_t mine = 0;
+          uint32_t* const row = mw + w * q4;
           for (int p = 0; p < m; p += 4) {
             const float4 ax = *reinterpret_cast<const float4*>(&S.px[p]);
             const float4 ay = *reinterpret_cast<const float4*>(&S.py[p]);
@@ -772,17 +781,10 @@ __device__ __forceinline__ uint32_t scan_warp(const KP& kp, int i, bool live, Pl
             f2_unpack(f2_add(f2_add(f2_mul(dx1, dx1), f2_mul(dy1, dy1)), f2_mul(dz1, dz1)), d2, d3);
             const uint32_t M0 = __ballot_sync(kAll, d0 <= r2), M1 = __ballot_sync(kAll, d1 <= r2);
             const uint32_t M2 = __ballot_sync(kAll, d2 <= r2), M3 = __ballot_sync(kAll, d3 <= r2);
-            const int d = mp - p;
-            mine = d == 0 ? M0 : mine;
-            mine = d == 1 ? M1 : mine;
-            mine = d == 2 ? M2 : mine;
-            mine = d == 3 ? M3 : mine;
-          }
-          if (in_seg) {
-            if ((vself >> 5) == (uint32_t)w) mine &= ~(1u << (vself & 31u));
-            S.mask[lane * kMaskStride + w] = mine;
+            if (lane == 0) *reinterpret_cast<uint4*>(row + p) = make_uint4(M0, M1, M2, M3);
           }
         }
+        mbase += (uint32_t)(nw * q4);
       }
       __syncwarp();
     }
@@ -797,15 +799,24 @@ __device__ __forceinline__ uint32_t scan_warp(const KP& kp, int i, bool live, Pl
         listed = record_neighbors(qx, qy, qz, i, pl, ctab, ScanGeo(k), nbr, n);
       } else {
         fed = true;
-        const uint32_t* words = S.mask + lane * kMaskStride;
+        const uint32_t q4 = S.mquad[s];
+        const uint32_t* words = S.mask + S.mbase[s] + (lane - myhead);  // word w at words[w q4]
+        // this lane's own slot in the sequence (its home range is range R/2), cleared from its masks
+        const uint32_t vself = S.vstart[s][R / 2] + ((uint32_t)i - S.sstart[s][R / 2]);
+        const int wself = (int)(vself >> 5);
+        const uint32_t bself = ~(1u << (vself & 31u));
         int w = 0, r = 0;
         uint32_t M = words[0];
+        if (wself == 0) M &= bself;
         uint32_t vnext = S.vstart[s][1];
         uint32_t delta = S.sstart[s][0] - S.vstart[s][0];  // slot - sequence index within range r
         size_t at = (size_t)i;
         // the next neighbour's slot, stored as the next entry; false when none is left
         auto next = [&](uint32_t& slot) {
-          while (M == 0u && w + 1 < nw) M = words[++w];
+          while (M == 0u && w + 1 < nw) {
+            M = words[++w * q4];
+            if (w == wself) M &= bself;
+          }
           if (M == 0u) return false;
           const uint32_t v = (uint32_t)(w * 32 + __ffs(M) - 1);
           M &= M - 1u;
