@@ -931,10 +931,25 @@ k_xsph_drift(KP kp, int n, const float* __restrict__ dtp, const float4* __restri
         term(p1, h1, bx, by, bz, bx * bx + by * by + bz * bz);
       };
       const uint32_t* e = nbr + i;  // entry c at e[c n]
+      // the next four entries are loaded a round ahead, so that a round's
+      // record gathers do not wait for its list loads (XSPH -2 %; in k_forces,
+      // which holds more live registers, the same is slower)
+      int n0 = 0, n1 = 0, n2 = 0, n3 = 0;
+      if (cnt >= 4) {
+        n0 = (int)__ldg(e);
+        n1 = (int)__ldg(e + n);
+        n2 = (int)__ldg(e + 2 * (size_t)n);
+        n3 = (int)__ldg(e + 3 * (size_t)n);
+      }
       for (; c + 3 < cnt; c += 4) {
-        const int s0 = (int)__ldg(e), s1 = (int)__ldg(e + n), s2 = (int)__ldg(e + 2 * (size_t)n),
-                  s3 = (int)__ldg(e + 3 * (size_t)n);
+        const int s0 = n0, s1 = n1, s2 = n2, s3 = n3;
         e += 4 * (size_t)n;
+        if (c + 7 < cnt) {
+          n0 = (int)__ldg(e);
+          n1 = (int)__ldg(e + n);
+          n2 = (int)__ldg(e + 2 * (size_t)n);
+          n3 = (int)__ldg(e + 3 * (size_t)n);
+        }
         pair(s0, s1);
         pair(s2, s3);
       }
