@@ -106,6 +106,10 @@ struct SphHandle {
   uint8_t* bact = nullptr;  // per boundary particle: an occupied cell lists it (k_adami_mark)
   uint32_t* bc_cells = nullptr;  // the linear cells whose boundary candidate list is not empty
   int nbc_cells = 0;
+  // the boundary particles sorted by the (global) cell that holds them, for
+  // k_adami_cells; used when every instance is in the row or linear order
+  uint32_t* border = nullptr;
+  bool adami_cells = false;
   uint32_t *bc_start = nullptr, *bc_list = nullptr;
   // SDF node grid and wall table (boundary_mode SPH_BOUNDARY_SDF), or the
   // geometry SDF(s) of the closure features
@@ -601,8 +605,13 @@ void enqueue_adami(SphHandle* h) {
       k_adami_mark<<<grid_for(h->nbc_cells, 8), 256, 0, h->st>>>(h->nbc_cells, h->bc_cells, h->ctab, h->bc_start,
                                                                   h->bc_list, h->bact);
     dispatch(h, true, [&](auto kp) {
-      k_adami<<<grid_for(h->nb, kAdamiWarps), kAdamiWarps * 32, 0, h->st>>>(
-          kp, h->nb, h->bpos, h->bpress, h->pos, h->rf, h->pr, h->id, h->ctab, h->err, h->bact);
+      if (h->adami_cells)
+        k_adami_cells<<<grid_for(h->nb, kAdamiWarps * 32), kAdamiWarps * 32, 0, h->st>>>(
+            kp, h->nb, h->border, h->bpos, h->bpress, h->pos, planes(h), h->rf, h->pr, h->id, h->ctab, h->err,
+            h->bact);
+      else
+        k_adami<<<grid_for(h->nb, kAdamiWarps), kAdamiWarps * 32, 0, h->st>>>(
+            kp, h->nb, h->bpos, h->bpress, h->pos, h->rf, h->pr, h->id, h->ctab, h->err, h->bact);
     });
     h->launches += 2;
   }
@@ -1091,6 +1100,33 @@ int create_impl(int ninst, const SphParams* PP, const SphParticlesView* pvs,
   }
   if (totals.joinable()) totals.join();
   trace.mark("cell ranks, lists, totals");
+  // the boundary particles ordered by the global cell that holds them
+  // (counting sort, ascending index within a cell), for k_adami_cells
+  std::vector<uint32_t> border_h;
+  h->adami_cells = nb > 0;
+  for (int q = 0; q < ninst; ++q) h->adami_cells = h->adami_cells && h->ktab_h[q].rows != 0;
+  if (h->adami_cells) {
+    std::vector<uint32_t> bkey(nb), bnext(C + 1, 0);
+    for (int q = 0; q < ninst; ++q) {
+      const SimConst& kq = h->ktab_h[q];
+      auto cell_of = [&](float p, int a) {  // axis_cell, in the same f32 operations
+        float f = std::floor((p - kq.gmin[a]) / kq.cell);
+        f = std::fmax(f, 0.0f);
+        f = std::fmin(f, (float)(kq.dims[a] - 1));
+        return (uint32_t)f;
+      };
+      for (size_t i = h->boff[q]; i < h->boff[q + 1]; ++i) {
+        const float4 v = hb[i];
+        bkey[i] = (uint32_t)kq.coff + cell_of(v.x, 0) +
+                  (uint32_t)kq.dims[0] * (cell_of(v.y, 1) + (uint32_t)kq.dims[1] * cell_of(v.z, 2));
+        ++bnext[bkey[i] + 1];
+      }
+    }
+    for (uint64_t c = 0; c < C; ++c) bnext[c + 1] += bnext[c];
+    border_h.resize(nb);
+    for (size_t i = 0; i < nb; ++i) border_h[bnext[bkey[i]]++] = (uint32_t)i;
+  }
+  trace.mark("boundary order");
   h->k = h->ktab_h[0];
   h->C = (int)C;
   h->boundary_candidates = blist.size();
@@ -1119,6 +1155,7 @@ int create_impl(int ninst, const SphParams* PP, const SphParticlesView* pvs,
   if (e == cudaSuccess) e = ue;
   if (e == cudaSuccess) e = dalloc(h, &h->bc_list, blist.size());
   if (e == cudaSuccess) e = dalloc(h, &h->bc_cells, bcells.size());
+  if (e == cudaSuccess && h->adami_cells) e = dalloc(h, &h->border, nb);
   h->nbc_cells = (int)bcells.size();
   if (e == cudaSuccess && sdf_mode) e = dalloc(h, &h->wall_tab, wall_host.size());
   if (e != cudaSuccess) {
@@ -1134,6 +1171,7 @@ int create_impl(int ninst, const SphParams* PP, const SphParticlesView* pvs,
   up(h->bc_start, bstart.data(), (C + 1) * sizeof(uint32_t));
   up(h->bc_list, blist.data(), blist.size() * sizeof(uint32_t));
   up(h->bc_cells, bcells.data(), bcells.size() * sizeof(uint32_t));
+  if (h->adami_cells) up(h->border, border_h.data(), nb * sizeof(uint32_t));
   up(h->hcc, hcc.data(), ninst * sizeof(float4));
   if (ninst > 1) up(h->ktab, h->ktab_h.data(), ninst * sizeof(SimConst));
   for (int q = 0; sdf_mode && q < ninst; ++q)

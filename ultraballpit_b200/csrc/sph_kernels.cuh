@@ -1430,24 +1430,35 @@ __global__ void k_adami_mark(int ncl, const uint32_t* __restrict__ cells, const 
   for (uint32_t q = __ldg(&bc_start[c]) + lane; q < q1; q += 32) act[__ldg(&bc_list[q])] = 1;
 }
 
-template <class KP>
-__global__ void __launch_bounds__(kAdamiWarps * 32)
-k_adami(KP kp, int nb, const float4* __restrict__ bpos, float* __restrict__ bpress,
-        const float4* __restrict__ pos, const float2* __restrict__ rf, const float* __restrict__ pr,
-        const uint32_t* __restrict__ id, const uint2* __restrict__ ctab, uint32_t* __restrict__ err,
-        const uint8_t* __restrict__ act) {
-  __shared__ uint32_t s_id[kAdamiWarps][kAdamiCap];
-  __shared__ float s_w[kAdamiWarps][kAdamiCap];
-  __shared__ float s_wp[kAdamiWarps][kAdamiCap];
-  int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  int b = blockIdx.x * kAdamiWarps + warp;
-  if (b >= nb || *err) return;
-  if (!act[b]) {  // no fluid particle can be in support (k_adami_mark)
-    if (lane == 0) bpress[b] = 0.0f;
-    return;
-  }
-  const SimConst& k = kp.at(b);
-  float4 bp = bpos[b];
+// One boundary particle's in-support fluid term (boundary.rs:100-115): its
+// kernel weight w, the weighted extrapolated pressure w p_ext and the fluid
+// particle's original index (the order of the reference's sum).
+template <class KC>
+__device__ __forceinline__ bool adami_term(const KC& k, const float4& bp, int s, const float4* __restrict__ pos,
+                                           const float2* __restrict__ rf, const float* __restrict__ pr,
+                                           const uint32_t* __restrict__ id, float& w, float& wp, uint32_t& fid) {
+  float4 pf = __ldg(&pos[s]);
+  float dx = bp.x - pf.x, dy = bp.y - pf.y, dz = bp.z - pf.z;
+  float d2 = dx * dx + dy * dy + dz * dz;
+  if (!(d2 <= k.sup_d2)) return false;
+  w = w_c2(sqrtf(d2), k);
+  float g_dot_dr = k.grav[0] * dx + k.grav[1] * dy + k.grav[2] * dz;
+  float p_ext = __ldg(&pr[s]) + __ldg(&rf[s]).x * g_dot_dr;
+  wp = w * p_ext;
+  fid = __ldg(&id[s]) & kIdMask;
+  return true;
+}
+
+// The in-support fluid terms of boundary particle bp (one warp): the cells of
+// a widened range around it are looked up 32 at a time, and their candidates
+// taken 32 at a time across cells; the terms go to sid / sw / swp (up to
+// kAdamiCap) in candidate order. Returns the term count; `overflow` is set
+// on every lane when it exceeds kAdamiCap.
+__device__ __forceinline__ int adami_search(const SimConst& k, const float4& bp, const float4* __restrict__ pos,
+                                            const float2* __restrict__ rf, const float* __restrict__ pr,
+                                            const uint32_t* __restrict__ id, const uint2* __restrict__ ctab,
+                                            uint32_t* sid, float* sw, float* swp, bool& overflow) {
+  const int lane = threadIdx.x & 31;
   int lo[3], hi[3];
   float bc[3] = {bp.x, bp.y, bp.z};
 #pragma unroll
@@ -1456,7 +1467,7 @@ k_adami(KP kp, int nb, const float4* __restrict__ bpos, float* __restrict__ bpre
     hi[a] = axis_cell(bc[a] + k.reach, k.gmin[a], k.cell, k.dims[a]);
   }
   int count = 0;
-  bool overflow = false;
+  overflow = false;
   // Lanes look up the (at most 4x4x4) cells of the range in parallel; only
   // occupied cells whose box comes within 2h are then scanned (the box is
   // widened by a margin far above the rounding of the binning, edge cells
@@ -1504,29 +1515,16 @@ k_adami(KP kp, int nb, const float4* __restrict__ bpos, float* __restrict__ bpre
       uint32_t st = __shfl_sync(0xffffffffu, mine.x, src);
       uint32_t s = st + (t - __shfl_sync(0xffffffffu, excl, src));
       {
-        bool inr = false;
         float w = 0.0f, wp = 0.0f;
         uint32_t fid = 0;
-        if (t < total) {
-          float4 pf = __ldg(&pos[s]);
-          float dx = bp.x - pf.x, dy = bp.y - pf.y, dz = bp.z - pf.z;
-          float d2 = dx * dx + dy * dy + dz * dz;
-          if (d2 <= k.sup_d2) {
-            inr = true;
-            w = w_c2(sqrtf(d2), k);
-            float g_dot_dr = k.grav[0] * dx + k.grav[1] * dy + k.grav[2] * dz;
-            float p_ext = __ldg(&pr[s]) + __ldg(&rf[s]).x * g_dot_dr;
-            wp = w * p_ext;
-            fid = __ldg(&id[s]) & kIdMask;
-          }
-        }
+        const bool inr = t < total && adami_term(k, bp, (int)s, pos, rf, pr, id, w, wp, fid);
         unsigned m = __ballot_sync(0xffffffffu, inr);
         int off = count + __popc(m & ((1u << lane) - 1u));
         if (inr) {
           if (off < kAdamiCap) {
-            s_id[warp][off] = fid;
-            s_w[warp][off] = w;
-            s_wp[warp][off] = wp;
+            sid[off] = fid;
+            sw[off] = w;
+            swp[off] = wp;
           } else {
             overflow = true;
           }
@@ -1535,7 +1533,19 @@ k_adami(KP kp, int nb, const float4* __restrict__ bpos, float* __restrict__ bpre
       }
     }
   }
-  if (__any_sync(0xffffffffu, overflow) || count > kAdamiCap) {
+  overflow = __any_sync(0xffffffffu, overflow);
+  return count;
+}
+
+// The Adami pressure of one boundary particle from its `count` terms in
+// sid / sw / swp (one warp): the terms are ordered by fluid index (bitonic,
+// in registers up to 32 terms, else in shared memory) and summed in that
+// order, as the reference sums over the fluid particles in index order
+// (boundary.rs:100-123); lane 0 writes *out.
+__device__ __forceinline__ void adami_sum(int count, bool overflow, uint32_t* sid, float* sw, float* swp,
+                                          float* __restrict__ out, uint32_t* __restrict__ err) {
+  const int lane = threadIdx.x & 31;
+  if (overflow || count > kAdamiCap) {
     if (lane == 0) atomicOr(err, kErrAdamiCap);
     return;
   }
@@ -1543,9 +1553,9 @@ k_adami(KP kp, int nb, const float4* __restrict__ bpos, float* __restrict__ bpre
     // up to 32 terms: one per lane, bitonic-sorted by fluid index across the
     // lanes, then summed in that order (the same additions as below)
     __syncwarp();
-    uint32_t key = lane < count ? s_id[warp][lane] : 0xffffffffu;
-    float w = lane < count ? s_w[warp][lane] : 0.0f;
-    float wp = lane < count ? s_wp[warp][lane] : 0.0f;
+    uint32_t key = lane < count ? sid[lane] : 0xffffffffu;
+    float w = lane < count ? sw[lane] : 0.0f;
+    float wp = lane < count ? swp[lane] : 0.0f;
     for (int kk = 2; kk <= 32; kk <<= 1) {
       for (int j = kk >> 1; j > 0; j >>= 1) {
         uint32_t ok = __shfl_xor_sync(0xffffffffu, key, j);
@@ -1564,12 +1574,12 @@ k_adami(KP kp, int nb, const float4* __restrict__ bpos, float* __restrict__ bpre
       weighted_pressure += __shfl_sync(0xffffffffu, wp, q);
       weight_sum += __shfl_sync(0xffffffffu, w, q);
     }
-    if (lane == 0) bpress[b] = weight_sum > 1.0e-12f ? fmaxf(weighted_pressure / weight_sum, 0.0f) : 0.0f;
+    if (lane == 0) *out = weight_sum > 1.0e-12f ? fmaxf(weighted_pressure / weight_sum, 0.0f) : 0.0f;
     return;
   }
   int m2 = 1;
   while (m2 < count) m2 <<= 1;
-  for (int q = count + lane; q < m2; q += 32) s_id[warp][q] = 0xffffffffu;
+  for (int q = count + lane; q < m2; q += 32) sid[q] = 0xffffffffu;
   __syncwarp();
   for (int kk = 2; kk <= m2; kk <<= 1) {
     for (int j = kk >> 1; j > 0; j >>= 1) {
@@ -1577,11 +1587,11 @@ k_adami(KP kp, int nb, const float4* __restrict__ bpos, float* __restrict__ bpre
         int pq = q ^ j;
         if (pq > q) {
           bool up = (q & kk) == 0;
-          uint32_t a = s_id[warp][q], c = s_id[warp][pq];
+          uint32_t a = sid[q], c = sid[pq];
           if ((a > c) == up) {
-            s_id[warp][q] = c; s_id[warp][pq] = a;
-            float t = s_w[warp][q]; s_w[warp][q] = s_w[warp][pq]; s_w[warp][pq] = t;
-            t = s_wp[warp][q]; s_wp[warp][q] = s_wp[warp][pq]; s_wp[warp][pq] = t;
+            sid[q] = c; sid[pq] = a;
+            float t = sw[q]; sw[q] = sw[pq]; sw[pq] = t;
+            t = swp[q]; swp[q] = swp[pq]; swp[pq] = t;
           }
         }
       }
@@ -1591,10 +1601,259 @@ k_adami(KP kp, int nb, const float4* __restrict__ bpos, float* __restrict__ bpre
   if (lane == 0) {
     float weighted_pressure = 0.0f, weight_sum = 0.0f;
     for (int q = 0; q < count; ++q) {
-      weighted_pressure += s_wp[warp][q];
-      weight_sum += s_w[warp][q];
+      weighted_pressure += swp[q];
+      weight_sum += sw[q];
     }
-    bpress[b] = weight_sum > 1.0e-12f ? fmaxf(weighted_pressure / weight_sum, 0.0f) : 0.0f;
+    *out = weight_sum > 1.0e-12f ? fmaxf(weighted_pressure / weight_sum, 0.0f) : 0.0f;
+  }
+}
+
+template <class KP>
+__global__ void __launch_bounds__(kAdamiWarps * 32)
+k_adami(KP kp, int nb, const float4* __restrict__ bpos, float* __restrict__ bpress,
+        const float4* __restrict__ pos, const float2* __restrict__ rf, const float* __restrict__ pr,
+        const uint32_t* __restrict__ id, const uint2* __restrict__ ctab, uint32_t* __restrict__ err,
+        const uint8_t* __restrict__ act) {
+  __shared__ uint32_t s_id[kAdamiWarps][kAdamiCap];
+  __shared__ float s_w[kAdamiWarps][kAdamiCap];
+  __shared__ float s_wp[kAdamiWarps][kAdamiCap];
+  int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  int b = blockIdx.x * kAdamiWarps + warp;
+  if (b >= nb || *err) return;
+  if (!act[b]) {  // no fluid particle can be in support (k_adami_mark)
+    if (lane == 0) bpress[b] = 0.0f;
+    return;
+  }
+  bool overflow;
+  const int count = adami_search(kp.at(b), bpos[b], pos, rf, pr, id, ctab, s_id[warp], s_w[warp], s_wp[warp],
+                                 overflow);
+  adami_sum(count, overflow, s_id[warp], s_w[warp], s_wp[warp], bpress + b, err);
+}
+
+// Adami boundary pressure with the boundary particles taken cell by cell (the
+// row cell order, where a row's cells are consecutive). The boundary
+// particles are visited in `border`, sorted once by the cell that holds them
+// (they do not move), so that a warp's 32 entries fall into few cells. The
+// active particles of one cell run (a "segment") share one candidate
+// sequence: the (y, z) rows of the union of their widened ranges, each row
+// the union's x-cells as one slot range, less the rows whose (y, z) box lies
+// farther than 2h from the segment's bounding box (with adami_search's margin
+// and unbounded edge cells). Every cell that adami_search scans for one of
+// them lies in it, so no in-support fluid particle is missed. The lanes load
+// 32 candidates of the sequence at a time and test them against four of the
+// segment's particles at a time (two f32x2 chains, rounded as the scalar
+// expression), one ballot mask per particle. Each particle's in-support
+// candidates are then gathered, their terms evaluated one per lane
+// (adami_term), and summed by adami_sum in fluid-index order. A segment whose
+// sequence passes the masks' capacity takes adami_search per particle.
+constexpr int kAdamiRows = 25;   // (y, z) rows per segment: at most 5 x 5
+constexpr int kAdamiWords = 32;  // mask words per particle: up to 1024 candidates
+struct __align__(16) AdamiWarp {
+  float px[36], py[36], pz[36];          // the segment's particles, padded to quads with NaN
+  uint32_t mask[kAdamiWords * 32];       // [word][particle]
+  uint32_t vstart[kAdamiRows + 1];       // sequence index of each row's first candidate; [R] = total
+  uint32_t sstart[kAdamiRows];           // slot of each row's first candidate
+  uint32_t sid[kAdamiCap];               // a particle's candidates (sequence index), then its terms' fluid ids
+  float sw[kAdamiCap], swp[kAdamiCap];
+};
+static_assert(offsetof(AdamiWarp, py) % 16 == 0 && offsetof(AdamiWarp, pz) % 16 == 0 &&
+                  offsetof(AdamiWarp, mask) % 16 == 0 && sizeof(AdamiWarp) % 16 == 0,
+              "quad loads and stores");
+
+template <class KP>
+__global__ void __launch_bounds__(kAdamiWarps * 32)
+k_adami_cells(KP kp, int nb, const uint32_t* __restrict__ border, const float4* __restrict__ bpos,
+              float* __restrict__ bpress, const float4* __restrict__ pos, Planes pl,
+              const float2* __restrict__ rf, const float* __restrict__ pr, const uint32_t* __restrict__ id,
+              const uint2* __restrict__ ctab, uint32_t* __restrict__ err, const uint8_t* __restrict__ act) {
+  __shared__ AdamiWarp s_aw[kAdamiWarps];
+  constexpr unsigned kAll = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  AdamiWarp& S = s_aw[threadIdx.x >> 5];
+  const int e0 = (blockIdx.x * kAdamiWarps + (threadIdx.x >> 5)) * 32;
+  if (e0 >= nb || *err) return;  // whole warps
+  const int e = e0 + lane;
+  const bool valid = e < nb;
+  const int b = valid ? (int)__ldg(&border[e]) : (int)__ldg(&border[e0]);
+  const bool live = valid && act[b];
+  if (valid && !live) bpress[b] = 0.0f;  // no fluid particle can be in support (k_adami_mark)
+  const uint32_t livemask = __ballot_sync(kAll, live);
+  if (!livemask) return;
+  const float* xs = pl.xyz;
+  const float* ys = xs + pl.stride;
+  const float* zs = ys + pl.stride;
+  const float nan = __int_as_float(0x7fc00000);
+  const float4 bp = __ldg(&bpos[b]);
+  uint32_t key = 0xffffffffu;
+  if (live) {
+    const SimConst& k = kp.at(b);
+    key = (uint32_t)(k.coff + cell_hash(axis_cell(bp.x, k.gmin[0], k.cell, k.dims[0]),
+                                        axis_cell(bp.y, k.gmin[1], k.cell, k.dims[1]),
+                                        axis_cell(bp.z, k.gmin[2], k.cell, k.dims[2]), k));
+  }
+  const uint32_t prev = __shfl_up_sync(kAll, key, 1);
+  const uint32_t heads = __ballot_sync(kAll, live && (lane == 0 || prev != key));
+  for (uint32_t hh = heads; hh; hh &= hh - 1u) {
+    const int hl = __ffs(hh) - 1;
+    const uint32_t after = heads & ~(hl == 31 ? kAll : (2u << hl) - 1u);
+    const int he = after ? __ffs(after) - 1 : 32;
+    const uint32_t segmask = (he == 32 ? kAll : (1u << he) - 1u) & ~((1u << hl) - 1u);
+    const uint32_t members = livemask & segmask;  // the segment's active particles
+    const int m = __popc(members);
+    const bool mine = (members >> lane) & 1u;
+    const SimConst& k = kp.at(__shfl_sync(kAll, b, hl));
+    // bounding box of the members, and the union of their widened ranges
+    float lo3[3] = {mine ? bp.x : INFINITY, mine ? bp.y : INFINITY, mine ? bp.z : INFINITY};
+    float hi3[3] = {mine ? bp.x : -INFINITY, mine ? bp.y : -INFINITY, mine ? bp.z : -INFINITY};
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        lo3[a] = fminf(lo3[a], __shfl_xor_sync(kAll, lo3[a], o));
+        hi3[a] = fmaxf(hi3[a], __shfl_xor_sync(kAll, hi3[a], o));
+      }
+    int clo[3], chi[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      clo[a] = axis_cell(lo3[a] - k.reach, k.gmin[a], k.cell, k.dims[a]);
+      chi[a] = axis_cell(hi3[a] + k.reach, k.gmin[a], k.cell, k.dims[a]);
+    }
+    const int ny = chi[1] - clo[1] + 1, nz = chi[2] - clo[2] + 1, R = ny * nz;
+    uint32_t len = 0, st = 0;
+    if (lane < R && R <= kAdamiRows) {
+      const int cy = clo[1] + lane % ny, cz = clo[2] + lane / ny;
+      const float margin = 1.0e-5f * k.cell + 1.0e-6f;  // as adami_search
+      float gap2 = 0.0f;
+      const int c2[2] = {cy, cz};
+#pragma unroll
+      for (int q = 0; q < 2; ++q) {
+        const int a = q + 1;
+        const float face = k.gmin[a] + (float)c2[q] * k.cell;
+        const float below = c2[q] > 0 ? face - margin - hi3[a] : 0.0f;
+        const float above = c2[q] < k.dims[a] - 1 ? lo3[a] - (face + k.cell + margin) : 0.0f;
+        const float g = fmaxf(fmaxf(below, above), 0.0f);
+        gap2 += g * g;
+      }
+      if (gap2 <= k.radius_sq) {
+        const int row = k.coff + (cy + cz * k.dims[1]) * k.dims[0];
+        const uint2 sa = __ldg(&ctab[row + clo[0]]), sb = __ldg(&ctab[row + chi[0]]);
+        st = sa.x;
+        len = sb.x + sb.y - sa.x;
+      }
+    }
+    uint32_t incl = len;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t v = __shfl_up_sync(kAll, incl, o);
+      if (lane >= o) incl += v;
+    }
+    const uint32_t total = __shfl_sync(kAll, incl, 31);
+    const int nw = (int)((total + 31u) / 32u);
+    const int q4 = (m + 3) & ~3;
+    const bool fits = R <= kAdamiRows && nw <= kAdamiWords;
+    __syncwarp();  // the previous segment's last reads of the tables are done
+    if (lane < R && R <= kAdamiRows) {
+      S.vstart[lane] = incl - len;
+      S.sstart[lane] = st;
+    }
+    if (lane == 0 && R <= kAdamiRows) S.vstart[R] = total;
+    const int mp = __popc(members & ((1u << lane) - 1u));  // this lane's index among the members
+    if (mine) {
+      S.px[mp] = bp.x;
+      S.py[mp] = bp.y;
+      S.pz[mp] = bp.z;
+    }
+    if (lane >= m && lane < q4) {
+      S.px[lane] = nan;
+      S.py[lane] = nan;
+      S.pz[lane] = nan;
+    }
+    __syncwarp();
+    // the row holding sequence index v (< total): the last row starting at or before it
+    auto row_of = [&](uint32_t v) {
+      int r = 0;
+#pragma unroll
+      for (int step = 16; step > 0; step >>= 1)
+        if (r + step < R && S.vstart[r + step] <= v) r += step;
+      return r;
+    };
+    if (fits) {
+      const float r2 = k.sup_d2;
+      float nxv = nan, nyv = nan, nzv = nan;
+      auto fetch = [&](int w) {  // candidate 32 w + lane (NaN past the end: in no particle's support)
+        const uint32_t v = (uint32_t)(w * 32 + lane);
+        nxv = nan;
+        nyv = nan;
+        nzv = nan;
+        if (v < total) {
+          const int r = row_of(v);
+          const uint32_t slot = S.sstart[r] + (v - S.vstart[r]);
+          nxv = __ldg(&xs[slot]);
+          nyv = __ldg(&ys[slot]);
+          nzv = __ldg(&zs[slot]);
+        }
+      };
+      fetch(0);
+      for (int w = 0; w < nw; ++w) {
+        const unsigned long long CX = f2_pack(nxv, nxv), CY = f2_pack(nyv, nyv), CZ = f2_pack(nzv, nzv);
+        if (w + 1 < nw) fetch(w + 1);
+        uint32_t* const row = S.mask + w * q4;
+        for (int p = 0; p < m; p += 4) {  // boundary minus fluid, as adami_term
+          const float4 ax = *reinterpret_cast<const float4*>(&S.px[p]);
+          const float4 ay = *reinterpret_cast<const float4*>(&S.py[p]);
+          const float4 az = *reinterpret_cast<const float4*>(&S.pz[p]);
+          const unsigned long long dx0 = f2_sub(f2_pack(ax.x, ax.y), CX), dx1 = f2_sub(f2_pack(ax.z, ax.w), CX);
+          const unsigned long long dy0 = f2_sub(f2_pack(ay.x, ay.y), CY), dy1 = f2_sub(f2_pack(ay.z, ay.w), CY);
+          const unsigned long long dz0 = f2_sub(f2_pack(az.x, az.y), CZ), dz1 = f2_sub(f2_pack(az.z, az.w), CZ);
+          float d0, d1, d2, d3;
+          f2_unpack(f2_add(f2_add(f2_mul(dx0, dx0), f2_mul(dy0, dy0)), f2_mul(dz0, dz0)), d0, d1);
+          f2_unpack(f2_add(f2_add(f2_mul(dx1, dx1), f2_mul(dy1, dy1)), f2_mul(dz1, dz1)), d2, d3);
+          const uint32_t M0 = __ballot_sync(kAll, d0 <= r2), M1 = __ballot_sync(kAll, d1 <= r2);
+          const uint32_t M2 = __ballot_sync(kAll, d2 <= r2), M3 = __ballot_sync(kAll, d3 <= r2);
+          if (lane == 0) *reinterpret_cast<uint4*>(row + p) = make_uint4(M0, M1, M2, M3);
+        }
+      }
+    }
+    __syncwarp();
+    // each member in turn: its terms, then their ordered sum
+    for (uint32_t mm = members; mm; mm &= mm - 1u) {
+      const int ml = __ffs(mm) - 1;
+      const int p = __popc(members & ((1u << ml) - 1u));
+      const int bm = __shfl_sync(kAll, b, ml);
+      const float4 bpm = make_float4(__shfl_sync(kAll, bp.x, ml), __shfl_sync(kAll, bp.y, ml),
+                                     __shfl_sync(kAll, bp.z, ml), 0.0f);
+      int count = 0;
+      bool overflow = false;
+      if (fits) {
+        for (int w = 0; w < nw; ++w) {  // the in-support candidates, in sequence order
+          const uint32_t M = S.mask[w * q4 + p];
+          if (M == 0u) continue;
+          if ((M >> lane) & 1u) {
+            const int at = count + __popc(M & ((1u << lane) - 1u));
+            if (at < kAdamiCap) S.sid[at] = (uint32_t)(w * 32 + lane);
+          }
+          count += __popc(M);
+        }
+        overflow = count > kAdamiCap;
+        __syncwarp();
+        const int nt = count < kAdamiCap ? count : kAdamiCap;
+        for (int t = lane; t < nt; t += 32) {
+          const uint32_t v = S.sid[t];
+          const int r = row_of(v);
+          float w = 0.0f, wp = 0.0f;
+          uint32_t fid = 0;
+          adami_term(k, bpm, (int)(S.sstart[r] + (v - S.vstart[r])), pos, rf, pr, id, w, wp, fid);
+          S.sid[t] = fid;
+          S.sw[t] = w;
+          S.swp[t] = wp;
+        }
+        __syncwarp();
+      } else {
+        count = adami_search(k, bpm, pos, rf, pr, id, ctab, S.sid, S.sw, S.swp, overflow);
+      }
+      adami_sum(count, overflow, S.sid, S.sw, S.swp, bpress + bm, err);
+      __syncwarp();
+    }
   }
 }
 
