@@ -386,3 +386,32 @@ def test_device_capacity_bounds_are_reported_not_exceeded():
         k.compute_timestep()
     assert e.value.status == 6
     k.close()
+
+
+def test_dense_block_takes_the_per_thread_scans_bit_exact():
+    """A fluid block packed so densely (spacing 0.45 h, about 88 particles
+    per cell) that the warp scans' masks cannot hold a neighbourhood: every
+    fluid particle's 27 cells hold some 2,400 candidates (the density kernel
+    takes its per-thread scan) and ~500 neighbours (past the stored list's
+    128: density, forces and XSPH visit the cells again), and the boundary
+    plane under it sees over 1,024 candidates per cell group (the Adami pass
+    takes its per-particle search) with under 256 terms each. Three steps
+    against the oracle, bit for bit, with the boundary pressures."""
+    h, s = 0.01, 0.0045
+    g = (np.arange(12, dtype=np.float32) * np.float32(s) + np.float32(0.03)).astype(np.float32)
+    x, y, z = (a.ravel() for a in np.meshgrid(g, g, g + np.float32(0.0045), indexing="ij"))
+    p = ParticleArrays.from_positions(x, y, z, np.float32(1000.0 * s ** 3))
+    bg = (np.arange(14, dtype=np.float32) * np.float32(s) + np.float32(0.03 - s)).astype(np.float32)
+    bx, by = (a.ravel() for a in np.meshgrid(bg, bg, indexing="ij"))
+    nbp = bx.size
+    b = BoundaryParticles.from_arrays(bx, by, np.full(nbp, 0.03, np.float32), np.full(nbp, 1000.0 * s ** 3),
+                                      np.zeros(nbp), np.zeros(nbp), np.ones(nbp))
+    sc = domain.Scenario("dense_block", p, b, h, (0, 0, -9.81), 20.0, 0.25, 0.0, (0, 0, 0), (0.12, 0.12, 0.12))
+    gpu, cpu = make_pair(sc)
+    for _ in range(3):
+        gpu.step(1e-5)
+        cpu.step(1e-5)
+        assert_same(gpu.particles(), cpu.particles())
+        np.testing.assert_array_equal(gpu.boundary_pressure(), cpu.boundary_pressure())
+    assert np.count_nonzero(gpu.boundary_pressure()) > 0
+    gpu.close()
