@@ -1549,32 +1549,46 @@ __device__ __forceinline__ void adami_sum(int count, bool overflow, uint32_t* si
     if (lane == 0) atomicOr(err, kErrAdamiCap);
     return;
   }
-  if (count <= 32) {
-    // up to 32 terms: one per lane, bitonic-sorted by fluid index across the
-    // lanes, then summed in that order (the same additions as below)
-    __syncwarp();
-    uint32_t key = lane < count ? sid[lane] : 0xffffffffu;
-    float w = lane < count ? sw[lane] : 0.0f;
-    float wp = lane < count ? swp[lane] : 0.0f;
-    for (int kk = 2; kk <= 32; kk <<= 1) {
-      for (int j = kk >> 1; j > 0; j >>= 1) {
-        uint32_t ok = __shfl_xor_sync(0xffffffffu, key, j);
-        float ow = __shfl_xor_sync(0xffffffffu, w, j);
-        float owp = __shfl_xor_sync(0xffffffffu, wp, j);
-        bool up = (lane & kk) == 0, lower = (lane & j) == 0;
-        if (lower == up ? ok < key : ok > key) {
-          key = ok;
-          w = ow;
-          wp = owp;
-        }
-      }
-    }
+  // lane 0 sums the ordered terms, in order (four at a time per 16-byte load
+  // where the arrays allow it; the additions are the same)
+  auto ordered_sum = [&]() {
     float weighted_pressure = 0.0f, weight_sum = 0.0f;
-    for (int q = 0; q < count; ++q) {
-      weighted_pressure += __shfl_sync(0xffffffffu, wp, q);
-      weight_sum += __shfl_sync(0xffffffffu, w, q);
+    int q = 0;
+    if ((reinterpret_cast<uintptr_t>(sw) & 15u) == 0 && (reinterpret_cast<uintptr_t>(swp) & 15u) == 0)
+      for (; q + 3 < count; q += 4) {
+        const float4 a = *reinterpret_cast<const float4*>(swp + q), c = *reinterpret_cast<const float4*>(sw + q);
+        weighted_pressure += a.x;
+        weighted_pressure += a.y;
+        weighted_pressure += a.z;
+        weighted_pressure += a.w;
+        weight_sum += c.x;
+        weight_sum += c.y;
+        weight_sum += c.z;
+        weight_sum += c.w;
+      }
+    for (; q < count; ++q) {
+      weighted_pressure += swp[q];
+      weight_sum += sw[q];
     }
-    if (lane == 0) *out = weight_sum > 1.0e-12f ? fmaxf(weighted_pressure / weight_sum, 0.0f) : 0.0f;
+    *out = weight_sum > 1.0e-12f ? fmaxf(weighted_pressure / weight_sum, 0.0f) : 0.0f;
+  };
+  if (count <= 32) {
+    // up to 32 terms, one per lane: each lane's rank is the number of smaller
+    // fluid indices (they are distinct), and the terms are stored at their
+    // ranks, i.e. in fluid-index order
+    __syncwarp();
+    const uint32_t key = lane < count ? sid[lane] : 0xffffffffu;
+    const float w = lane < count ? sw[lane] : 0.0f;
+    const float wp = lane < count ? swp[lane] : 0.0f;
+    int rank = 0;
+    for (int q = 0; q < count; ++q) rank += __shfl_sync(0xffffffffu, key, q) < key ? 1 : 0;
+    __syncwarp();
+    if (lane < count) {
+      sw[rank] = w;
+      swp[rank] = wp;
+    }
+    __syncwarp();
+    if (lane == 0) ordered_sum();
     return;
   }
   int m2 = 1;
@@ -1598,14 +1612,7 @@ __device__ __forceinline__ void adami_sum(int count, bool overflow, uint32_t* si
       __syncwarp();
     }
   }
-  if (lane == 0) {
-    float weighted_pressure = 0.0f, weight_sum = 0.0f;
-    for (int q = 0; q < count; ++q) {
-      weighted_pressure += swp[q];
-      weight_sum += sw[q];
-    }
-    *out = weight_sum > 1.0e-12f ? fmaxf(weighted_pressure / weight_sum, 0.0f) : 0.0f;
-  }
+  if (lane == 0) ordered_sum();
 }
 
 template <class KP>
@@ -1651,13 +1658,14 @@ constexpr int kAdamiWords = 32;  // mask words per particle: up to 1024 candidat
 struct __align__(16) AdamiWarp {
   float px[36], py[36], pz[36];          // the segment's particles, padded to quads with NaN
   uint32_t mask[kAdamiWords * 32];       // [word][particle]
-  uint32_t vstart[kAdamiRows + 1];       // sequence index of each row's first candidate; [R] = total
-  uint32_t sstart[kAdamiRows];           // slot of each row's first candidate
   uint32_t sid[kAdamiCap];               // a particle's candidates (sequence index), then its terms' fluid ids
   float sw[kAdamiCap], swp[kAdamiCap];
+  uint32_t vstart[kAdamiRows + 1];       // sequence index of each row's first candidate; [R] = total
+  uint32_t sstart[kAdamiRows];           // slot of each row's first candidate
 };
 static_assert(offsetof(AdamiWarp, py) % 16 == 0 && offsetof(AdamiWarp, pz) % 16 == 0 &&
-                  offsetof(AdamiWarp, mask) % 16 == 0 && sizeof(AdamiWarp) % 16 == 0,
+                  offsetof(AdamiWarp, mask) % 16 == 0 && offsetof(AdamiWarp, sw) % 16 == 0 &&
+                  offsetof(AdamiWarp, swp) % 16 == 0 && sizeof(AdamiWarp) % 16 == 0,
               "quad loads and stores");
 
 template <class KP>
