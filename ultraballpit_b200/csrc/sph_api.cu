@@ -4,6 +4,7 @@
 // buffers and CUDA graphs. The step body (9 kernels) is captured once into a
 // graph and replayed; dt lives in device memory so the graph never changes.
 #include <algorithm>
+#include <array>
 #include <chrono>
 #include <cmath>
 #include <cstdlib>
@@ -110,6 +111,7 @@ struct SphHandle {
   // k_adami_cells; used when every instance is in the row or linear order
   uint32_t* border = nullptr;
   bool adami_cells = false;
+  int pool = -1;  // device arrays from the library's pool (1) or cudaMalloc (0); set by the first one
   uint32_t *bc_start = nullptr, *bc_list = nullptr;
   // SDF node grid and wall table (boundary_mode SPH_BOUNDARY_SDF), or the
   // geometry SDF(s) of the closure features
@@ -173,11 +175,37 @@ int cuda_status(SphHandle* h, cudaError_t e, const char* what) {
     if (_e != cudaSuccess) return cuda_status(h, _e, #call); \
   } while (0)
 
+// The handles' device arrays come from one memory pool per device, owned by
+// this library, in stream order on the handle's stream. The pool keeps what
+// a closed handle frees (release threshold: unlimited), so a process that
+// creates simulations one after another reuses mapped memory instead of
+// asking the driver to map it again each time; the memory stays reserved for
+// this library until the process exits.
+cudaMemPool_t device_pool(int dev) {
+  static std::mutex mu;
+  static std::map<int, cudaMemPool_t> pools;
+  std::lock_guard<std::mutex> lock(mu);
+  auto it = pools.find(dev);
+  if (it != pools.end()) return it->second;
+  cudaMemPoolProps props{};
+  props.allocType = cudaMemAllocationTypePinned;
+  props.location.type = cudaMemLocationTypeDevice;
+  props.location.id = dev;
+  cudaMemPool_t pool = nullptr;
+  if (cudaMemPoolCreate(&pool, &props) != cudaSuccess) return nullptr;
+  uint64_t keep = UINT64_MAX;
+  cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  pools[dev] = pool;
+  return pool;
+}
+
 template <class T>
 cudaError_t dalloc(SphHandle* h, T** p, size_t count) {
   *p = nullptr;
   if (count == 0) count = 1;
-  cudaError_t e = cudaMalloc((void**)p, count * sizeof(T));
+  if (h->pool < 0) h->pool = (h->st && device_pool(h->dev)) ? 1 : 0;  // fixed for the handle's life
+  cudaError_t e = h->pool ? cudaMallocFromPoolAsync((void**)p, count * sizeof(T), device_pool(h->dev), h->st)
+                          : cudaMalloc((void**)p, count * sizeof(T));
   if (e == cudaSuccess) h->allocs.push_back((void*)*p);
   return e;
 }
@@ -741,7 +769,12 @@ void ensure_red(SphHandle* h) {
 
 void free_all(SphHandle* h) {
   drop_graphs(h);
-  for (void* p : h->allocs) cudaFree(p);
+  if (h->pool == 1) {  // back to the pool, in stream order
+    for (void* p : h->allocs) cudaFreeAsync(p, h->st);
+    cudaStreamSynchronize(h->st);
+  } else {
+    for (void* p : h->allocs) cudaFree(p);
+  }
   h->allocs.clear();
   if (h->st) cudaStreamDestroy(h->st);
 }
@@ -1013,6 +1046,56 @@ int create_impl(int ninst, const SphParams* PP, const SphParticlesView* pvs,
       h->init_e[q] = e;
     }
   };
+  // The boundary particles ordered by the global cell that holds them
+  // (counting sort, ascending index within a cell), for k_adami_cells; the
+  // cells are those of the grid built below (same f32 operations), on a
+  // thread of its own while this one builds the tables.
+  std::vector<uint32_t> border_h;
+  h->adami_cells = nb > 0;
+  for (int q = 0; q < ninst; ++q)
+    h->adami_cells = h->adami_cells &&
+                     (PP[q].cell_order == SPH_CELL_ORDER_LINEAR || PP[q].cell_order == SPH_CELL_ORDER_ROWS);
+  auto boundary_order = [&] {
+    uint64_t Ctot = 0;
+    std::vector<uint64_t> coffs(ninst);
+    std::vector<std::array<uint32_t, 3>> dimq(ninst);
+    for (int q = 0; q < ninst; ++q) {
+      const float cell = 2.0f * PP[q].h;
+      uint64_t Cq = 1;
+      for (int a = 0; a < 3; ++a) {
+        dimq[q][a] = (uint32_t)fmaxf(ceilf((PP[q].domain_max[a] - PP[q].domain_min[a]) / cell), 1.0f);
+        Cq *= dimq[q][a];
+      }
+      coffs[q] = Ctot;
+      Ctot += Cq;
+    }
+    std::vector<uint32_t> bkey(nb), bnext(Ctot + 1, 0);
+    for (int q = 0; q < ninst; ++q) {
+      const float cell = 2.0f * PP[q].h;
+      auto cell_of = [&](float p, int a) {  // axis_cell, in the same f32 operations
+        float f = std::floor((p - PP[q].domain_min[a]) / cell);
+        f = std::fmax(f, 0.0f);
+        f = std::fmin(f, (float)(dimq[q][a] - 1));
+        return (uint32_t)f;
+      };
+      for (size_t i = h->boff[q]; i < h->boff[q + 1]; ++i) {
+        const float4 v = hb[i];
+        bkey[i] = (uint32_t)coffs[q] + cell_of(v.x, 0) + dimq[q][0] * (cell_of(v.y, 1) + dimq[q][1] * cell_of(v.z, 2));
+        ++bnext[bkey[i] + 1];
+      }
+    }
+    for (uint64_t c = 0; c < Ctot; ++c) bnext[c + 1] += bnext[c];
+    border_h.resize(nb);
+    for (size_t i = 0; i < nb; ++i) border_h[bnext[bkey[i]]++] = (uint32_t)i;
+  };
+  std::thread border_thread;
+  if (h->adami_cells) {
+    try {
+      border_thread = std::thread(boundary_order);
+    } catch (...) {  // no thread to be had: order them here
+      boundary_order();
+    }
+  }
   std::thread totals;
   try {
     totals = std::thread(initial_totals);
@@ -1100,32 +1183,7 @@ int create_impl(int ninst, const SphParams* PP, const SphParticlesView* pvs,
   }
   if (totals.joinable()) totals.join();
   trace.mark("cell ranks, lists, totals");
-  // the boundary particles ordered by the global cell that holds them
-  // (counting sort, ascending index within a cell), for k_adami_cells
-  std::vector<uint32_t> border_h;
-  h->adami_cells = nb > 0;
-  for (int q = 0; q < ninst; ++q) h->adami_cells = h->adami_cells && h->ktab_h[q].rows != 0;
-  if (h->adami_cells) {
-    std::vector<uint32_t> bkey(nb), bnext(C + 1, 0);
-    for (int q = 0; q < ninst; ++q) {
-      const SimConst& kq = h->ktab_h[q];
-      auto cell_of = [&](float p, int a) {  // axis_cell, in the same f32 operations
-        float f = std::floor((p - kq.gmin[a]) / kq.cell);
-        f = std::fmax(f, 0.0f);
-        f = std::fmin(f, (float)(kq.dims[a] - 1));
-        return (uint32_t)f;
-      };
-      for (size_t i = h->boff[q]; i < h->boff[q + 1]; ++i) {
-        const float4 v = hb[i];
-        bkey[i] = (uint32_t)kq.coff + cell_of(v.x, 0) +
-                  (uint32_t)kq.dims[0] * (cell_of(v.y, 1) + (uint32_t)kq.dims[1] * cell_of(v.z, 2));
-        ++bnext[bkey[i] + 1];
-      }
-    }
-    for (uint64_t c = 0; c < C; ++c) bnext[c + 1] += bnext[c];
-    border_h.resize(nb);
-    for (size_t i = 0; i < nb; ++i) border_h[bnext[bkey[i]]++] = (uint32_t)i;
-  }
+  if (border_thread.joinable()) border_thread.join();
   trace.mark("boundary order");
   h->k = h->ktab_h[0];
   h->C = (int)C;
