@@ -189,9 +189,14 @@ void sph_params_default(SphParams *p);
  * plus the obstacle whose SDF `sdf` gives (NULL, or NULL distances: no
  * obstacle); otherwise `sdf` is ignored. Creation uses the host's hardware
  * threads (up to 32) for its tables and allocates the device arrays on a
- * second thread; it returns once the handle is ready. */
+ * second thread; it returns once the handle is ready. The device arrays come
+ * from a memory pool the library keeps per device. */
 int sph_create(const SphParams *params, const SphParticlesView *particles,
                const SphBoundaryView *boundary, const SphSdfView *sdf, SphHandle **out);
+/* Releases the handle. Its device arrays go back to the library's pool,
+ * which keeps them for the next handle created on that device (creating
+ * simulations one after another then skips the driver's mapping of fresh
+ * memory); the pool's memory stays reserved until the process exits. */
 void sph_destroy(SphHandle *h);
 
 /* SimulationKernel::step (lib.rs:287-335). Enqueued asynchronously. */
