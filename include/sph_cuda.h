@@ -22,6 +22,13 @@
  * All arrays are plain host pointers; the library copies inputs to its own
  * device memory at creation and owns every device allocation, stream and
  * CUDA graph it uses.
+ *
+ * Environment variables read at creation: SPH_TRACE (any value) prints the
+ * creation's phase times on stderr; SPH_WARP_SCAN_MIN and
+ * SPH_ADAMI_CELLS_MIN (counts) replace the sizes from which the density scan
+ * and the boundary pressure take their warp-cooperative forms (2048 fluid
+ * and 4096 boundary particles per SM; 0 = always). Both forms give the same
+ * results bit for bit.
  */
 #ifndef SPH_CUDA_H
 #define SPH_CUDA_H

@@ -388,15 +388,20 @@ def test_device_capacity_bounds_are_reported_not_exceeded():
     k.close()
 
 
-def test_dense_block_takes_the_per_thread_scans_bit_exact():
+def test_dense_block_takes_the_per_thread_scans_bit_exact(monkeypatch):
     """A fluid block packed so densely (spacing 0.45 h, about 88 particles
-    per cell) that the warp scans' masks cannot hold a neighbourhood: every
-    fluid particle's 27 cells hold some 2,400 candidates (the density kernel
-    takes its per-thread scan) and ~500 neighbours (past the stored list's
-    128: density, forces and XSPH visit the cells again), and the boundary
-    plane under it sees over 1,024 candidates per cell group (the Adami pass
-    takes its per-particle search) with under 256 terms each. Three steps
-    against the oracle, bit for bit, with the boundary pressures."""
+    per cell) that the warp scans' masks cannot hold a neighbourhood: many
+    fluid particles' 27 cells hold up to some 1,600 candidates (the density
+    kernel's warp scan hands them to its per-thread scan) and up to ~360
+    neighbours (past the stored list's 128: density, forces and XSPH visit
+    the cells again), and the boundary plane under it sees over 1,024
+    candidates per cell group (the cell-wise Adami pass takes its
+    per-particle search) with under 256 terms each. The warp-cooperative
+    forms are forced (the block is below the sizes at which the library
+    picks them). Three steps against the oracle, bit for bit, with the
+    boundary pressures."""
+    monkeypatch.setenv("SPH_WARP_SCAN_MIN", "0")
+    monkeypatch.setenv("SPH_ADAMI_CELLS_MIN", "0")
     h, s = 0.01, 0.0045
     g = (np.arange(12, dtype=np.float32) * np.float32(s) + np.float32(0.03)).astype(np.float32)
     x, y, z = (a.ravel() for a in np.meshgrid(g, g, g + np.float32(0.0045), indexing="ij"))

@@ -112,6 +112,12 @@ struct SphHandle {
   uint32_t* border = nullptr;
   bool adami_cells = false;
   int pool = -1;  // device arrays from the library's pool (1) or cudaMalloc (0); set by the first one
+  // Below these sizes the per-particle forms of the density scan and of the
+  // boundary pressure run instead of the warp-cooperative ones: a warp per 32
+  // particles (or boundary particles) then leaves the SMs too few warps to
+  // hide the longer per-warp chains. Set at creation from the SM count.
+  int warp_scan_min = 0;
+  size_t adami_cells_min = 0;
   uint32_t *bc_start = nullptr, *bc_list = nullptr;
   // SDF node grid and wall table (boundary_mode SPH_BOUNDARY_SDF), or the
   // geometry SDF(s) of the closure features
@@ -566,6 +572,20 @@ void dispatch(SphHandle* h, bool boundary, F&& f) {
 
 sph::Planes planes(SphHandle* h) { return sph::Planes{h->xyz, h->xyz_stride}; }
 
+// Sizes per SM from which the warp-cooperative density scan (particles) and
+// the cell-wise boundary pressure (boundary particles) run, measured on B200.
+// Below them the per-particle forms are faster (2M-particle dam break and its
+// coarser versions: the density scans break even near 250k particles, the
+// boundary passes between 376k and 848k boundary particles). The environment
+// variables SPH_WARP_SCAN_MIN and SPH_ADAMI_CELLS_MIN, read at creation,
+// replace them with absolute counts (0: always the warp-cooperative form).
+#ifndef SPH_WARP_SCAN_MIN_PER_SM
+#define SPH_WARP_SCAN_MIN_PER_SM 2048
+#endif
+#ifndef SPH_ADAMI_CELLS_MIN_PER_SM
+#define SPH_ADAMI_CELLS_MIN_PER_SM 4096
+#endif
+
 // Lets the density kernels take up to 128 KiB of dynamic shared memory (the
 // warp scan's per-warp scratch passes the default 48 KiB at 512 threads) on
 // the current device. Set at handle creation, before any graph capture.
@@ -602,7 +622,8 @@ void enqueue_density_only(SphHandle* h) {
   if (h->cl_mode) cudaMemsetAsync(h->cl_count, 0, sizeof(uint32_t), h->st);
   // the warp scan's scratch per warp; closure mode 2 adds a 16-sample network
   // tile per warp (the fused inference)
-  const size_t smem = (bs / 32) * sizeof(ScanWarp);
+  const int warp_scan = h->n >= h->warp_scan_min ? 1 : 0;
+  const size_t smem = warp_scan ? (bs / 32) * sizeof(ScanWarp) : 0;
   const size_t smem_cl = smem + (bs / 32) * kClTileWords * sizeof(uint32_t);
   dispatch(h, false, [&](auto kp) {
     using KPT = decltype(kp);
@@ -610,15 +631,18 @@ void enqueue_density_only(SphHandle* h) {
     if (h->cl_mode == 2)
       k_density<KPT, 2><<<grid, bs, smem_cl, h->st>>>(kp, h->n, h->dt, h->pos, planes(h), h->rv, h->id, h->ctab,
                                                      h->bc_start, h->bc_list, h->bpos, h->rf, h->pr, h->err,
-                                                     h->nbr, h->ncount, h->sdf, h->wall_tab, cb);
+                                                     h->nbr, h->ncount, h->sdf, h->wall_tab, cb,
+                                                  warp_scan);
     else if (h->cl_mode)
       k_density<KPT, 1><<<grid, bs, smem, h->st>>>(kp, h->n, h->dt, h->pos, planes(h), h->rv, h->id, h->ctab,
                                                   h->bc_start, h->bc_list, h->bpos, h->rf, h->pr, h->err,
-                                                  h->nbr, h->ncount, h->sdf, h->wall_tab, cb);
+                                                  h->nbr, h->ncount, h->sdf, h->wall_tab, cb,
+                                                  warp_scan);
     else
       k_density<KPT, 0><<<grid, bs, smem, h->st>>>(kp, h->n, h->dt, h->pos, planes(h), h->rv, h->id, h->ctab,
                                                   h->bc_start, h->bc_list, h->bpos, h->rf, h->pr, h->err,
-                                                  h->nbr, h->ncount, h->sdf, h->wall_tab, cb);
+                                                  h->nbr, h->ncount, h->sdf, h->wall_tab, cb,
+                                                  warp_scan);
   });
   h->launches += 1;
 }
@@ -633,7 +657,7 @@ void enqueue_adami(SphHandle* h) {
       k_adami_mark<<<grid_for(h->nbc_cells, 8), 256, 0, h->st>>>(h->nbc_cells, h->bc_cells, h->ctab, h->bc_start,
                                                                   h->bc_list, h->bact);
     dispatch(h, true, [&](auto kp) {
-      if (h->adami_cells)
+      if (h->adami_cells && (size_t)h->nb >= h->adami_cells_min)
         k_adami_cells<<<grid_for(h->nb, kAdamiWarps * 32), kAdamiWarps * 32, 0, h->st>>>(
             kp, h->nb, h->border, h->bpos, h->bpress, h->pos, planes(h), h->rf, h->pr, h->id, h->ctab, h->err,
             h->bact);
@@ -925,6 +949,12 @@ int create_impl(int ninst, const SphParams* PP, const SphParticlesView* pvs,
     }
     ae = cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking);
     allow_density_smem();
+    int sms = 148;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->dev) != cudaSuccess) sms = 148;
+    h->warp_scan_min = sms * SPH_WARP_SCAN_MIN_PER_SM;
+    h->adami_cells_min = (size_t)sms * SPH_ADAMI_CELLS_MIN_PER_SM;
+    if (const char* v = std::getenv("SPH_WARP_SCAN_MIN")) h->warp_scan_min = std::atoi(v);
+    if (const char* v = std::getenv("SPH_ADAMI_CELLS_MIN")) h->adami_cells_min = (size_t)std::atoll(v);
 #define ALLOC(ptr, cnt) \
   if (ae == cudaSuccess) ae = dalloc(h, &h->ptr, (cnt))
     ALLOC(pos, n); ALLOC(vel, n); ALLOC(velout, n); ALLOC(acc, n);

@@ -1211,7 +1211,7 @@ k_density(KP kp, int n, const float* __restrict__ dtp, const float4* __restrict_
           const uint32_t* __restrict__ bc_list, const float4* __restrict__ bpos,
           float2* __restrict__ rf, float* __restrict__ pr, const uint32_t* __restrict__ err,
           uint32_t* __restrict__ nbr, uint32_t* __restrict__ ncount, const float* __restrict__ sdf,
-          const float2* __restrict__ wall_tab, ClosureBufs cb) {
+          const float2* __restrict__ wall_tab, ClosureBufs cb, int warp_scan) {
   // a warp wholly past the end leaves at once; every other lane takes part
   // in the warp scan (and, with CL = 2, in the network epilogue)
   if (blockIdx.x * blockDim.x + (threadIdx.x & ~31u) >= (unsigned)n) return;
@@ -1258,10 +1258,16 @@ k_density(KP kp, int n, const float* __restrict__ dtp, const float4* __restrict_
     term(s, pj, dx, dy, dz, dx * dx + dy * dy + dz * dz);
   };
   // Phase 1: the warp scan lists every lane's in-support slots in visit order
-  // and feeds them to the terms as it lists them.
+  // and feeds them to the terms as it lists them. A simulation too small to
+  // fill the GPU with warps of 32 particles (warp_scan = 0) takes the
+  // per-thread scan instead: more, shorter warps hide its latency better.
   bool fed = false;
-  const uint32_t listed = scan_warp(kp, i, live, pl, ctab, reinterpret_cast<ScanWarp*>(s_dyn)[threadIdx.x >> 5],
-                                    nbr, n, pair, single, fed);
+  uint32_t listed = 0;
+  if (warp_scan)
+    listed = scan_warp(kp, i, live, pl, ctab, reinterpret_cast<ScanWarp*>(s_dyn)[threadIdx.x >> 5], nbr, n, pair,
+                       single, fed);
+  else if (live)
+    listed = record_neighbors(pi.x, pi.y, pi.z, i, pl, ctab, ScanGeo(k), nbr, n);
   bool near_wall = false;
   float f[16];
   float rho_pre = 0.0f;
@@ -1376,7 +1382,7 @@ k_density(KP kp, int n, const float* __restrict__ dtp, const float4* __restrict_
   if (CL == 2) {
     // network epilogue: up to 16 of the warp's near-wall particles per tile
     const int lane = threadIdx.x & 31;
-    uint32_t* tile = reinterpret_cast<uint32_t*>(s_dyn + (blockDim.x >> 5) * sizeof(ScanWarp)) +
+    uint32_t* tile = reinterpret_cast<uint32_t*>(s_dyn + (warp_scan ? (blockDim.x >> 5) * sizeof(ScanWarp) : 0)) +
                      (threadIdx.x >> 5) * kClTileWords;
     __nv_bfloat16* xt = reinterpret_cast<__nv_bfloat16*>(tile);
     float* yt = reinterpret_cast<float*>(tile + 16 * 16 / 2);
