@@ -44,9 +44,11 @@ CLOSURE_WEIGHTS = os.path.join(ROOT, "ultraballpit_b200", "data", "closure_weigh
 
 
 def pair_stats(sc, sample: int = 20000, seed: int = 0) -> dict:
-    """Mean in-support neighbours (interactions) and mean 27-cell candidates
-    after the kernel's cell culling, per particle, on a seeded sample of the
-    initial state (2h grid cells, as the kernels bin)."""
+    """Mean in-support neighbours (interactions) and mean candidates per
+    particle on a seeded sample of the initial state (2h grid cells, as the
+    kernels bin): every particle of the 27 cells, as the reference's neighbour
+    loop tests them (neighbor.rs:129-182) and as the warp-cooperative density
+    scan does, and the fewer left after the per-thread scan's cell culling."""
     from scipy.spatial import cKDTree
     p = sc.particles
     pos = np.stack([p.x, p.y, p.z], axis=1).astype(np.float64)
@@ -65,16 +67,20 @@ def pair_stats(sc, sample: int = 20000, seed: int = 0) -> dict:
     lo2 = np.maximum(pq - face, 0.0) ** 2
     hi2 = np.maximum(face + cell - pq, 0.0) ** 2
     cand = np.zeros(len(pick))
+    cand_all = np.zeros(len(pick))
     for dz in (-1, 0, 1):
         for dy in (-1, 0, 1):
             for dx in (-1, 0, 1):
                 d = np.array([dx, dy, dz])
                 e = sum(np.where(d[a] < 0, lo2[:, a], np.where(d[a] > 0, hi2[:, a], 0.0)) for a in range(3))
                 nc = cq + d
-                ok = np.all((nc >= 0) & (nc < dims), axis=1) & (e <= r * r)
+                inside = np.all((nc >= 0) & (nc < dims), axis=1)
+                ok = inside & (e <= r * r)
                 l2 = (nc[:, 2] * dims[1] + nc[:, 1]) * dims[0] + nc[:, 0]
                 cand += np.where(ok, counts[np.where(ok, l2, 0)], 0)
-    return {"interactions_per_particle": float(inter.mean()), "candidates_per_particle": float(cand.mean() - 1),
+                cand_all += np.where(inside, counts[np.where(inside, l2, 0)], 0)
+    return {"interactions_per_particle": float(inter.mean()), "candidates_per_particle": float(cand_all.mean() - 1),
+            "candidates_after_culling_per_particle": float(cand.mean() - 1),
             "sample": f"{len(pick)} particles of the initial state"}
 
 

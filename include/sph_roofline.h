@@ -39,11 +39,13 @@
  * the FP32 peak: 128 lanes per SM x 148 SMs x the SM clock.
  *
  *   candidate test of the 27-cell scan: 3 sub, 3 mul, 2 add, 1 compare     9
+ *     (per particle of the 27 cells, as the reference's neighbour loop
+ *     tests them, neighbor.rs:129-182)
  *   density interaction: distance 8, sqrt 1, gradient 17, r.gradW 5,
  *     density difference 1, delta-SPH term 6, W 10, rho += m W 2           50
  *   forces interaction: distance 8, sqrt 1, gradient 17, pressure factor 3,
- *     pressure sum 6, dv 3, v.r 5, compare 1, viscous term 18 (counted
- *     as always taken: an upper bound)                                     62
+ *     pressure sum 6, dv 3, v.r 5, compare 1, viscous term 18 (evaluated
+ *     for every pair, a receding one adding a signed zero)                 62
  *   XSPH interaction: distance 8, sqrt 1, W 10, rho avg 2, factor 3,
  *     velocity sum 9                                                       33
  */
