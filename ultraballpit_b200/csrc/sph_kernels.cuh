@@ -1829,7 +1829,27 @@ k_adami_cells(KP kp, int nb, const uint32_t* __restrict__ border, const float4* 
       }
     }
     __syncwarp();
-    // each member in turn: its terms, then their ordered sum
+    // Each member in turn: its terms, then their ordered sum. A member with
+    // up to 32 terms leaves them ordered in sw / swp from `base`, and its sum
+    // waits: the pending members are summed together, one per lane, each in
+    // its own order (the same additions as adami_sum's), when the arrays
+    // fill up, before a member that needs them whole, and at the end.
+    int npend = 0, base = 0;
+    int pend_b = 0, pend_base = 0, pend_count = 0;  // lane j: pending member j
+    auto flush = [&]() {
+      __syncwarp();
+      if (lane < npend) {
+        float weighted_pressure = 0.0f, weight_sum = 0.0f;
+        for (int q = 0; q < pend_count; ++q) {
+          weighted_pressure += S.swp[pend_base + q];
+          weight_sum += S.sw[pend_base + q];
+        }
+        bpress[pend_b] = weight_sum > 1.0e-12f ? fmaxf(weighted_pressure / weight_sum, 0.0f) : 0.0f;
+      }
+      __syncwarp();
+      npend = 0;
+      base = 0;
+    };
     for (uint32_t mm = members; mm; mm &= mm - 1u) {
       const int ml = __ffs(mm) - 1;
       const int p = __popc(members & ((1u << ml) - 1u));
@@ -1850,6 +1870,33 @@ k_adami_cells(KP kp, int nb, const uint32_t* __restrict__ border, const float4* 
         }
         overflow = count > kAdamiCap;
         __syncwarp();
+        if (count <= 32) {
+          // one term per lane, placed at its rank (the count of smaller fluid indices)
+          float w = 0.0f, wp = 0.0f;
+          uint32_t fid = 0xffffffffu;
+          if (lane < count) {
+            const uint32_t v = S.sid[lane];
+            const int r = row_of(v);
+            adami_term(k, bpm, (int)(S.sstart[r] + (v - S.vstart[r])), pos, rf, pr, id, w, wp, fid);
+          }
+          int rank = 0;
+          for (int q = 0; q < count; ++q) rank += __shfl_sync(kAll, fid, q) < fid ? 1 : 0;
+          if (base + count > kAdamiCap || npend == 32) flush();
+          if (lane < count) {
+            S.sw[base + rank] = w;
+            S.swp[base + rank] = wp;
+          }
+          if (lane == npend) {
+            pend_b = bm;
+            pend_base = base;
+            pend_count = count;
+          }
+          ++npend;
+          base += count;
+          __syncwarp();
+          continue;
+        }
+        flush();  // the arrays are needed whole
         const int nt = count < kAdamiCap ? count : kAdamiCap;
         for (int t = lane; t < nt; t += 32) {
           const uint32_t v = S.sid[t];
@@ -1863,11 +1910,13 @@ k_adami_cells(KP kp, int nb, const uint32_t* __restrict__ border, const float4* 
         }
         __syncwarp();
       } else {
+        flush();
         count = adami_search(k, bpm, pos, rf, pr, id, ctab, S.sid, S.sw, S.swp, overflow);
       }
       adami_sum(count, overflow, S.sid, S.sw, S.swp, bpress + bm, err);
       __syncwarp();
     }
+    flush();
   }
 }
 
