@@ -70,7 +70,17 @@ def _same(a, b):
         np.testing.assert_array_equal(getattr(a, f), getattr(b, f), err_msg=f)
 
 
-def test_capture_mode_and_zero_network_leave_the_step_unchanged():
+@pytest.fixture(params=["warp_scan", "per_thread_scan"])
+def scan_form(request, monkeypatch):
+    """The density kernel in each of its scan forms (the fused network and the
+    feature capture sit in its epilogue, after either)."""
+    v = "0" if request.param == "warp_scan" else str(1 << 40)
+    monkeypatch.setenv("SPH_WARP_SCAN_MIN", v)
+    monkeypatch.setenv("SPH_ADAMI_CELLS_MIN", v)
+    return request.param
+
+
+def test_capture_mode_and_zero_network_leave_the_step_unchanged(scan_form):
     sc = _tank()
     plain = _sdf_kernel(sc)
     cap = _sdf_kernel(sc)
@@ -90,7 +100,7 @@ def test_capture_mode_and_zero_network_leave_the_step_unchanged():
     np.testing.assert_allclose(np.linalg.norm(feat[:, 1:4], axis=1), 1.0, atol=1e-4)
 
 
-def test_applied_density_correction_is_the_network_output():
+def test_applied_density_correction_is_the_network_output(scan_form):
     sc = _tank(seed=12)
     net = closure.ClosureNet(seed=7)
     k = _sdf_kernel(sc)
