@@ -185,9 +185,9 @@ def test_trained_closure_gain_over_the_plain_method():
 
 
 def test_shipped_closure_lowers_the_near_wall_pressure_error_of_tanks_at_rest():
-    """The shipped network (trained on 64 tank pairs)
+    """The shipped network (trained on 64 pairs of 4 mm and 2 mm tank runs)
     against the plain 4 mm method on two tanks at rest that training never
-    saw, both judged by the 2 mm run: the closure's mean near-wall pressure
+    saw, both measured against the 2 mm run: the closure's mean near-wall pressure
     error is below the plain method's. (In tanks set moving, the coarse
     error is the sloshing phase, which near-wall features cannot predict;
     there the closure gains nothing.)"""

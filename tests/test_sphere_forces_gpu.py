@@ -1,4 +1,4 @@
-"""The force series of BASELINE config 2 (``ultraballpit_b200.sphere_run``)
+"""The sphere force series (``ultraballpit_b200.sphere_run``)
 against the CPU oracle: the first 10 steps of the 2,000,000-particle dam
 break with the sphere, sampled every 5 steps. The states are bit-identical
 (correctly rounded x^7 in both; every field of every particle compared after

@@ -1,5 +1,5 @@
-"""BASELINE config 2 as specified: the 2,000,000-particle dam break with the
-fixed sphere for 2000 steps, reporting the pressure and viscous force
+"""The 2,000,000-particle dam break (dx = 1 mm) with the fixed sphere for
+2000 steps, reporting the pressure and viscous force
 integrals on the sphere.
 
     python -m ultraballpit_b200.sphere_run [--steps 2000] [--every 50] [--out FILE]
