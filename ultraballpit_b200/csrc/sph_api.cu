@@ -510,22 +510,26 @@ void build_boundary_lists(const SimConst& k, const SphBoundaryView* b, int C,
         if (!(pos[a] == pos[a])) empty = true;
       }
       if (empty) continue;
+      // squared distance from the particle to each candidate cell's slab, per
+      // axis (a cell's box is widened by `margin`, edge cells unbounded
+      // outward); a cell's d2 is their sum, x + y + z in that order
+      double e2[3][8];
+      for (int a = 0; a < 3; ++a)
+        for (int c = lo[a]; c <= hi[a] && c - lo[a] < 8; ++c) {
+          double blo = c == 0 ? -1e300 : k.gmin[a] + c * cs - margin;
+          double bhi = c == k.dims[a] - 1 ? 1e300 : k.gmin[a] + (c + 1) * cs + margin;
+          double d = pos[a] < blo ? blo - pos[a] : (pos[a] > bhi ? pos[a] - bhi : 0.0);
+          e2[a][c - lo[a]] = d * d;
+        }
       for (int cz = lo[2]; cz <= hi[2]; ++cz)
-        for (int cy = lo[1]; cy <= hi[1]; ++cy)
+        for (int cy = lo[1]; cy <= hi[1]; ++cy) {
+          const double ezy = e2[1][cy - lo[1]];
+          const uint64_t row = (uint64_t)cy * k.dims[0] + (uint64_t)cz * k.dims[0] * k.dims[1];
           for (int cx = lo[0]; cx <= hi[0]; ++cx) {
-            int c3[3] = {cx, cy, cz};
-            double d2 = 0.0;
-            for (int a = 0; a < 3; ++a) {
-              double blo = c3[a] == 0 ? -1e300 : k.gmin[a] + c3[a] * cs - margin;
-              double bhi = c3[a] == k.dims[a] - 1 ? 1e300 : k.gmin[a] + (c3[a] + 1) * cs + margin;
-              double d = pos[a] < blo ? blo - pos[a] : (pos[a] > bhi ? pos[a] - bhi : 0.0);
-              d2 += d * d;
-            }
-            if (d2 < reach * reach) {
-              uint64_t lin = (uint64_t)cx + (uint64_t)cy * k.dims[0] + (uint64_t)cz * k.dims[0] * k.dims[1];
-              out.push_back((lin << 32) | (uint64_t)bi);
-            }
+            const double d2 = (e2[0][cx - lo[0]] + ezy) + e2[2][cz - lo[2]];
+            if (d2 < reach * reach) out.push_back(((row + (uint64_t)cx) << 32) | (uint64_t)bi);
           }
+        }
     }
     std::lock_guard<std::mutex> lock(mu);
     used = std::max(used, t + 1);
