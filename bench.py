@@ -92,15 +92,26 @@ def roofline_bytes():
 KERNEL_SOURCES = ["ultraballpit_b200/csrc/sph_kernels.cuh", "ultraballpit_b200/csrc/sph_mlp.cuh"]
 
 
-def kernel_sources_digest() -> str:
-    """sha1 over the step's kernel sources (whitespace removed, so a change of
-    layout alone keeps it) and the default launch shapes: an ncu figure
-    recorded with the same digest was captured on these kernels."""
+def strip_source(src: bytes) -> bytes:
+    """C++ source without comments and whitespace: what a digest of the
+    kernels should see (string literals in these files hold no comment
+    markers)."""
+    src = re.sub(rb"/\*.*?\*/", b"", src, flags=re.S)
+    src = re.sub(rb"//[^\n]*", b"", src)
+    return re.sub(rb"\s+", b"", src)
+
+
+def kernel_sources_digest(read=None) -> str:
+    """sha1 over the step's kernel sources (comments and whitespace removed,
+    so a change of wording or layout alone keeps it) and the default launch
+    shapes: an ncu figure recorded with the same digest was captured on these
+    kernels. `read(path)` returns a file's bytes (default: this tree)."""
     import hashlib
+    read = read or (lambda f: open(os.path.join(ROOT, f), "rb").read())
     h = hashlib.sha1()
     for f in KERNEL_SOURCES:
-        h.update(re.sub(rb"\s+", b"", open(os.path.join(ROOT, f), "rb").read()))
-    api = open(os.path.join(ROOT, "ultraballpit_b200", "csrc", "sph_api.cu")).read()
+        h.update(strip_source(read(f)))
+    api = read("ultraballpit_b200/csrc/sph_api.cu").decode()
     h.update(re.search(r"int bs_xsph = \d+, bs_density = \d+, bs_forces = \d+;", api).group(0).encode())
     return h.hexdigest()
 

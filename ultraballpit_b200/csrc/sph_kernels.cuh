@@ -1277,8 +1277,9 @@ k_density(KP kp, int n, const float* __restrict__ dtp, const float4* __restrict_
     float rho_wall = 0.0f;  // closure: wall density
     uint32_t nwall = 0;
     ncount[i] = listed;
-    // Phase 2 (a neighbourhood too large for the warp scan's masks): the
-    // terms over the list just stored, or over the cells past its capacity.
+    // Phase 2 (the per-thread scan, or a neighbourhood too large for the warp
+    // scan's masks): the terms over the list just stored, or over the cells
+    // past its capacity.
     if (!fed) {
       if (listed <= kNbrCap) {
         // the list was written above by this thread: plain (coherent) loads
